@@ -1,0 +1,619 @@
+// ridge.cu -- batched weighted ridge solves over node-sorted segments.
+//
+// One call solves K independent systems (n_k rows, d_k inputs, p_k
+// features) following solve_weighted_ridge (art/models.py:218-371):
+//   G = Phi^T diag(max(w, floor)) Phi,  h = Phi^T (max(w, floor) y),
+//   lambda = ridge * trace(G) / p,  (G + lambda I) beta = h.
+// Features are generated on chip from x and never stored in HBM (the
+// reference's batched form materialises Phi and W*Phi,
+// art/_cuda_batched_cholesky_kernels.cu:138-148).
+//
+// Launch sequence (all stream-ordered, no host sync):
+//   plan_hist -> plan_scan -> plan_scatter : per-class work lists, largest
+//       cost first (log2 buckets of n*(p+1)^2), built on the device;
+//   [mixed] ridge_tc_kernel                : tcgen05 Gram + refinement;
+//   ridge_fp64_kernel<4>, <8>              : persistent FP64 work queues;
+//   ridge_fp64_kernel<8> on the resolve list (mixed systems that did not
+//       converge); ridge_qr_kernel on the auto-solver fallback list.
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+#include <algorithm>
+
+#include "ridge.cuh"
+
+namespace art {
+
+// ====================================================================== plan
+__device__ __forceinline__ int plan_class(const RidgeArgs& a, int p) {
+  if (a.precision == ART_PRECISION_MIXED && p >= kTensorMinP) return CLS_TENSOR;
+  return (p + 1 <= kSmallMaxAug) ? CLS_SMALL : CLS_LARGE;
+}
+
+__device__ __forceinline__ int plan_bucket(int64_t n, int p) {
+  double cost = (double)(n + 1) * (double)(p + 1) * (double)(p + 1);
+  int e = ilogb(cost);
+  return kBuckets - 1 - max(0, min(kBuckets - 1, e));  // bucket 0 = largest
+}
+
+// Validate each item, pick its class and cost bucket, count.
+__global__ void ridge_plan_hist(RidgeArgs a, RidgeLists L) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.K) return;
+  const int d = a.dims[k], kind = a.features[k];
+  const int p = feature_count(d, kind);
+  const int64_t n = a.row_offsets[k + 1] - a.row_offsets[k];
+  if (d < 1 || d > a.dmax || p < 1 || p > a.pmax || n < 0) {
+    const double nan = __longlong_as_double(0x7ff8000000000000ll);
+    a.status[k] = -4;
+    if (a.ridge_eff) a.ridge_eff[k] = nan;
+    if (a.cond) a.cond[k] = nan;
+    if (a.info) a.info[k] = 0u;
+    for (int i = 0; i < a.pmax; ++i) a.beta[k * a.beta_stride + i] = nan;
+    return;
+  }
+  atomicAdd(&L.hist[plan_class(a, p) * kBuckets + plan_bucket(n, p)], 1);
+}
+
+__global__ void ridge_plan_scan(RidgeLists L) {
+  // one block of kPlanClasses warps; warp c scans class c's buckets
+  const int c = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (c >= kPlanClasses) return;
+  int carry = 0;
+  for (int base = 0; base < kBuckets; base += 32) {
+    int v = L.hist[c * kBuckets + base + lane];
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    L.start[c * kBuckets + base + lane] = carry + incl - v;
+    carry += __shfl_sync(0xffffffffu, incl, 31);
+  }
+  if (lane == 0) L.count[c] = carry;
+}
+
+__global__ void ridge_plan_scatter(RidgeArgs a, RidgeLists L) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.K) return;
+  const int d = a.dims[k], kind = a.features[k];
+  const int p = feature_count(d, kind);
+  const int64_t n = a.row_offsets[k + 1] - a.row_offsets[k];
+  if (d < 1 || d > a.dmax || p < 1 || p > a.pmax || n < 0) return;
+  const int c = plan_class(a, p), b = plan_bucket(n, p);
+  const int slot = atomicSub(&L.hist[c * kBuckets + b], 1) - 1;
+  L.list[(int64_t)c * a.K + L.start[c * kBuckets + b] + slot] = (int32_t)k;
+}
+
+// ============================================================ FP64 kernel
+// Shared-memory layout, identical on host and device.
+struct Fp64Layout {
+  int ldp;        // max padded augmented width
+  int chunk;
+  size_t off_x[2], off_y[2], off_w[2], off_bar, off_phi, off_q, off_gram, off_fa, off_fb,
+      off_vec, total;
+};
+
+__host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
+
+__host__ __device__ inline Fp64Layout fp64_layout(int pmax, int dmax, int ts, int chunk) {
+  Fp64Layout L;
+  const int pa = pmax + 1;
+  L.ldp = ((pa + ts - 1) / ts) * ts;
+  L.chunk = chunk;
+  size_t o = 0;
+  for (int s = 0; s < 2; ++s) {
+    L.off_x[s] = o; o = align16(o + (size_t)chunk * dmax * 8 + 16);
+    L.off_y[s] = o; o = align16(o + (size_t)chunk * 8 + 16);
+    L.off_w[s] = o; o = align16(o + (size_t)chunk * 8 + 16);
+  }
+  L.off_bar = o; o = align16(o + 2 * 8);
+  L.off_phi = o; o = align16(o + (size_t)chunk * L.ldp * 8);
+  L.off_q = o; o = align16(o + (size_t)chunk * 8);
+  L.off_gram = o; o = align16(o + (size_t)pa * (pa + 1) / 2 * 8);
+  L.off_fa = o; o = align16(o + (size_t)L.ldp * 2);
+  L.off_fb = o; o = align16(o + (size_t)L.ldp * 2);
+  L.off_vec = o; o = align16(o + (size_t)3 * (pa + 1) * 8);
+  L.total = o;
+  return L;
+}
+
+__device__ __forceinline__ int tile_row(int t) {
+  int I = (int)((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
+  while (I * (I + 1) / 2 > t) --I;
+  while ((I + 1) * (I + 2) / 2 <= t) ++I;
+  return I;
+}
+
+// Issue the bulk copies of chunk c (x rows, y, w) into stage st.
+__device__ __forceinline__ void issue_chunk(const RidgeArgs& a, const RidgeItem& it, int chunk,
+                                            int64_t c, unsigned char* smem, const Fp64Layout& lay,
+                                            int st, uint64_t* bar) {
+  const int64_t rr = c * chunk;
+  const int rows = (int)min((int64_t)chunk, it.n - rr);
+  Granules gx = granules(a.x + it.xoff + rr * it.d, (uint64_t)rows * it.d * 8);
+  Granules gy = granules(a.y + it.r0 + rr, (uint64_t)rows * 8);
+  Granules gw = a.w ? granules(a.w + it.r0 + rr, (uint64_t)rows * 8) : Granules{nullptr, 0, 0};
+  mbar_arrive_expect_tx(bar, gx.bytes + gy.bytes + gw.bytes);
+  bulk_g2s(smem + lay.off_x[st], gx.base, gx.bytes, bar);
+  bulk_g2s(smem + lay.off_y[st], gy.base, gy.bytes, bar);
+  if (a.w) bulk_g2s(smem + lay.off_w[st], gw.base, gw.bytes, bar);
+}
+
+template <int TS, int CHUNK>
+__global__ void __launch_bounds__(kRidgeThreads) ridge_fp64_kernel(RidgeArgs a, RidgeLists L,
+                                                                   int cls, int pcap) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_item, s_fail;
+  __shared__ double s_scalar[4];
+  const Fp64Layout lay = fp64_layout(pcap, a.dmax, TS, CHUNK);
+  uint64_t* bars = (uint64_t*)(smem + lay.off_bar);
+  double* phi = (double*)(smem + lay.off_phi);
+  double* q = (double*)(smem + lay.off_q);
+  double* G = (double*)(smem + lay.off_gram);
+  int16_t* fa = (int16_t*)(smem + lay.off_fa);
+  int16_t* fb = (int16_t*)(smem + lay.off_fb);
+  double* vec = (double*)(smem + lay.off_vec);
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  uint32_t uses0 = 0, uses1 = 0;  // completed phases per stage (uniform)
+  const int count = L.count[cls];
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(&L.cursor[cls], 1);
+    __syncthreads();
+    const int item = s_item;
+    __syncthreads();
+    if (item >= count) break;
+    const int k = L.list[(int64_t)cls * a.K + item];
+    const RidgeItem it = load_item(a, k);
+    const int p = it.p, pa = p + 1, d = it.d;
+    const int nb = (pa + TS - 1) / TS;
+    const int ldpi = nb * TS;
+    const int T = nb * (nb + 1) / 2;
+    const int S = max(1, kRidgeThreads / T);
+    for (int f = tid; f < ldpi; f += kRidgeThreads) {
+      int fa_, fb_;
+      if (f < p) feature_factors(d, it.kind, f, fa_, fb_);
+      else if (f == p) { fa_ = -2; fb_ = -1; }
+      else { fa_ = -3; fb_ = -1; }
+      fa[f] = (int16_t)fa_;
+      fb[f] = (int16_t)fb_;
+    }
+    const bool mine = tid < T * S;
+    const int tile = tid % T, slice = tid / T;
+    const int I = tile_row(tile), J = tile - I * (I + 1) / 2;
+    double acc[TS][TS];
+#pragma unroll
+    for (int i = 0; i < TS; ++i)
+#pragma unroll
+      for (int j = 0; j < TS; ++j) acc[i][j] = 0.0;
+    int bad = 0;
+    const int64_t nchunks = (it.n + CHUNK - 1) / CHUNK;
+    if (tid == 0) {
+      for (int64_t c = 0; c < min((int64_t)2, nchunks); ++c)
+        issue_chunk(a, it, CHUNK, c, smem, lay, (int)c, &bars[c]);
+    }
+    __syncthreads();  // fa/fb visible
+    bool timed_out = false;
+    for (int64_t c = 0; c < nchunks; ++c) {
+      const int st = (int)(c & 1);
+      const uint32_t par = st ? (uses1 & 1) : (uses0 & 1);
+      const bool ok = mbar_wait(&bars[st], par);
+      if (st) ++uses1; else ++uses0;
+      if (!__syncthreads_and(ok)) { timed_out = true; break; }
+      const int rows = (int)min((int64_t)CHUNK, it.n - c * CHUNK);
+      const double* xs =
+          (const double*)(smem + lay.off_x[st] +
+                          (((uintptr_t)(a.x + it.xoff + c * CHUNK * d)) & 15));
+      const double* ys =
+          (const double*)(smem + lay.off_y[st] + (((uintptr_t)(a.y + it.r0 + c * CHUNK)) & 15));
+      const double* ws =
+          a.w ? (const double*)(smem + lay.off_w[st] +
+                                (((uintptr_t)(a.w + it.r0 + c * CHUNK)) & 15))
+              : nullptr;
+      for (int e = tid; e < rows * d; e += kRidgeThreads) bad |= isfinite(xs[e]) ? 0 : 1;
+      for (int r = tid; r < rows; r += kRidgeThreads) {
+        bad |= isfinite(ys[r]) ? 0 : 1;
+        double wv = ws ? ws[r] : 1.0;
+        if (!(wv >= 0.0) || !isfinite(wv)) bad |= 2;
+        q[r] = fmax(wv, a.weight_floor);
+      }
+      for (int e = tid; e < rows * ldpi; e += kRidgeThreads) {
+        const int r = e / ldpi, f = e - r * ldpi;
+        const int ia = fa[f], ib = fb[f];
+        double v;
+        if (ia == -3) v = 0.0;
+        else if (ia == -2) v = ys[r];
+        else {
+          const double* xr = xs + (int64_t)r * d;
+          v = (ia < 0 ? 1.0 : xr[ia]) * (ib < 0 ? 1.0 : xr[ib]);
+        }
+        phi[r * ldpi + f] = v;
+      }
+      __syncthreads();
+      if (tid == 0 && c + 2 < nchunks) issue_chunk(a, it, CHUNK, c + 2, smem, lay, st, &bars[st]);
+      if (mine) {
+        for (int r = slice; r < rows; r += S) {
+          const double* pr = phi + r * ldpi;
+          const double qv = q[r];
+          double av[TS], bv[TS];
+#pragma unroll
+          for (int i = 0; i < TS; ++i) av[i] = pr[I * TS + i];
+#pragma unroll
+          for (int j = 0; j < TS; ++j) bv[j] = qv * pr[J * TS + j];
+#pragma unroll
+          for (int i = 0; i < TS; ++i)
+#pragma unroll
+            for (int j = 0; j < TS; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+        }
+      }
+      __syncthreads();
+    }
+    if (timed_out) {
+      if (tid == 0) {
+        atomicExch(L.err, 1);
+        a.status[k] = -5;
+      }
+      return;  // barrier phases are no longer consistent: stop this CTA
+    }
+    {
+      const int bw = __syncthreads_or(bad & 2), bx = __syncthreads_or(bad & 1);
+      bad = (bw ? 2 : 0) | (bx ? 1 : 0);
+    }
+    // deterministic slice reduction into the packed augmented Gram
+    for (int s = 0; s < S; ++s) {
+      if (mine && slice == s) {
+#pragma unroll
+        for (int i = 0; i < TS; ++i)
+#pragma unroll
+          for (int j = 0; j < TS; ++j) {
+            const int r = I * TS + i, cc = J * TS + j;
+            if (r < pa && cc <= r) {
+              double* g = &G[pk(r, cc)];
+              *g = (s == 0) ? acc[i][j] : *g + acc[i][j];
+            }
+          }
+      }
+      __syncthreads();
+    }
+    finish_fp64<TS>(a, L, k, it, G, bad, vec, &s_fail, s_scalar,
+                (cls == CLS_RESOLVE) ? ART_INFO_FP64_RESOLVE : 0u);
+  }
+}
+
+// ============================================================== QR kernel
+// FP64 Householder QR of the augmented least-squares problem
+//   [sqrt(W) Phi | sqrt(W) y ; sqrt(lambda) I | 0]
+// streamed in row chunks, keeping only R (with Q^T b as its last column);
+// the fallback of solve_weighted_ridge's auto solver (models.py:334-357,
+// _solve_augmented_ridge 374-448).  Rank-revealing pivoting (gelsy) is not
+// used: the regularised problem has full column rank whenever lambda > 0.
+constexpr int kQrChunk = 32;
+
+__host__ __device__ inline size_t qr_smem(int pmax, int dmax) {
+  const int pa = pmax + 1;
+  size_t o = 0;
+  o = align16(o + (size_t)pa * (pa + 1) / 2 * 8);   // R packed upper
+  o = align16(o + (size_t)kQrChunk * pa * 8);       // V chunk
+  o = align16(o + (size_t)kQrChunk * 8);            // reflector
+  o = align16(o + (size_t)kQrChunk * dmax * 8);     // x chunk
+  o = align16(o + (size_t)(pa + 1) * 8);            // solution
+  o = align16(o + (size_t)pa * 4);                  // factor indices
+  return o;
+}
+
+__device__ __forceinline__ int ru(int i, int j, int pa) {  // packed upper, row-major
+  return i * pa - i * (i - 1) / 2 + (j - i);
+}
+
+__global__ void __launch_bounds__(kRidgeThreads) ridge_qr_kernel(RidgeArgs a, RidgeLists L) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_item;
+  __shared__ double s_tau;
+  const int pa_max = a.pmax + 1;
+  double* R = (double*)smem;
+  double* V = (double*)(smem + align16((size_t)pa_max * (pa_max + 1) / 2 * 8));
+  double* vb = V + align16((size_t)kQrChunk * pa_max * 8) / 8;
+  double* xs = vb + align16((size_t)kQrChunk * 8) / 8;
+  double* sol = xs + align16((size_t)kQrChunk * a.dmax * 8) / 8;
+  int16_t* fidx = (int16_t*)(sol + align16((size_t)(pa_max + 1) * 8) / 8);
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int count = L.count[CLS_QR];
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(&L.cursor[CLS_QR], 1);
+    __syncthreads();
+    const int item = s_item;
+    __syncthreads();
+    if (item >= count) break;
+    const int k = L.list[(int64_t)CLS_QR * a.K + item];
+    const RidgeItem it = load_item(a, k);
+    const int p = it.p, pa = p + 1, d = it.d;
+    const double lam = L.lambda[k];
+    for (int e = tid; e < pa * (pa + 1) / 2; e += kRidgeThreads) R[e] = 0.0;
+    for (int f = tid; f < p; f += kRidgeThreads) {
+      int fa_, fb_;
+      feature_factors(d, it.kind, f, fa_, fb_);
+      fidx[2 * f] = (int16_t)fa_;
+      fidx[2 * f + 1] = (int16_t)fb_;
+    }
+    __syncthreads();
+    const int64_t n_lam = (lam > 0.0) ? p : 0;
+    const int64_t total = it.n + n_lam;
+    for (int64_t c0 = 0; c0 < total; c0 += kQrChunk) {
+      const int rows = (int)min((int64_t)kQrChunk, total - c0);
+      // build V rows
+      const int64_t data_rows = max((int64_t)0, min((int64_t)rows, it.n - c0));
+      for (int e = tid; e < data_rows * d; e += kRidgeThreads)
+        xs[e] = a.x[it.xoff + c0 * d + e];
+      __syncthreads();
+      for (int e = tid; e < rows * pa; e += kRidgeThreads) {
+        const int r = e / pa, f = e - r * pa;
+        const int64_t g = c0 + r;
+        double v;
+        if (g < it.n) {
+          double wv = a.w ? a.w[it.r0 + g] : 1.0;
+          double sw = sqrt(fmax(wv, a.weight_floor));
+          if (f == p) v = sw * a.y[it.r0 + g];
+          else {
+            const int ia = fidx[2 * f], ib = fidx[2 * f + 1];
+            const double* xr = xs + (int64_t)r * d;
+            v = sw * ((ia < 0 ? 1.0 : xr[ia]) * (ib < 0 ? 1.0 : xr[ib]));
+          }
+        } else {
+          const int64_t li = g - it.n;  // ridge row li
+          v = (f == li) ? sqrt(lam) : 0.0;
+        }
+        V[r * pa + f] = v;
+      }
+      __syncthreads();
+      for (int j = 0; j < p; ++j) {
+        if (tid < 32) {
+          double sig = 0.0;
+          for (int r = lane; r < rows; r += 32) sig += V[r * pa + j] * V[r * pa + j];
+          sig = warp_sum(sig);
+          const double x0 = R[ru(j, j, pa)];
+          double tau = 0.0, scale = 0.0, beta = x0;
+          if (sig > 0.0) {
+            const double mu = sqrt(x0 * x0 + sig);
+            beta = -copysign(mu, x0);
+            tau = (beta - x0) / beta;
+            scale = 1.0 / (x0 - beta);
+          }
+          for (int r = lane; r < rows; r += 32) vb[r] = V[r * pa + j] * scale;
+          if (lane == 0) {
+            s_tau = tau;
+            R[ru(j, j, pa)] = beta;
+          }
+        }
+        __syncthreads();
+        const double tau = s_tau;
+        if (tau != 0.0) {
+          for (int col = j + 1 + tid; col < pa; col += kRidgeThreads) {
+            double s = R[ru(j, col, pa)];
+            for (int r = 0; r < rows; ++r) s = fma(vb[r], V[r * pa + col], s);
+            s *= tau;
+            R[ru(j, col, pa)] -= s;
+            for (int r = 0; r < rows; ++r) V[r * pa + col] = fma(-s, vb[r], V[r * pa + col]);
+          }
+        }
+        __syncthreads();
+      }
+    }
+    // back substitution R beta = c, c = R[:, p]
+    if (tid < 32) {
+      for (int i = lane; i < p; i += 32) sol[i] = R[ru(i, p, pa)];
+      __syncwarp();
+      for (int j = p - 1; j >= 0; --j) {
+        if (lane == 0) sol[j] = sol[j] / R[ru(j, j, pa)];
+        __syncwarp();
+        const double bj = sol[j];
+        for (int i = lane; i < j; i += 32) sol[i] -= R[ru(i, j, pa)] * bj;
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    int nonfinite = 0;
+    for (int i = tid; i < p; i += kRidgeThreads) {
+      nonfinite |= !isfinite(sol[i]);
+      a.beta[(int64_t)k * a.beta_stride + i] = sol[i];
+    }
+    nonfinite = __syncthreads_or(nonfinite);
+    if (tid == 0) a.status[k] = nonfinite ? -3 : 0;
+    __syncthreads();
+  }
+}
+
+// ================================================================== host
+static int g_sm_count[64];
+
+int device_sm_count() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return 148;
+  if (!g_sm_count[dev]) {
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    g_sm_count[dev] = v > 0 ? v : 148;
+  }
+  return g_sm_count[dev];
+}
+
+struct WsLayout {
+  size_t off_count, off_cursor, off_hist, off_start, off_err, off_lambda, off_list, header,
+      total;
+};
+static WsLayout ws_layout(int64_t K) {
+  WsLayout w;
+  size_t o = 0;
+  w.off_count = o; o += kClasses * 4;
+  w.off_cursor = o; o += kClasses * 4;
+  w.off_hist = o; o += kPlanClasses * kBuckets * 4;
+  w.off_start = o; o += kPlanClasses * kBuckets * 4;
+  w.off_err = o; o += 16;
+  w.header = o;  // zeroed every call
+  o = (o + 255) & ~(size_t)255;
+  w.off_lambda = o; o += (size_t)K * 8;
+  o = (o + 255) & ~(size_t)255;
+  w.off_list = o; o += (size_t)kClasses * K * 4;
+  w.total = (o + 255) & ~(size_t)255;
+  return w;
+}
+
+template <typename Kern>
+static int launch_persistent(Kern kern, size_t smem, int64_t max_items, cudaStream_t s,
+                             RidgeArgs a, RidgeLists L, int cls, int pcap, const char* name) {
+  if (smem > 227 * 1024) {
+    set_error("%s: shared memory %zu bytes exceeds the 227 KB limit", name, smem);
+    return ART_E_UNSUPPORTED;
+  }
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kRidgeThreads, smem);
+  if (occ < 1) occ = 1;
+  int64_t grid = (int64_t)device_sm_count() * occ;
+  if (grid > max_items) grid = max_items;
+  if (grid < 1) grid = 1;
+  prof_begin(name, s);
+  kern<<<(unsigned)grid, kRidgeThreads, smem, s>>>(a, L, cls, pcap);
+  prof_end(s);
+  count_launch();
+  return check_launch(name);
+}
+
+}  // namespace art
+
+using namespace art;
+
+extern "C" size_t art_ridge_workspace_size(int64_t count, int32_t max_features) {
+  (void)max_features;
+  if (count < 0) return 0;
+  return ws_layout(count).total;
+}
+
+extern "C" int art_ridge_batched(const ArtRidgeProblem* pr, const ArtRidgeResult* res,
+                                 void* workspace, size_t ws_bytes, art_stream_t stream) {
+  if (!pr || !res) { set_error("art_ridge_batched: null problem/result"); return ART_E_INVALID; }
+  const int64_t K = pr->seg.count;
+  if (K < 0) { set_error("art_ridge_batched: negative count"); return ART_E_INVALID; }
+  if (K == 0) return ART_OK;
+  if (!pr->seg.row_offsets || !pr->seg.x_offsets || !pr->seg.dims || !pr->seg.features ||
+      !pr->x || !pr->y || !pr->ridge || !res->beta || !res->status) {
+    set_error("art_ridge_batched: null device pointer");
+    return ART_E_INVALID;
+  }
+  if (pr->max_features < 1 || pr->max_features > ART_MAX_FEATURES) {
+    set_error("art_ridge_batched: max_features %d outside [1, %d]", pr->max_features,
+              ART_MAX_FEATURES);
+    return ART_E_UNSUPPORTED;
+  }
+  if (res->beta_stride < pr->max_features) {
+    set_error("art_ridge_batched: beta_stride %lld < max_features %d",
+              (long long)res->beta_stride, pr->max_features);
+    return ART_E_INVALID;
+  }
+  if (pr->solver != ART_SOLVER_NORMAL && pr->solver != ART_SOLVER_AUTO &&
+      pr->solver != ART_SOLVER_QR) {
+    set_error("art_ridge_batched: unknown solver %d", pr->solver);
+    return ART_E_INVALID;
+  }
+  if (pr->precision != ART_PRECISION_FP64 && pr->precision != ART_PRECISION_MIXED) {
+    set_error("art_ridge_batched: unknown precision %d", pr->precision);
+    return ART_E_INVALID;
+  }
+  if (!(pr->auto_rcond_threshold > 0.0 && pr->auto_rcond_threshold <= 1.0)) {
+    set_error("auto_rcond_threshold must satisfy 0 < value <= 1.");
+    return ART_E_INVALID;
+  }
+  if (!(pr->weight_floor >= 0.0)) {
+    set_error("art_ridge_batched: weight_floor must be nonnegative");
+    return ART_E_INVALID;
+  }
+  const WsLayout wl = ws_layout(K);
+  if (!workspace || ws_bytes < wl.total) {
+    set_error("art_ridge_batched: workspace %zu bytes < required %zu", ws_bytes, wl.total);
+    return ART_E_WORKSPACE;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned char* ws = (unsigned char*)workspace;
+  RidgeArgs a;
+  a.K = K;
+  a.row_offsets = pr->seg.row_offsets;
+  a.x_offsets = pr->seg.x_offsets;
+  a.dims = pr->seg.dims;
+  a.features = pr->seg.features;
+  a.x = pr->x; a.y = pr->y; a.w = pr->w; a.ridge = pr->ridge;
+  a.weight_floor = pr->weight_floor;
+  a.solver = pr->solver;
+  a.precision = pr->precision;
+  a.rcond_threshold = pr->auto_rcond_threshold;
+  a.pmax = pr->max_features;
+  a.dmax = pr->max_dim > 0 ? std::min(pr->max_dim, pr->max_features) : pr->max_features;
+  if (a.dmax > ART_MAX_FEATURES) a.dmax = ART_MAX_FEATURES;
+  a.beta = res->beta; a.beta_stride = res->beta_stride;
+  a.ridge_eff = res->ridge_effective; a.cond = res->cond_estimate;
+  a.status = res->status; a.info = res->info;
+  RidgeLists L;
+  L.count = (int32_t*)(ws + wl.off_count);
+  L.cursor = (int32_t*)(ws + wl.off_cursor);
+  L.hist = (int32_t*)(ws + wl.off_hist);
+  L.start = (int32_t*)(ws + wl.off_start);
+  L.err = (int32_t*)(ws + wl.off_err);
+  L.lambda = (double*)(ws + wl.off_lambda);
+  L.list = (int32_t*)(ws + wl.off_list);
+  if (cudaMemsetAsync(ws, 0, wl.header, s) != cudaSuccess) return check_launch("memset");
+  const unsigned pg = (unsigned)((K + 255) / 256);
+  prof_begin("ridge_plan", s);
+  ridge_plan_hist<<<pg, 256, 0, s>>>(a, L);
+  ridge_plan_scan<<<1, 32 * kPlanClasses, 0, s>>>(L);
+  ridge_plan_scatter<<<pg, 256, 0, s>>>(a, L);
+  prof_end(s);
+  count_launch();
+  count_launch();
+  count_launch();
+  int rc = check_launch("ridge plan");
+  if (rc) return rc;
+  if (a.precision == ART_PRECISION_MIXED) {
+    rc = launch_ridge_tensor(a, L, s);
+    if (rc) return rc;
+  }
+  {
+    const int pcap = std::min(a.pmax, kSmallMaxAug - 1);
+    const size_t sm = fp64_layout(pcap, a.dmax, 4, 64).total;
+    rc = launch_persistent(ridge_fp64_kernel<4, 64>, sm, K, s, a, L, CLS_SMALL, pcap,
+                           "ridge_fp64<4>");
+    if (rc) return rc;
+  }
+  if (a.pmax + 1 > kSmallMaxAug || a.precision == ART_PRECISION_MIXED) {
+    const size_t sm = fp64_layout(a.pmax, a.dmax, 8, 32).total;
+    rc = launch_persistent(ridge_fp64_kernel<8, 32>, sm, K, s, a, L, CLS_LARGE, a.pmax,
+                           "ridge_fp64<8>");
+    if (rc) return rc;
+    if (a.precision == ART_PRECISION_MIXED) {
+      rc = launch_persistent(ridge_fp64_kernel<8, 32>, sm, K, s, a, L, CLS_RESOLVE, a.pmax,
+                             "ridge_fp64<8> resolve");
+      if (rc) return rc;
+    }
+  }
+  if (a.solver == ART_SOLVER_AUTO || a.solver == ART_SOLVER_QR) {
+    const size_t sm = qr_smem(a.pmax, a.dmax);
+    if (sm > 227 * 1024) {
+      set_error("ridge_qr: shared memory %zu bytes exceeds the 227 KB limit", sm);
+      return ART_E_UNSUPPORTED;
+    }
+    cudaFuncSetAttribute(ridge_qr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    int64_t grid = std::min<int64_t>(K, device_sm_count());
+    prof_begin("ridge_qr", s);
+    ridge_qr_kernel<<<(unsigned)grid, kRidgeThreads, sm, s>>>(a, L);
+    prof_end(s);
+    count_launch();
+    rc = check_launch("ridge_qr");
+    if (rc) return rc;
+  }
+  return ART_OK;
+}

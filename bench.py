@@ -1,0 +1,437 @@
+#!/usr/bin/env python
+"""Benchmark of the ART hot path on B200: batched weighted ridge solves.
+
+Workload (one step): 65,536 independent weighted ridge systems, n_k
+log-uniform in [64, 8192] (about 110M rows), x uniform on [-1,1]^d with
+d in {8, 16}, affine or full quadratic features (p = 9, 17, 45, 153; a
+quarter each), weights = products of 1-8 sigmoids, noisy random quadratic
+y, ridge log-uniform in [1e-8, 1e-2]; seeded synthetic data generated on the
+device.  The inputs (~12 GB) are larger than L2, so no flush is needed
+between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun each rank solves its own 65,536-system batch (weak scaling, no
+data-path collective); rank 0 prints one JSON line with the max-over-ranks
+device time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "adaptive-regression-trees-art-_b200"))
+sys.path.insert(0, str(ROOT))
+
+METRIC = "ridge solves/s"
+UNIT = "solves/s"
+WORKLOAD = ("batched weighted ridge: 65,536 systems/GPU, n log-uniform [64, 8192], d in {8,16}, "
+            "affine or quadratic features (p = 9/17/45/153), sigmoid-product weights, "
+            "ridge log-uniform [1e-8, 1e-2], solver normal")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--systems", type=int, default=65536)
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--cpu-per-class", type=int, default=48,
+                    help="systems per feature class in the timed CPU sample")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ helpers
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"art_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in self.path.read_text().splitlines():
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 8:
+                    rows.append(parts)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        smax = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def gpu_id_for(device_index: int) -> str:
+    import torch
+
+    try:
+        uuid = str(torch.cuda.get_device_properties(device_index).uuid)
+        return uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+    except Exception:
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        return vis.split(",")[device_index] if vis else str(device_index)
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def algorithmic(wl, idx=None):
+    """SURVEY 8(d) formulas: F = n p(p+1) + 2np + p^3/3 + 2p^2 ; B = n (d+2) 8 + 8p."""
+
+    from art.models import kind_feature_count
+
+    n = np.diff(wl.row_offsets).astype(float)
+    d = wl.dims.astype(float)
+    p = np.array([kind_feature_count(int(a), int(b)) for a, b in zip(wl.dims, wl.kinds)], float)
+    if idx is not None:
+        n, d, p = n[idx], d[idx], p[idx]
+    flops = n * p * (p + 1) + 2 * n * p + p ** 3 / 3 + 2 * p ** 2
+    nbytes = n * (d + 2) * 8 + 8 * p
+    return float(flops.sum()), float(nbytes.sum())
+
+
+def stratified_sample(wl, per_class: int, seed: int = 0):
+    """Systems evenly spaced in n within each (d, kind) class."""
+
+    idx = []
+    n = np.diff(wl.row_offsets)
+    for key in sorted(set(zip(wl.dims.tolist(), wl.kinds.tolist()))):
+        members = np.flatnonzero((wl.dims == key[0]) & (wl.kinds == key[1]))
+        order = members[np.argsort(n[members], kind="stable")]
+        take = np.linspace(0, order.size - 1, min(per_class, order.size)).round().astype(int)
+        idx.append(order[take])
+    return np.concatenate(idx)
+
+
+def cpu_solve_rate(wl, per_class, repeats: int = 1, mix=None):
+    """Time the oracle (reference CPU algorithm) on a stratified sample; scale to the mix.
+
+    ``per_class=None`` means ``wl`` already is the sample and ``mix`` holds
+    the class counts of the full workload.
+    """
+
+    from oracle import ridge as O
+    from threadpoolctl import threadpool_limits
+
+    cores = len(os.sched_getaffinity(0))
+    if per_class is None:
+        sample = np.arange(wl.count)
+        sub = wl
+    else:
+        sample = stratified_sample(wl, per_class)
+        sub = wl.subset(sample)
+        mix = {key: int(np.sum((wl.dims == key[0]) & (wl.kinds == key[1])))
+               for key in set(zip(wl.dims.tolist(), wl.kinds.tolist()))}
+    per_class_time = {}
+    t_all = 0.0
+    with threadpool_limits(limits=cores):
+        for _ in range(repeats):
+            for k in range(sub.count):
+                r0, r1 = sub.row_offsets[k], sub.row_offsets[k + 1]
+                d = int(sub.dims[k])
+                X = sub.x[sub.x_offsets[k]: sub.x_offsets[k] + (r1 - r0) * d].reshape(-1, d)
+                t0 = time.perf_counter()
+                phi = O.features(X, int(sub.kinds[k]))
+                try:
+                    O.solve_weighted_ridge(phi, sub.y[r0:r1], sub.w[r0:r1], float(sub.ridge[k]), solver="normal")
+                except np.linalg.LinAlgError:
+                    pass
+                dt = time.perf_counter() - t0
+                key = (int(sub.dims[k]), int(sub.kinds[k]))
+                per_class_time.setdefault(key, []).append(dt)
+                t_all += dt
+    est = 0.0
+    total = 0
+    for key, ts in per_class_time.items():
+        est += mix[key] * float(np.mean(ts))
+        total += mix[key]
+    rate = total / est
+    return rate, cores, sample.size, t_all
+
+
+# ------------------------------------------------------------------ arms
+def run_reference(args):
+    """--impl reference: the reference CPU algorithm (oracle port) on the host cores."""
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    wl, mix = _cpu_workload(args.systems, args.cpu_per_class)
+    times = []
+    for i in range(args.warmup + args.steps):
+        rate, cores, sample, _ = cpu_solve_rate(wl, None, mix=mix)
+        if i >= args.warmup:
+            times.append(rate)
+    value = float(np.median(times))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * args.systems / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": WORKLOAD, "systems": args.systems, "solver": "normal"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{sample} systems stratified by n in each of 4 feature classes, scaled to the mix"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def _cpu_workload(systems, per_class):
+    """The stratified sample of the benchmark's systems with numpy-drawn rows.
+
+    Per-system parameters (n, d, features, ridge, weights, target) are the
+    device workload's own; only the row values come from numpy.  Returns the
+    sample and the class counts of the full mix.
+    """
+
+    from art import workloads
+
+    meta = workloads.ridge_systems(systems, seed=2, device=None, only=[])
+    full = _Meta(meta)
+    sample = stratified_sample(full, per_class)
+    wl = workloads.ridge_systems(systems, seed=2, device=None, only=sample)
+    return wl, full.class_counts()
+
+
+class _Meta:
+    """Per-system sizes of the full mix without rows."""
+
+    def __init__(self, empty_wl):
+        from art import workloads
+
+        rng_meta = workloads.ridge_meta(empty_wl)
+        self.row_offsets, self.dims, self.kinds = rng_meta
+
+    @property
+    def count(self):
+        return int(self.dims.shape[0])
+
+    def class_counts(self):
+        keys, counts = np.unique(np.stack([self.dims, self.kinds], 1), axis=0, return_counts=True)
+        return {(int(a), int(b)): int(c) for (a, b), c in zip(keys, counts)}
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    from art import _native as N
+    from art import workloads
+    from art.models import solve_weighted_ridge_batched
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    N.load_library()
+    wl = workloads.ridge_systems(args.systems, seed=2 + rank, device="cuda")
+    ro = torch.from_numpy(wl.row_offsets).to(dev)
+    xo = torch.from_numpy(wl.x_offsets).to(dev)
+    dims = torch.from_numpy(wl.dims).to(dev)
+    kinds = torch.from_numpy(wl.kinds).to(dev)
+    ridge = torch.from_numpy(wl.ridge).to(dev)
+    stream = torch.cuda.current_stream()
+
+    def solve(precision, out=None):
+        return solve_weighted_ridge_batched(
+            wl.x, wl.y, wl.w, ro, dims, kinds, ridge, x_offsets=xo, precision=precision,
+            max_features=wl.max_features, max_dim=wl.max_dim, out=out)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(precision):
+        out = None
+        for _ in range(args.warmup):
+            out = solve(precision, out)
+        barrier()
+        N.profile_reset()
+        N.profile_enable(True)
+        launches0 = N.launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            out = solve(precision, out)
+        e1.record(stream)
+        barrier()
+        N.profile_enable(False)
+        ms = e0.elapsed_time(e1)
+        launches = N.launch_count() - launches0
+        prof = N.profile_report()
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms / args.steps, launches // args.steps, prof, out
+
+    # plain FP64 form (the >=5x comparison point), then the headline form
+    plain_ms, _, plain_prof, plain_out = timed("fp64")
+    with Clocks(gpu_id_for(local)) as clocks:
+        ms, launches, prof, out = timed(args.precision)
+    clk = clocks.summary()
+    status = out.status.cpu().numpy()
+    info = out.info.cpu().numpy()
+    value = world * args.systems / (ms / 1000.0)
+
+    # roofline of the dominant kernel
+    hbm, bf16, peak_kind = peaks()
+    top = max(prof.items(), key=lambda kv: kv[1][1])
+    name, (n_launch, total_ms) = top
+    per_launch_ms = total_ms / max(n_launch, 1)
+    from art.models import kind_feature_count
+
+    p_all = np.array([kind_feature_count(int(a), int(b)) for a, b in zip(wl.dims, wl.kinds)])
+    if "fp64<4>" in name:
+        cls_idx = np.flatnonzero(p_all + 1 <= 48)
+    elif "fp64<8>" in name:
+        cls_idx = np.flatnonzero(p_all + 1 > 48) if args.precision == "fp64" else np.flatnonzero(info & N.INFO_FP64_RESOLVE)
+    else:
+        cls_idx = np.flatnonzero(p_all >= 33)
+    flops, nbytes = algorithmic(wl, cls_idx)
+    achieved_gbs = nbytes / (per_launch_ms / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "kernel": name, "achieved": achieved_gbs, "peak": hbm,
+                "unit": "GB/s", "frac": achieved_gbs / hbm, "traffic": None,
+                "peak_source": peak_kind,
+                "achieved_tflops": flops / (per_launch_ms / 1000.0) / 1e12,
+                "launch_ms": per_launch_ms, "kernel_share": total_ms / sum(v[1] for v in prof.values())}
+
+    # end-to-end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        hx = torch.empty(wl.x.shape, dtype=torch.float64, pin_memory=True)
+        hy = torch.empty(wl.y.shape, dtype=torch.float64, pin_memory=True)
+        hw = torch.empty(wl.w.shape, dtype=torch.float64, pin_memory=True)
+        hx.copy_(wl.x); hy.copy_(wl.y); hw.copy_(wl.w)
+        meta = [torch.from_numpy(a).pin_memory() for a in (wl.row_offsets, wl.x_offsets, wl.dims, wl.kinds, wl.ridge)]
+        hbeta = torch.empty((args.systems, wl.max_features), dtype=torch.float64, pin_memory=True)
+        hstat = torch.empty(args.systems, dtype=torch.int32, pin_memory=True)
+
+        def e2e_step():
+            o = solve_weighted_ridge_batched(hx, hy, hw, meta[0], meta[2], meta[3], meta[4], x_offsets=meta[1],
+                                             precision=args.precision, max_features=wl.max_features,
+                                             max_dim=wl.max_dim)
+            hbeta.copy_(o.beta, non_blocking=True)
+            hstat.copy_(o.status, non_blocking=True)
+
+        for _ in range(max(1, args.warmup // 2)):
+            e2e_step()
+        barrier()
+        t0 = time.perf_counter()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        e1.record(stream)
+        barrier()
+        e2e_ms = max(e0.elapsed_time(e1), 1000.0 * (time.perf_counter() - t0)) / args.steps
+        if world > 1:
+            t = torch.tensor([e2e_ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        h2d = sum(int(t.numel() * t.element_size()) for t in (hx, hy, hw, *meta))
+        d2h = int(hbeta.numel() * 8 + hstat.numel() * 4)
+        e2e = {"value": world * args.systems / (e2e_ms / 1000.0), "unit": UNIT,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms}
+        del hx, hy, hw
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        # the same systems the GPU solved: a stratified sample copied to the host
+        sample_idx = stratified_sample(wl, args.cpu_per_class)
+        mix = {key: int(np.sum((wl.dims == key[0]) & (wl.kinds == key[1])))
+               for key in set(zip(wl.dims.tolist(), wl.kinds.tolist()))}
+        rate, cores, sample, secs = cpu_solve_rate(wl.subset(sample_idx), None, mix=mix)
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{sample} systems stratified by n over the 4 feature classes "
+                         f"({secs:.1f} s of CPU work), scaled to the 65,536-system mix"}
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    ok = float(np.mean(status == 0))
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16x3+f32+f64" if args.precision == "mixed" else "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "systems_per_gpu": args.systems, "precision": args.precision,
+                   "rows_per_gpu": wl.n_rows, "l2": "inputs (~12 GB) larger than L2; no flush",
+                   "parallelism": f"replicas x{world}"},
+        "gpu_launches": int(launches),
+        "roofline": roofline,
+        "plain_fp64": {"ms_per_step": plain_ms, "value": world * args.systems / (plain_ms / 1000.0),
+                       "speedup_of_headline": plain_ms / ms},
+        "status_ok_fraction": ok,
+        "fp64_resolve_fraction": float(np.mean((info & N.INFO_FP64_RESOLVE) != 0)),
+        "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()},
+        "clocks": clk,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,171 @@
+"""Batched weighted ridge on the GPU vs the oracle and the reference's golden outputs.
+
+Tolerance (FP64 plain form): relative coefficient error
+    ||beta - beta_ref|| / ||beta_ref|| <= max(1e-10, 1e-14 * cond)
+where cond is the 2-norm condition number of G + lambda I: two FP64 solvers
+with different summation orders agree to about cond * 1e-16, so a fixed 1e-10
+holds for every system with cond <= 1e4 and the bound grows with cond above.
+"""
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, gpu_available
+from oracle import ridge as O
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not gpu_available(), reason="needs a CUDA device")]
+
+
+def rel_err(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def cond_of(phi, w, lam_rel, floor=1e-12):
+    sw = np.maximum(w, floor)
+    G = phi.T @ (phi * sw[:, None])
+    lam = lam_rel * np.trace(G) / G.shape[0]
+    return float(np.linalg.cond(G + lam * np.eye(G.shape[0])))
+
+
+def tol_for(cond):
+    return max(1e-10, 1e-14 * cond)
+
+
+def golden_cases():
+    g = np.load(GOLDEN / "ridge_golden.npz")
+    for i in range(int(g["count"])):
+        kind, lam, solver = g[f"c{i}_meta"]
+        yield dict(X=g[f"c{i}_X"], y=g[f"c{i}_y"], w=g[f"c{i}_w"], kind=int(kind), ridge=float(lam),
+                   solver=("normal", "auto")[int(solver)], beta=g[f"c{i}_beta"],
+                   ridge_eff=float(g[f"c{i}_ridge_eff"]), solver_used=str(g[f"c{i}_solver_used"]))
+
+
+@pytest.mark.parametrize("case", list(golden_cases()), ids=lambda c: f"{c['solver']}-k{c['kind']}-n{len(c['y'])}")
+def test_single_solves_match_reference_golden(case):
+    from art import models
+
+    res = models._solve_single(case["X"], case["y"], case["w"], case["ridge"], case["kind"],
+                               weight_floor=1e-12, solver=case["solver"], auto_rcond_threshold=1e-10)
+    phi = O.features(case["X"], case["kind"])
+    c = cond_of(phi, case["w"], case["ridge"])
+    assert rel_err(res.coefficients, case["beta"]) <= tol_for(c)
+    assert res.ridge_effective == pytest.approx(case["ridge_eff"], rel=1e-12, abs=1e-300)
+    assert res.solver_used == case["solver_used"]
+
+
+def make_batch(K=96, seed=7, n_max=700):
+    from art import workloads
+
+    return workloads.ridge_systems(K, seed=seed, n_min=1, n_max=n_max)
+
+
+@pytest.mark.parametrize("solver", ["normal", "auto"])
+def test_batched_fp64_matches_oracle_on_mixed_segments(solver):
+    from art.models import solve_weighted_ridge_batched
+
+    wl = make_batch()
+    out = solve_weighted_ridge_batched(wl.x, wl.y, wl.w, wl.row_offsets, wl.dims, wl.kinds, wl.ridge,
+                                       x_offsets=wl.x_offsets, solver=solver, precision="fp64",
+                                       max_features=wl.max_features, max_dim=wl.max_dim)
+    beta = out.beta.cpu().numpy()
+    status = out.status.cpu().numpy()
+    lam = out.ridge_effective.cpu().numpy()
+    for k in range(wl.count):
+        r0, r1 = wl.row_offsets[k], wl.row_offsets[k + 1]
+        d = int(wl.dims[k])
+        X = wl.x[wl.x_offsets[k]: wl.x_offsets[k] + (r1 - r0) * d].reshape(-1, d)
+        phi = O.features(X, int(wl.kinds[k]))
+        p = phi.shape[1]
+        try:
+            ref = O.solve_weighted_ridge(phi, wl.y[r0:r1], wl.w[r0:r1], wl.ridge[k], solver=solver)
+        except np.linalg.LinAlgError:
+            assert status[k] > 0
+            continue
+        assert status[k] == 0, (k, status[k])
+        assert lam[k] == pytest.approx(ref["ridge_effective"], rel=1e-12)
+        c = cond_of(phi, wl.w[r0:r1], wl.ridge[k])
+        assert rel_err(beta[k, :p], ref["coefficients"]) <= tol_for(c), (k, c)
+
+
+def test_batched_is_deterministic_and_ordering_independent():
+    import torch
+
+    from art.models import solve_weighted_ridge_batched
+
+    wl = make_batch(K=40, seed=11)
+    a = solve_weighted_ridge_batched(wl.x, wl.y, wl.w, wl.row_offsets, wl.dims, wl.kinds, wl.ridge,
+                                     x_offsets=wl.x_offsets, max_features=wl.max_features, max_dim=wl.max_dim)
+    b = solve_weighted_ridge_batched(wl.x, wl.y, wl.w, wl.row_offsets, wl.dims, wl.kinds, wl.ridge,
+                                     x_offsets=wl.x_offsets, max_features=wl.max_features, max_dim=wl.max_dim)
+    assert torch.equal(a.beta, b.beta)
+    # a system solved alone equals the same system inside the batch
+    sub = wl.subset([5])
+    c = solve_weighted_ridge_batched(sub.x, sub.y, sub.w, sub.row_offsets, sub.dims, sub.kinds, sub.ridge,
+                                     x_offsets=sub.x_offsets, max_features=wl.max_features, max_dim=wl.max_dim)
+    p = c.beta.shape[1]
+    np.testing.assert_array_equal(c.beta.cpu().numpy()[0], a.beta.cpu().numpy()[5, :p])
+
+
+def test_edge_cases_status_codes():
+    from art.models import solve_weighted_ridge_batched
+
+    rng = np.random.default_rng(5)
+    # systems: empty, one row, NaN x, negative weight, singular (ridge 0), unsupported d
+    d = 3
+    n = [0, 1, 10, 10, 10, 10]
+    X = rng.uniform(-1, 1, (sum(n), d))
+    X[1 + 2] = np.nan  # first row of system 2
+    y = rng.normal(size=sum(n))
+    w = np.ones(sum(n))
+    w[1 + 10 + 4] = -1.0  # system 3
+    X[21:31, 1] = 0.0    # system 4: zero column, ridge 0 -> singular
+    ro = np.concatenate([[0], np.cumsum(n)])
+    dims = np.array([d, d, d, d, d, 99])
+    kinds = np.zeros(6, dtype=np.int32)
+    ridge = np.array([1e-3, 1e-3, 1e-3, 1e-3, 0.0, 1e-3])
+    xo = ro[:-1] * d
+    out = solve_weighted_ridge_batched(X.reshape(-1), y, w, ro, dims, kinds, ridge, x_offsets=xo,
+                                       max_features=4, max_dim=d)
+    st = out.status.cpu().numpy()
+    assert st[0] == 1          # empty: G = 0, lambda = 0 -> first pivot fails
+    assert st[1] in (0, 2)     # one row, rank 1 + ridge: pivot 2 may still be tiny but positive
+    assert st[2] == -2         # non-finite x
+    assert st[3] == -1         # negative weight
+    assert st[4] == 2          # zero second column, no ridge
+    assert st[5] == -4         # d outside the compiled limit
+    beta = out.beta.cpu().numpy()
+    assert np.isnan(beta[2]).all() and np.isnan(beta[4]).all()
+
+
+def test_auto_solver_qr_fallback_reports_info_bits():
+    from art import _native as N
+    from art.models import solve_weighted_ridge_batched
+
+    rng = np.random.default_rng(16)
+    base = rng.normal(size=120)
+    X = np.column_stack([base, base + 1e-7 * rng.normal(size=120), rng.normal(size=120)])
+    y = rng.normal(size=120)
+    out = solve_weighted_ridge_batched(X.reshape(-1), y, None, [0, 120], [3], [N.FEATURES_POLY1_NOBIAS],
+                                       [0.0], solver="auto", max_features=3, max_dim=3)
+    info = int(out.info.cpu().numpy()[0])
+    assert info & N.INFO_QR_FALLBACK
+    ref = O.solve_weighted_ridge(X, y, np.ones(120), 0.0, solver="auto")
+    assert ref["solver_used"] == "qr"
+    c = np.linalg.cond(X.T @ X)
+    assert rel_err(out.beta.cpu().numpy()[0], ref["coefficients"]) <= max(1e-10, 1e-14 * c)
+
+
+def test_models_fit_on_gpu_match_oracle():
+    from art import AffineRidgeModel, PolynomialRidgeModel
+
+    rng = np.random.default_rng(21)
+    X = rng.uniform(-1, 1, (300, 4))
+    y = np.cos(X[:, 0]) + X[:, 1] * X[:, 2]
+    w = rng.uniform(0.1, 1, 300)
+    m = AffineRidgeModel(ridge=1e-6).fit_weighted(X, y, w)
+    ref = O.solve_weighted_ridge(O.features(X, O.AFFINE), y, w, 1e-6)
+    assert rel_err(m.coef_, ref["coefficients"]) < 1e-11
+    pm = PolynomialRidgeModel(degree=2, ridge=1e-8).fit(X, y)
+    ref = O.solve_weighted_ridge(O.features(X, O.POLY2), y, np.ones(300), 1e-8)
+    assert rel_err(pm.coef_, ref["coefficients"]) < 1e-9
+    np.testing.assert_allclose(pm.predict(X), O.features(X, O.POLY2) @ ref["coefficients"], rtol=1e-8, atol=1e-9)
