@@ -282,7 +282,7 @@ def solve_weighted_ridge_batched(
     if out is None:
         stride = int(max_features)
         out = BatchedRidgeResult(
-            beta=t.empty((K, stride), dtype=t.float64, device=dev),
+            beta=t.full((K, stride), float("nan"), dtype=t.float64, device=dev),
             ridge_effective=t.empty(K, dtype=t.float64, device=dev),
             cond_estimate=t.empty(K, dtype=t.float64, device=dev) if (condition or solver == "auto") else None,
             status=t.empty(K, dtype=t.int32, device=dev),

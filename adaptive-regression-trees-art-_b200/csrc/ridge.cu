@@ -222,31 +222,35 @@ __global__ void __launch_bounds__(kRidgeThreads) ridge_fp64_kernel(RidgeArgs a, 
         bad |= isfinite(ys[r]) ? 0 : 1;
         double wv = ws ? ws[r] : 1.0;
         if (!(wv >= 0.0) || !isfinite(wv)) bad |= 2;
-        q[r] = fmax(wv, a.weight_floor);
+        q[r] = sqrt(fmax(wv, a.weight_floor));
       }
-      for (int e = tid; e < rows * ldpi; e += kRidgeThreads) {
-        const int r = e / ldpi, f = e - r * ldpi;
-        const int ia = fa[f], ib = fb[f];
-        double v;
-        if (ia == -3) v = 0.0;
-        else if (ia == -2) v = ys[r];
-        else {
-          const double* xr = xs + (int64_t)r * d;
-          v = (ia < 0 ? 1.0 : xr[ia]) * (ib < 0 ? 1.0 : xr[ib]);
+      __syncthreads();
+      // phi[r][blk*TS + (j + blk) % TS] = sqrt(q_r) * feature(blk*TS + j): the
+      // per-block rotation spreads the lanes' loads over distinct banks.
+      const int warp = tid >> 5, lane = tid & 31;
+      for (int r = warp; r < rows; r += kRidgeThreads / 32) {
+        const double* xr = xs + (int64_t)r * d;
+        const double sq = q[r];
+        for (int f = lane; f < ldpi; f += 32) {
+          const int ia = fa[f], ib = fb[f];
+          double v;
+          if (ia == -3) v = 0.0;
+          else if (ia == -2) v = sq * ys[r];
+          else v = sq * ((ia < 0 ? 1.0 : xr[ia]) * (ib < 0 ? 1.0 : xr[ib]));
+          const int blk = f / TS, j = f - blk * TS;
+          phi[r * ldpi + blk * TS + ((j + blk) & (TS - 1))] = v;
         }
-        phi[r * ldpi + f] = v;
       }
       __syncthreads();
       if (tid == 0 && c + 2 < nchunks) issue_chunk(a, it, CHUNK, c + 2, smem, lay, st, &bars[st]);
       if (mine) {
         for (int r = slice; r < rows; r += S) {
           const double* pr = phi + r * ldpi;
-          const double qv = q[r];
           double av[TS], bv[TS];
 #pragma unroll
-          for (int i = 0; i < TS; ++i) av[i] = pr[I * TS + i];
+          for (int i = 0; i < TS; ++i) av[i] = pr[I * TS + ((i + I) & (TS - 1))];
 #pragma unroll
-          for (int j = 0; j < TS; ++j) bv[j] = qv * pr[J * TS + j];
+          for (int j = 0; j < TS; ++j) bv[j] = pr[J * TS + ((j + J) & (TS - 1))];
 #pragma unroll
           for (int i = 0; i < TS; ++i)
 #pragma unroll
@@ -551,6 +555,9 @@ extern "C" int art_ridge_batched(const ArtRidgeProblem* pr, const ArtRidgeResult
   a.weight_floor = pr->weight_floor;
   a.solver = pr->solver;
   a.precision = pr->precision;
+  // The tensor-core form stages rows of at most ART_MAX_DIM inputs; wider
+  // explicit designs are solved by the FP64 form.
+  if (a.precision == ART_PRECISION_MIXED && pr->max_dim > ART_MAX_DIM) a.precision = ART_PRECISION_FP64;
   a.rcond_threshold = pr->auto_rcond_threshold;
   a.pmax = pr->max_features;
   a.dmax = pr->max_dim > 0 ? std::min(pr->max_dim, pr->max_features) : pr->max_features;

@@ -1,9 +1,580 @@
-// ridge_tc.cu -- mixed-precision (tcgen05) ridge path.  Placeholder until the
-// tensor-core kernel lands: the mixed form is rejected explicitly.
+// ridge_tc.cu -- mixed-precision weighted ridge on the 5th-generation tensor
+// cores (sm_100a tcgen05), for systems with 33 <= p <= 160 features.
+//
+// Per system (one CTA, persistent work queue over the CLS_TENSOR list):
+//  1. Rows stream into shared memory by 1-D bulk copies (2 stages of 32 rows).
+//     256 threads generate v = sqrt(q) * phi(x) for every feature and row,
+//     split it into BF16 hi + lo parts and store both in the K-major
+//     core-matrix layout (8 rows x 16 bytes per core matrix, no swizzle).
+//     The same threads accumulate the exact FP64 h = Phi^T (q y) and
+//     diag(G) = sum q phi^2 (for the trace-scaled ridge, models.py:271).
+//  2. One thread issues tcgen05.mma kind::f16 (BF16 x BF16 -> FP32 in TMEM):
+//     G' = Hi Hi^T + Hi Lo^T + Lo Hi^T with M = 128 feature rows per tile
+//     (tile 1: features 0..127 x 0..P16-1; tile 2 covers features >= 128),
+//     committed to an mbarrier per stage so operand buffers recycle.
+//  3. The FP32 Gram is drained from TMEM (tcgen05.ld 32x32b), its diagonal
+//     replaced by the exact FP64 diag + lambda, and factored by an FP32
+//     Cholesky.
+//  4. FP64 iterative refinement: r = h - (G + lambda I) beta with G beta
+//     recomputed from the rows in FP64 each pass, delta = M^{-1} r with the
+//     FP32 factor, until the step is below 1e-12 of beta and has stopped
+//     shrinking.  Systems that fail the FP32 factorisation, stall, or carry
+//     bad inputs are appended to the FP64 resolve list.
+// Every wait on an mbarrier is bounded; TMEM is allocated once per CTA and
+// always released before the CTA exits.
+#include <algorithm>
+
+#include <cuda_bf16.h>
+
 #include "ridge.cuh"
+
 namespace art {
-int launch_ridge_tensor(const RidgeArgs&, const RidgeLists&, cudaStream_t) {
-  set_error("art_ridge_batched: the mixed-precision form is not built yet");
-  return ART_E_UNSUPPORTED;
+namespace {
+
+constexpr int kTcThreads = 256;
+constexpr int kKC = 32;                    // data rows per stage (MMA K per stage)
+constexpr int kPmax = 160;
+constexpr int kGroups = kPmax / 8;         // 8-feature core-matrix groups
+constexpr int kLBO = 128;                  // bytes between K-adjacent core matrices
+constexpr int kSBO = (kKC / 8) * 128;      // bytes between 8-feature groups
+constexpr int kOpBytes = kGroups * kSBO;   // one operand array (hi or lo)
+constexpr int kMaxRefine = 10;
+
+// ------------------------------------------------------------- PTX wrappers
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                   smem_u32(dst)),
+               "r"(ncols)
+               : "memory");
 }
+__device__ __forceinline__ void tmem_relinquish() {
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                         uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(bar))
+      : "memory");
+}
+// 32 lanes x 16 consecutive 32-bit columns; waits for completion.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Shared-memory matrix descriptor: K-major, no swizzle (layout type 0),
+// LBO = K-direction core-matrix stride, SBO = 8-row group stride, version 1.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)(kLBO >> 4) << 16) |
+         ((uint64_t)(kSBO >> 4) << 32) | (1ull << 46);
+}
+// Instruction descriptor, kind::f16: D = F32, A = B = BF16, both K-major.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
+}
+
+// ------------------------------------------------------------- smem layout
+struct TcLayout {
+  size_t x[2], y[2], w[2], q, sq, op, bars, tmem, gram, vec, fidx, total;
+};
+__host__ __device__ inline size_t a16(size_t v) { return (v + 15) & ~(size_t)15; }
+__host__ __device__ inline TcLayout tc_layout(int pmax, int dmax) {
+  TcLayout L;
+  size_t o = 0;
+  for (int s = 0; s < 2; ++s) {
+    L.x[s] = o; o = a16(o + (size_t)kKC * dmax * 8 + 16);
+    L.y[s] = o; o = a16(o + (size_t)kKC * 8 + 16);
+    L.w[s] = o; o = a16(o + (size_t)kKC * 8 + 16);
+  }
+  L.q = o; o = a16(o + kKC * 8);
+  L.sq = o; o = a16(o + kKC * 8);
+  o = (o + 127) & ~(size_t)127;
+  L.op = o; o = a16(o + (size_t)4 * kOpBytes);     // 2 stages x (hi, lo)
+  L.bars = o; o = a16(o + 4 * 8);
+  L.tmem = o; o = a16(o + 16);
+  L.gram = o; o = a16(o + (size_t)pmax * (pmax + 1) / 2 * 4);
+  L.vec = o; o = a16(o + (size_t)7 * (pmax + 1) * 8);
+  L.fidx = o; o = a16(o + (size_t)kPmax * 4);
+  L.total = o;
+  return L;
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 a, __nv_bfloat16 b) {
+  return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
+}
+
+struct TcState {
+  uint32_t load_uses[2];
+  uint32_t mma_commits[2];
+  uint32_t mma_waits[2];
+};
+
+__global__ void __launch_bounds__(kTcThreads, 2) ridge_tc_kernel(RidgeArgs a, RidgeLists L,
+                                                                 uint32_t tmem_cols) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ int s_item, s_fail, s_flag;
+  __shared__ double s_scalar[8];
+  const TcLayout lay = tc_layout(a.pmax, a.dmax);
+  uint64_t* load_bar = (uint64_t*)(smem + lay.bars);
+  uint64_t* mma_bar = load_bar + 2;
+  uint32_t* s_tmem = (uint32_t*)(smem + lay.tmem);
+  float* Gf = (float*)(smem + lay.gram);
+  double* vec = (double*)(smem + lay.vec);
+  int16_t* fidx = (int16_t*)(smem + lay.fidx);
+  double* sq_q = (double*)(smem + lay.q);
+  double* sq_s = (double*)(smem + lay.sq);
+  unsigned char* op = smem + lay.op;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+  if (warp == 0) {
+    tmem_alloc(s_tmem, tmem_cols);
+    tmem_relinquish();
+  }
+  if (tid == 0) {
+    for (int i = 0; i < 4; ++i) mbar_init(&load_bar[i], 1);
+    fence_mbar_init();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s_tmem;
+  TcState S = {{0, 0}, {0, 0}, {0, 0}};
+  bool abort = false;
+  const int count = L.count[CLS_TENSOR];
+
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(&L.cursor[CLS_TENSOR], 1);
+    __syncthreads();
+    const int item = s_item;
+    __syncthreads();
+    if (item >= count) break;
+    const int k = L.list[(int64_t)CLS_TENSOR * a.K + item];
+    const RidgeItem it = load_item(a, k);
+    const int p = it.p, d = it.d;
+    const int P16 = (p + 15) & ~15;
+    const bool two = P16 > 128;
+    const int N1 = P16, N2 = two ? P16 - 128 : 0;
+    const int g0 = two ? (P16 - 128) / 8 : 0;
+    const int64_t nchunks = (it.n + kKC - 1) / kKC;
+    if (nchunks == 0) {  // nothing to accumulate: the FP64 form reports the status
+      if (tid == 0) push_list(L, a.K, CLS_RESOLVE, k);
+      continue;
+    }
+    for (int f = tid; f < P16; f += kTcThreads) {
+      int fa_ = -3, fb_ = -1;
+      if (f < p) feature_factors(d, it.kind, f, fa_, fb_);
+      fidx[2 * f] = (int16_t)fa_;
+      fidx[2 * f + 1] = (int16_t)fb_;
+    }
+    // item slots of this thread: (f, octet) = (j % P16, j / P16), j = tid + 256 s
+    double hacc[3] = {0.0, 0.0, 0.0}, dacc[3] = {0.0, 0.0, 0.0};
+    int bad = 0;
+    if (tid == 0) {
+      for (int64_t c = 0; c < min((int64_t)2, nchunks); ++c) {
+        const int64_t rr = c * kKC;
+        const int rows = (int)min((int64_t)kKC, it.n - rr);
+        Granules gx = granules(a.x + it.xoff + rr * d, (uint64_t)rows * d * 8);
+        Granules gy = granules(a.y + it.r0 + rr, (uint64_t)rows * 8);
+        Granules gw = a.w ? granules(a.w + it.r0 + rr, (uint64_t)rows * 8) : Granules{nullptr, 0, 0};
+        mbar_arrive_expect_tx(&load_bar[c], gx.bytes + gy.bytes + gw.bytes);
+        bulk_g2s(smem + lay.x[c], gx.base, gx.bytes, &load_bar[c]);
+        bulk_g2s(smem + lay.y[c], gy.base, gy.bytes, &load_bar[c]);
+        if (a.w) bulk_g2s(smem + lay.w[c], gw.base, gw.bytes, &load_bar[c]);
+      }
+    }
+    __syncthreads();
+    const uint32_t id1 = idesc_bf16(128, N1), id2 = idesc_bf16(128, two ? N2 : 16);
+    for (int64_t c = 0; c < nchunks && !abort; ++c) {
+      const int st = (int)(c & 1);
+      bool ok = mbar_wait(&load_bar[st], S.load_uses[st] & 1);
+      S.load_uses[st]++;
+      if (c >= 2) {
+        ok = ok && mbar_wait(&mma_bar[st], S.mma_waits[st] & 1);
+        S.mma_waits[st]++;
+      }
+      if (!__syncthreads_and(ok)) { abort = true; break; }
+      const int rows = (int)min((int64_t)kKC, it.n - c * kKC);
+      const double* xs = (const double*)(smem + lay.x[st] +
+                                         (((uintptr_t)(a.x + it.xoff + c * kKC * d)) & 15));
+      const double* ys = (const double*)(smem + lay.y[st] +
+                                         (((uintptr_t)(a.y + it.r0 + c * kKC)) & 15));
+      const double* ws = a.w ? (const double*)(smem + lay.w[st] +
+                                               (((uintptr_t)(a.w + it.r0 + c * kKC)) & 15))
+                             : nullptr;
+      for (int e = tid; e < rows * d; e += kTcThreads) bad |= isfinite(xs[e]) ? 0 : 1;
+      if (tid < kKC) {
+        double qv = 0.0;
+        if (tid < rows) {
+          bad |= isfinite(ys[tid]) ? 0 : 1;
+          const double wv = ws ? ws[tid] : 1.0;
+          if (!(wv >= 0.0) || !isfinite(wv)) bad |= 2;
+          qv = fmax(wv, a.weight_floor);
+        }
+        sq_q[tid] = qv;
+        sq_s[tid] = sqrt(qv);
+      }
+      __syncthreads();
+      unsigned char* hi = op + (size_t)st * 2 * kOpBytes;
+      unsigned char* lo = hi + kOpBytes;
+      const int nitems = P16 * (kKC / 8);
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        const int j = tid + s * kTcThreads;
+        if (j < nitems) {
+          const int f = j % P16, oct = j / P16;
+          const int ia = fidx[2 * f], ib = fidx[2 * f + 1];
+          uint32_t ph[4], pl[4];
+#pragma unroll
+          for (int e = 0; e < 8; e += 2) {
+            __nv_bfloat16 h2[2], l2[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+              const int r = oct * 8 + e + u;
+              float v = 0.0f;
+              if (r < rows && ia != -3) {
+                const double* xr = xs + (int64_t)r * d;
+                const double phi = (ia < 0 ? 1.0 : xr[ia]) * (ib < 0 ? 1.0 : xr[ib]);
+                const double qphi = sq_q[r] * phi;
+                hacc[s] = fma(qphi, ys[r], hacc[s]);
+                dacc[s] = fma(qphi, phi, dacc[s]);
+                v = (float)(sq_s[r] * phi);
+              }
+              h2[u] = __float2bfloat16_rn(v);
+              l2[u] = __float2bfloat16_rn(v - __bfloat162float(h2[u]));
+            }
+            ph[e >> 1] = pack_bf16(h2[0], h2[1]);
+            pl[e >> 1] = pack_bf16(l2[0], l2[1]);
+          }
+          const size_t off = (size_t)(f >> 3) * kSBO + (size_t)oct * 128 + (size_t)(f & 7) * 16;
+          *(uint4*)(hi + off) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
+          *(uint4*)(lo + off) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+        }
+      }
+      fence_proxy_async();  // operand writes -> visible to the tensor core
+      __syncthreads();
+      if (tid == 0) {
+        if (c + 2 < nchunks) {
+          const int64_t rr = (c + 2) * kKC;
+          const int r2 = (int)min((int64_t)kKC, it.n - rr);
+          Granules gx = granules(a.x + it.xoff + rr * d, (uint64_t)r2 * d * 8);
+          Granules gy = granules(a.y + it.r0 + rr, (uint64_t)r2 * 8);
+          Granules gw = a.w ? granules(a.w + it.r0 + rr, (uint64_t)r2 * 8) : Granules{nullptr, 0, 0};
+          mbar_arrive_expect_tx(&load_bar[st], gx.bytes + gy.bytes + gw.bytes);
+          bulk_g2s(smem + lay.x[st], gx.base, gx.bytes, &load_bar[st]);
+          bulk_g2s(smem + lay.y[st], gy.base, gy.bytes, &load_bar[st]);
+          if (a.w) bulk_g2s(smem + lay.w[st], gw.base, gw.bytes, &load_bar[st]);
+        }
+        tc_fence_after();
+        const uint32_t hb = smem_u32(hi), lb = smem_u32(lo);
+#pragma unroll
+        for (int s = 0; s < kKC / 16; ++s) {
+          const uint32_t ko = (uint32_t)s * 2 * kLBO;
+#pragma unroll
+          for (int prod = 0; prod < 3; ++prod) {
+            const uint32_t A = (prod == 2) ? lb : hb;
+            const uint32_t B = (prod == 1) ? lb : hb;
+            const uint32_t acc = (c == 0 && s == 0 && prod == 0) ? 0u : 1u;
+            mma_bf16(tmem, smem_desc(A + ko), smem_desc(B + ko), id1, acc);
+            if (two)
+              mma_bf16(tmem + (uint32_t)N1, smem_desc(A + (uint32_t)g0 * kSBO + ko),
+                       smem_desc(B + 16u * kSBO + ko), id2, acc);
+          }
+        }
+        mma_commit(&mma_bar[st]);
+      }
+      S.mma_commits[st]++;
+    }
+    // all MMAs of this system complete
+    bool ok = !abort;
+    for (int st = 0; st < 2; ++st)
+      while (S.mma_waits[st] < S.mma_commits[st]) {
+        ok = mbar_wait(&mma_bar[st], S.mma_waits[st] & 1) && ok;
+        S.mma_waits[st]++;
+      }
+    if (!__syncthreads_and(ok) || abort) {
+      abort = true;
+      if (tid == 0) { atomicExch(L.err, 1); a.status[k] = -5; }
+      break;
+    }
+    tc_fence_after();
+    // ---- drain the FP32 Gram from TMEM into packed lower storage
+    {
+      const int sp = warp & 3, half = warp >> 2;
+      const int row = 32 * sp + lane;
+      const uint32_t lane_base = tmem + ((uint32_t)(32 * sp) << 16);
+      for (int cb = half * 16; cb < N1; cb += 32) {
+        float v[16];
+        tmem_ld16(lane_base + (uint32_t)cb, v);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int col = cb + j;
+          if (row < p && col <= row) Gf[pk(row, col)] = v[j];
+        }
+      }
+      if (two) {
+        const int frow = g0 * 8 + row;
+        for (int cb = half * 16; cb < N2; cb += 32) {
+          float v[16];
+          tmem_ld16(lane_base + (uint32_t)(N1 + cb), v);
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int col = 128 + cb + j;
+            if (frow >= 128 && frow < p && col <= frow) Gf[pk(frow, col)] = v[j];
+          }
+        }
+      }
+    }
+    tc_fence_before();
+    // ---- reduce exact h and diag over the row octets (fixed order)
+    double* red = (double*)op;  // operand buffers are idle now
+    const int nitems = P16 * (kKC / 8);
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+      const int j = tid + s * kTcThreads;
+      if (j < nitems) {
+        red[2 * j] = hacc[s];
+        red[2 * j + 1] = dacc[s];
+      }
+    }
+    {
+      const int bw = __syncthreads_or(bad & 2), bx = __syncthreads_or(bad & 1);
+      bad = (bw ? 2 : 0) | (bx ? 1 : 0);
+    }
+    const int vs = a.pmax + 1;  // vector stride (tc_layout reserves 7 * vs)
+    double* h = vec;
+    double* dg = vec + vs;
+    double* beta = vec + 2 * vs;
+    double* r = vec + 3 * vs;
+    double* v1 = vec + 4 * vs;
+    double* v2 = vec + 5 * vs;
+    for (int f = tid; f < p; f += kTcThreads) {
+      double hs = 0.0, ds = 0.0;
+      for (int oct = 0; oct < kKC / 8; ++oct) {
+        hs += red[2 * (oct * P16 + f)];
+        ds += red[2 * (oct * P16 + f) + 1];
+      }
+      h[f] = hs;
+      dg[f] = ds;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double tr = 0.0;
+      for (int f = 0; f < p; ++f) tr += dg[f];
+      const double lam = it.ridge * tr / p;
+      s_scalar[0] = lam;
+      L.lambda[k] = lam;
+    }
+    __syncthreads();
+    const double lam = s_scalar[0];
+    if (bad) {
+      if (tid == 0) push_list(L, a.K, CLS_RESOLVE, k);
+      continue;
+    }
+    for (int f = tid; f < p; f += kTcThreads) Gf[pk(f, f)] = (float)(dg[f] + lam);
+    __syncthreads();
+    const bool want_cond = (a.cond != nullptr) || (a.solver == ART_SOLVER_AUTO);
+    if (want_cond && warp == 0) {
+      const double an = warp_sym_norm1(Gf, p);
+      if (lane == 0) s_scalar[1] = an;
+    }
+    const int fail = chol_packed<float, 8>(Gf, p, &s_fail);
+    if (fail) {
+      if (tid == 0) push_list(L, a.K, CLS_RESOLVE, k);
+      continue;
+    }
+    // ---- FP64 iterative refinement
+    for (int f = tid; f < p; f += kTcThreads) { beta[f] = 0.0; r[f] = h[f]; }
+    __syncthreads();
+    const int dp = d + 1;  // padded row stride in the refinement buffer
+    int KR = (int)((size_t)(4 * kOpBytes) / ((size_t)dp * 8 + 16));
+    KR = min(KR, kTcThreads);
+    double* xr = (double*)op;           // KR rows, stride dp
+    double* se = xr + (size_t)KR * dp;  // KR scaled row errors
+    double nd_prev = 0.0;
+    int outcome = 0;  // 1 converged, 2 stalled/failed
+    uint32_t info = 0;
+    for (int iter = 0; iter < kMaxRefine && outcome == 0; ++iter) {
+      if (iter > 0) {
+        // r = h - lambda beta - sum_k q_k (phi_k . beta) phi_k, in FP64 from the rows.
+        // Phase 1: one warp per row, lane l owns features l + 32 m (m < 5).
+        int fa_r[5], fb_r[5];
+        double b_r[5];
+#pragma unroll
+        for (int m = 0; m < 5; ++m) {
+          const int f = lane + 32 * m;
+          fa_r[m] = f < p ? fidx[2 * f] : -3;
+          fb_r[m] = f < p ? fidx[2 * f + 1] : -1;
+          b_r[m] = f < p ? beta[f] : 0.0;
+        }
+        const int ia2 = tid < p ? fidx[2 * tid] : -3, ib2 = tid < p ? fidx[2 * tid + 1] : -1;
+        double accf = 0.0;
+        for (int64_t c0 = 0; c0 < it.n; c0 += KR) {
+          const int rows = (int)min((int64_t)KR, it.n - c0);
+          for (int e = tid; e < rows * d; e += kTcThreads) {
+            const int rr = e / d, cc = e - rr * d;
+            xr[rr * dp + cc] = a.x[it.xoff + (c0 + rr) * d + cc];
+          }
+          __syncthreads();
+          for (int rr = warp; rr < rows; rr += kTcThreads / 32) {
+            const double* xk = xr + rr * dp;
+            double e_ = 0.0;
+#pragma unroll
+            for (int m = 0; m < 5; ++m) {
+              if (fa_r[m] != -3)
+                e_ = fma((fa_r[m] < 0 ? 1.0 : xk[fa_r[m]]) * (fb_r[m] < 0 ? 1.0 : xk[fb_r[m]]),
+                         b_r[m], e_);
+            }
+            e_ = warp_sum(e_);
+            if (lane == 0) {
+              const double wv = a.w ? a.w[it.r0 + c0 + rr] : 1.0;
+              se[rr] = fmax(wv, a.weight_floor) * e_;
+            }
+          }
+          __syncthreads();
+          if (tid < p) {
+            for (int rr = 0; rr < rows; ++rr) {
+              const double* xk = xr + rr * dp;
+              accf = fma(se[rr], (ia2 < 0 ? 1.0 : xk[ia2]) * (ib2 < 0 ? 1.0 : xk[ib2]), accf);
+            }
+          }
+          __syncthreads();
+        }
+        if (tid < p) r[tid] = h[tid] - lam * beta[tid] - accf;
+        __syncthreads();
+      }
+      if (warp == 0) {
+        for (int f = lane; f < p; f += 32) v1[f] = r[f];
+        __syncwarp();
+        warp_forward<float, double>(Gf, v1, p);
+        warp_backward<float, double>(Gf, v1, p);
+        double nd = 0.0, nb = 0.0;
+        for (int f = lane; f < p; f += 32) {
+          const double b = beta[f] + v1[f];
+          beta[f] = b;
+          nd = fmax(nd, fabs(v1[f]));
+          nb = fmax(nb, fabs(b));
+        }
+        nd = warp_max(nd);
+        nb = warp_max(nb);
+        if (lane == 0) {
+          int out = 0;
+          if (!(nd <= 1e300) || !(nb <= 1e300)) out = 2;           // non-finite
+          else if (nd <= 2.3e-16 * nb) out = 1;                     // at working precision
+          else if (iter >= 1 && nd > 0.5 * nd_prev) out = (nd <= 1e-12 * nb) ? 1 : 2;
+          else if (iter == kMaxRefine - 1) out = (nd <= 1e-12 * nb) ? 3 : 2;
+          s_flag = out;
+        }
+        nd_prev = nd;
+      }
+      __syncthreads();
+      outcome = s_flag;
+      if (outcome == 3) { outcome = 1; info |= ART_INFO_REFINE_CAP; }
+    }
+    if (outcome != 1) {
+      if (tid == 0) push_list(L, a.K, CLS_RESOLVE, k);
+      continue;
+    }
+    double cond = __longlong_as_double(0x7ff8000000000000ll);
+    if (want_cond) {
+      if (warp == 0) {
+        const double est = warp_inv_norm1_estimate<float>(Gf, p, v1, v2);
+        if (lane == 0) {
+          const double an = s_scalar[1];
+          s_scalar[2] = (est > 0.0 && isfinite(est) && an > 0.0) ? 1.0 / (an * est) : 0.0;
+        }
+      }
+      __syncthreads();
+      const double rcond = s_scalar[2];
+      if (a.solver == ART_SOLVER_AUTO && rcond < a.rcond_threshold) {
+        // let the FP64 form apply the auto policy exactly
+        if (tid == 0) push_list(L, a.K, CLS_RESOLVE, k);
+        continue;
+      }
+      cond = rcond > 0.0 ? sqrt(1.0 / fmin(rcond, 1.0)) : __longlong_as_double(0x7ff0000000000000ll);
+    }
+    for (int f = tid; f < p; f += kTcThreads) a.beta[(int64_t)k * a.beta_stride + f] = beta[f];
+    if (tid == 0) {
+      a.status[k] = 0;
+      if (a.ridge_eff) a.ridge_eff[k] = lam;
+      if (a.cond) a.cond[k] = cond;
+      if (a.info) a.info[k] = info;
+    }
+    __syncthreads();
+  }
+  // release TMEM (after a bounded wait for any MMA still in flight)
+  for (int st = 0; st < 2; ++st)
+    while (S.mma_waits[st] < S.mma_commits[st]) {
+      mbar_wait(&mma_bar[st], S.mma_waits[st] & 1);
+      S.mma_waits[st]++;
+    }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) tmem_dealloc(tmem, tmem_cols);
+}
+
+}  // namespace
+
+int launch_ridge_tensor(const RidgeArgs& a, const RidgeLists& L, cudaStream_t s) {
+  if (a.dmax > ART_MAX_DIM) {
+    set_error("mixed precision requires max_dim <= %d", ART_MAX_DIM);
+    return ART_E_UNSUPPORTED;
+  }
+  const int P16 = (std::min(a.pmax, kPmax) + 15) & ~15;
+  const int cols_needed = P16 + (P16 > 128 ? P16 - 128 : 0);
+  uint32_t cols = 32;
+  while ((int)cols < cols_needed) cols <<= 1;
+  size_t smem = tc_layout(a.pmax, a.dmax).total;
+  // TMEM: CTAs resident on one SM must fit 512 columns together; widen the
+  // shared-memory request if occupancy would allow more CTAs than that.
+  const int max_ctas = (int)(512 / cols);
+  cudaFuncSetAttribute(ridge_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  int occ = 0;
+  for (;;) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ridge_tc_kernel, kTcThreads, smem);
+    if (occ <= max_ctas || smem >= 200 * 1024) break;
+    smem += 8 * 1024;
+  }
+  if (occ > max_ctas || occ < 1) {
+    set_error("ridge_tc: cannot place CTAs within TMEM capacity (occ %d, cols %u)", occ, cols);
+    return ART_E_UNSUPPORTED;
+  }
+  cudaFuncSetAttribute(ridge_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int64_t grid = std::min<int64_t>((int64_t)device_sm_count() * occ, a.K);
+  prof_begin("ridge_tc", s);
+  ridge_tc_kernel<<<(unsigned)std::max<int64_t>(grid, 1), kTcThreads, smem, s>>>(a, L, cols);
+  prof_end(s);
+  count_launch();
+  return check_launch("ridge_tc");
+}
+
 }  // namespace art
