@@ -240,6 +240,7 @@ int launch_har_l(const HarArgs& a, int maxk, cudaStream_t s) {
 using namespace art;
 
 extern "C" int art_hit_and_run(const ArtPolytopes* P, const ArtChains* C, art_stream_t stream) {
+  cudaGetLastError();
   if (!P || !C) { set_error("art_hit_and_run: null argument"); return ART_E_INVALID; }
   if (C->count < 0 || P->count < 0) { set_error("art_hit_and_run: negative count"); return ART_E_INVALID; }
   if (C->count == 0) return ART_OK;

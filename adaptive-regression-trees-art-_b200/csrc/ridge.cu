@@ -476,9 +476,17 @@ static int launch_persistent(Kern kern, size_t smem, int64_t max_items, cudaStre
     set_error("%s: shared memory %zu bytes exceeds the 227 KB limit", name, smem);
     return ART_E_UNSUPPORTED;
   }
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    set_error("%s: cannot reserve %zu bytes of shared memory", name, smem);
+    return ART_E_UNSUPPORTED;
+  }
   int occ = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kRidgeThreads, smem);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kRidgeThreads, smem) != cudaSuccess) {
+    cudaGetLastError();
+    occ = 1;
+  }
   if (occ < 1) occ = 1;
   int64_t grid = (int64_t)device_sm_count() * occ;
   if (grid > max_items) grid = max_items;
@@ -544,6 +552,7 @@ extern "C" int art_ridge_batched(const ArtRidgeProblem* pr, const ArtRidgeResult
     return ART_E_WORKSPACE;
   }
   cudaStream_t s = (cudaStream_t)stream;
+  cudaGetLastError();  // clear a stale, non-sticky error left by an earlier runtime call
   unsigned char* ws = (unsigned char*)workspace;
   RidgeArgs a;
   a.K = K;
@@ -613,7 +622,12 @@ extern "C" int art_ridge_batched(const ArtRidgeProblem* pr, const ArtRidgeResult
       set_error("ridge_qr: shared memory %zu bytes exceeds the 227 KB limit", sm);
       return ART_E_UNSUPPORTED;
     }
-    cudaFuncSetAttribute(ridge_qr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (cudaFuncSetAttribute(ridge_qr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      set_error("ridge_qr: cannot reserve %zu bytes of shared memory", sm);
+      return ART_E_UNSUPPORTED;
+    }
     int64_t grid = std::min<int64_t>(K, device_sm_count());
     prof_begin("ridge_qr", s);
     ridge_qr_kernel<<<(unsigned)grid, kRidgeThreads, sm, s>>>(a, L);

@@ -557,18 +557,26 @@ int launch_ridge_tensor(const RidgeArgs& a, const RidgeLists& L, cudaStream_t s)
   // TMEM: CTAs resident on one SM must fit 512 columns together; widen the
   // shared-memory request if occupancy would allow more CTAs than that.
   const int max_ctas = (int)(512 / cols);
-  cudaFuncSetAttribute(ridge_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
   int occ = 0;
   for (;;) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ridge_tc_kernel, kTcThreads, smem);
-    if (occ <= max_ctas || smem >= 200 * 1024) break;
+    if (cudaFuncSetAttribute(ridge_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("ridge_tc: cannot reserve %zu bytes of shared memory", smem);
+      return ART_E_UNSUPPORTED;
+    }
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ridge_tc_kernel, kTcThreads, smem) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      occ = 0;
+    }
+    if (occ <= max_ctas || smem + 8 * 1024 > 200 * 1024) break;
     smem += 8 * 1024;
   }
   if (occ > max_ctas || occ < 1) {
     set_error("ridge_tc: cannot place CTAs within TMEM capacity (occ %d, cols %u)", occ, cols);
     return ART_E_UNSUPPORTED;
   }
-  cudaFuncSetAttribute(ridge_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int64_t grid = std::min<int64_t>((int64_t)device_sm_count() * occ, a.K);
   prof_begin("ridge_tc", s);
   ridge_tc_kernel<<<(unsigned)std::max<int64_t>(grid, 1), kTcThreads, smem, s>>>(a, L, cols);

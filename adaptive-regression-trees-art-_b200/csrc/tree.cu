@@ -111,6 +111,7 @@ using namespace art;
 extern "C" int art_partition_rows(const ArtSegments* seg, const double* x, const double* theta,
                                   int64_t theta_stride, const int8_t* split, int64_t* perm,
                                   int32_t* n_right, art_stream_t stream) {
+  cudaGetLastError();
   if (!seg || !x || !theta || !perm) { set_error("art_partition_rows: null argument"); return ART_E_INVALID; }
   if (seg->count < 0 || seg->count > 0x7fffffff) { set_error("art_partition_rows: bad count"); return ART_E_INVALID; }
   if (seg->count == 0) return ART_OK;
@@ -127,6 +128,7 @@ extern "C" int art_tree_predict(int32_t dim, int64_t n_nodes, const int32_t* chi
                                 const double* theta, int64_t theta_stride, const double* coef,
                                 int64_t coef_stride, const int32_t* features, int64_t n_points,
                                 const double* x, int32_t* leaf, double* pred, art_stream_t stream) {
+  cudaGetLastError();
   if (dim < 1 || dim > ART_MAX_DIM) { set_error("art_tree_predict: bad dim %d", dim); return ART_E_UNSUPPORTED; }
   if (n_nodes < 1 || !child || !theta || !x || (pred && (!coef || !features))) {
     set_error("art_tree_predict: null argument");

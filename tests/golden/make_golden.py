@@ -94,6 +94,76 @@ def ridge_cases(ref):
     print("ridge cases:", len(cases))
 
 
+SPLIT_SPECS = [
+    # (seed, n, d, kind, T, ridge, restarts, max_iters, extra splitter kwargs)
+    (101, 200, 2, 0, 0.1, 1e-6, 1, 30, {}),
+    (102, 150, 3, 2, 0.3, 1e-4, 2, 15, {}),
+    (103, 300, 4, 0, 0.05, 1e-6, 3, 40, {"adaptive_alpha": False, "alpha0": 0.5}),
+    (104, 120, 2, 0, 0.02, 1e-6, 1, 25, {"min_side_points": 40, "min_side_fallback": True,
+                                         "min_side_fraction": 0.0}),
+    (105, 400, 6, 0, 0.2, 1e-5, 2, 20, {"max_backtracks": 6, "heavy_backtrack_threshold": 3}),
+    (106, 250, 3, 1, 0.15, 1e-3, 1, 12, {"alpha_max": 1e8, "max_line_search_failures": 5}),
+]
+
+
+def split_target(X, rng):
+    a = rng.normal(size=X.shape[1])
+    a /= np.linalg.norm(a)
+    return np.tanh(6 * (X @ a - 0.1)) + 0.3 * X[:, 0] ** 2 + 0.01 * rng.normal(size=X.shape[0])
+
+
+def split_cases(ref):
+    from oracle import ridge as O
+    from oracle import split as S
+
+    out = {}
+    for i, (seed, n, d, kind, T, lam, R, iters, extra) in enumerate(SPLIT_SPECS):
+        rng = np.random.default_rng(seed)
+        X = rng.uniform(-1, 1, (n, d))
+        y = split_target(X, rng)
+        if kind == O.AFFINE:
+            model = ref.models.AffineRidgeModel(ridge=lam)
+        else:
+            model = ref.models.PolynomialRidgeModel(degree=2 if kind == O.POLY2 else 1, ridge=lam)
+        kw = dict(max_iters=iters, n_restarts=R, random_state=seed + 1000)
+        kw.update(extra)
+        splitter = ref.splitters.SoftObliqueSplitter(model, T, **kw)
+        res = splitter.split(X, y)
+        # oracle with the same theta0 draws
+        init_rng = np.random.default_rng(seed + 1000)
+        theta0s = [S.initialize_theta(X, init_rng) for _ in range(R)]
+        params = S.Params(max_iters=iters, n_restarts=R, **{k: v for k, v in extra.items()})
+        phi = O.features(X, kind)
+        parent = O.solve_weighted_ridge(phi, y, np.ones(n), lam)["coefficients"]
+        parent_loss = float(np.mean((y - phi @ parent) ** 2))
+        mine = S.split(X, y, theta0s, T, kind, lam, parent_loss, params)
+        np.testing.assert_allclose(np.r_[mine["w"], mine["z"]], np.r_[res.w, res.z], rtol=1e-9, atol=1e-11)
+        assert mine["stop_reason"] == res.stop_reason and mine["n_iters"] == res.n_iters
+        np.testing.assert_allclose(mine["losses"], res.metadata["soft_loss_history"], rtol=1e-9, atol=1e-13)
+        np.testing.assert_allclose(mine["loss"], res.loss, rtol=1e-9)
+        assert mine["n_right"] == res.n_right
+        out[f"s{i}_X"] = X
+        out[f"s{i}_y"] = y
+        out[f"s{i}_theta0"] = np.array(theta0s)
+        out[f"s{i}_meta"] = np.array([kind, T, lam, R, iters, parent_loss], dtype=float)
+        out[f"s{i}_extra"] = np.array(repr(extra))
+        out[f"s{i}_theta"] = np.r_[res.w, res.z]
+        out[f"s{i}_loss"] = np.array(res.loss)
+        out[f"s{i}_n_right"] = np.array(res.n_right)
+        out[f"s{i}_n_iters"] = np.array(res.n_iters)
+        out[f"s{i}_stop"] = np.array(res.stop_reason)
+        out[f"s{i}_soft_losses"] = np.array(res.metadata["soft_loss_history"])
+        out[f"s{i}_steps"] = np.array(res.metadata["step_size_history"])
+        out[f"s{i}_backtracks"] = np.array(res.metadata["backtrack_history"])
+        out[f"s{i}_grad_norms"] = np.array(res.metadata["projected_grad_norm_history"])
+        out[f"s{i}_beta_left"] = res.left_model.coef_
+        out[f"s{i}_beta_right"] = res.right_model.coef_
+        out[f"s{i}_fallback"] = np.array(bool(res.metadata.get("min_side_fallback", False)))
+    out["count"] = np.array(len(SPLIT_SPECS))
+    np.savez_compressed(HERE / "split_golden.npz", **out)
+    print("split cases:", len(SPLIT_SPECS))
+
+
 def main():
     root = Path(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ART_REFERENCE", ""))
     if not (root / "art" / "__init__.py").exists():
