@@ -39,6 +39,8 @@ INFO_CHOLESKY_FAILED = 4
 INFO_FP64_RESOLVE = 8
 INFO_REFINE_CAP = 16
 INFO_COND_FAILED = 32
+INFO_REFINE_SHIFT = 8
+RIDGE_OPT_FP64_FACTOR = 1
 
 MAX_FEATURES = 160
 MAX_DIM = 64
@@ -72,6 +74,7 @@ class ArtRidgeProblem(C.Structure):
         ("seg", ArtSegments), ("x", P), ("y", P), ("w", P), ("ridge", P),
         ("weight_floor", F64), ("solver", I32), ("precision", I32),
         ("auto_rcond_threshold", F64), ("max_features", I32), ("max_dim", I32),
+        ("options", C.c_uint32), ("reserved", I32),
     ]
 
 
@@ -131,6 +134,7 @@ class ArtChains(C.Structure):
 SIGNATURES = {
     "art_ridge_workspace_size": (C.c_size_t, [I64, I32]),
     "art_ridge_batched": (C.c_int, [C.POINTER(ArtRidgeProblem), C.POINTER(ArtRidgeResult), P, C.c_size_t, P]),
+    "art_ridge_gram": (C.c_int, [C.POINTER(ArtRidgeProblem), P, I64, P, P, C.c_size_t, P]),
     "art_split_workspace_size": (C.c_size_t, [I64, I32, I32, I32]),
     "art_split_level": (C.c_int, [C.POINTER(ArtSplitProblem), C.POINTER(ArtSplitParams),
                                   C.POINTER(ArtSplitResult), P, C.c_size_t, P]),

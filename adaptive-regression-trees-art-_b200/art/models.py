@@ -233,6 +233,7 @@ def solve_weighted_ridge_batched(
     max_features: int | None = None,
     max_dim: int | None = None,
     condition: bool = False,
+    fp64_factor: bool = False,
     out: BatchedRidgeResult | None = None,
     stream=None,
 ) -> BatchedRidgeResult:
@@ -243,7 +244,8 @@ def solve_weighted_ridge_batched(
     one value per row, system k owning rows ``row_offsets[k]:row_offsets[k+1]``.
     ``weights=None`` means unit weights.  All array arguments may be numpy or
     torch; they are moved to the current CUDA device.  No host sync happens
-    unless the caller reads the result.
+    unless the caller reads the result.  ``fp64_factor`` makes the mixed form
+    factor its tensor-core Gram in FP64 (``ART_RIDGE_OPT_FP64_FACTOR``).
     """
 
     t = torch()
@@ -292,6 +294,7 @@ def solve_weighted_ridge_batched(
     prob = N.ArtRidgeProblem(
         seg, ptr(x), ptr(y), ptr(w), ptr(ridge_t), float(weight_floor), _SOLVER_CODES[solver],
         _PRECISION_CODES[precision], float(auto_rcond_threshold), int(max_features), int(max_dim),
+        N.RIDGE_OPT_FP64_FACTOR if fp64_factor else 0, 0,
     )
     res = N.ArtRidgeResult(
         ptr(out.beta), int(out.beta.shape[1]), ptr(out.ridge_effective), ptr(out.cond_estimate),
@@ -304,6 +307,47 @@ def solve_weighted_ridge_batched(
     # keep inputs alive until the stream has consumed them
     out._keepalive = (x, y, w, ro, xo, dims_t, feats, ridge_t)
     return out
+
+
+def ridge_gram_batched(x, y, weights, row_offsets, dims, features, *, x_offsets=None,
+                       weight_floor: float = 1e-12, max_features: int | None = None,
+                       max_dim: int | None = None, stream=None):
+    """Tensor-core weighted Grams (BF16 hi/lo split products, FP32 accumulation).
+
+    Returns (packed lower-triangular Grams [K, pmax(pmax+1)/2] float32, status[K]);
+    systems outside 33 <= p <= 160 get status -4.
+    """
+
+    t = torch()
+    lib = N.load_library()
+    dev = require_cuda()
+    x = to_device(x, t.float64, dev)
+    y = to_device(y, t.float64, dev)
+    w = None if weights is None else to_device(weights, t.float64, dev)
+    ro = to_device(row_offsets, t.int64, dev)
+    dims_t = to_device(dims, t.int32, dev)
+    feats = to_device(features, t.int32, dev)
+    K = int(dims_t.numel())
+    if x_offsets is None:
+        x_offsets = ro[:-1] * dims_t.to(t.int64)
+    xo = to_device(x_offsets, t.int64, dev)
+    if max_features is None:
+        max_features = max(kind_feature_count(int(d), int(f)) for d, f in zip(dims_t.cpu().numpy(), feats.cpu().numpy()))
+    if max_dim is None:
+        max_dim = int(dims_t.max().item())
+    ridge_t = t.zeros(K, dtype=t.float64, device=dev)
+    E = max_features * (max_features + 1) // 2
+    gram = t.full((K, E), float("nan"), dtype=t.float32, device=dev)
+    status = t.empty(K, dtype=t.int32, device=dev)
+    seg = N.ArtSegments(K, ptr(ro), ptr(xo), ptr(dims_t), ptr(feats))
+    prob = N.ArtRidgeProblem(seg, ptr(x), ptr(y), ptr(w), ptr(ridge_t), float(weight_floor), N.SOLVER_NORMAL,
+                             N.PRECISION_MIXED, 1e-10, int(max_features), int(max_dim), 0, 0)
+    nbytes = lib.art_ridge_workspace_size(K, int(max_features))
+    ws = WORKSPACES.get(nbytes, stream)
+    rc = lib.art_ridge_gram(C.byref(prob), ptr(gram), E, ptr(status), ptr(ws), ws.numel(), stream_handle(stream))
+    N.check(rc, "art_ridge_gram")
+    gram._keepalive = (x, y, w, ro, xo, dims_t, feats, ridge_t)
+    return gram, status
 
 
 # ---------------------------------------------------------------- single

@@ -1,0 +1,434 @@
+"""Hit-and-run sampling in node polytopes on the GPU.
+
+Drop-in for the reference ``art/sampling.py``: ``HitAndRunSampler``
+(sampling.py:432-564), ``BatchedHitAndRunSampler`` and its numba variants
+(601-1025) and the host helpers.  Chains run in ``art_hit_and_run``; box rows
+(``+-e_i``) are applied structurally, every other row densely, all in FP64.
+
+Random draws come from one of two sources:
+
+* ``rng_mode="reference"`` -- the directions and chord uniforms are drawn on
+  the host from ``random_state`` in exactly the order the reference consumes
+  its generator, then injected; the chain then equals the reference chain
+  to rounding (the parity mode used by the tree builder's parity tests).
+* ``rng_mode="device"`` -- counter-based Philox4x32-10 on the device, keyed
+  per chain from ``random_state`` (the fast mode).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field, replace
+from typing import Literal, Protocol, Sequence, runtime_checkable
+
+import numpy as np
+
+from . import _native as N
+from ._device import ptr, require_cuda, stream_handle, to_device, torch
+from .domain import BoxDomain, PolytopeRegion
+
+RandomState = int | np.random.Generator | None
+RngMode = Literal["reference", "device"]
+
+
+def as_rng(random_state: RandomState = None) -> np.random.Generator:
+    if isinstance(random_state, np.random.Generator):
+        return random_state
+    return np.random.default_rng(random_state)
+
+
+@runtime_checkable
+class Sampler(Protocol):
+    def sample(self, region: PolytopeRegion, n: int, random_state: RandomState = None,
+               x0: np.ndarray | None = None) -> np.ndarray: ...
+
+
+def sample_uniform_box(bounds: np.ndarray, n: int, random_state: RandomState = None) -> np.ndarray:
+    """sampling.py:67-83 (host; the root of a box domain)."""
+
+    bounds = np.asarray(bounds, dtype=float)
+    if bounds.ndim != 2 or bounds.shape[1] != 2:
+        raise ValueError(f"bounds must have shape (d, 2), got {bounds.shape}.")
+    if np.any(bounds[:, 0] >= bounds[:, 1]):
+        raise ValueError("Each bound must satisfy low < high.")
+    if n < 0:
+        raise ValueError("n must be nonnegative.")
+    return as_rng(random_state).uniform(bounds[:, 0], bounds[:, 1], size=(int(n), bounds.shape[0]))
+
+
+def sample_covariance_eigendecomposition(samples, *, assume_centered: bool = False):
+    """sampling.py:86-106."""
+
+    values = np.asarray(samples, dtype=float)
+    if values.ndim != 2:
+        raise ValueError(f"samples must have shape (n_samples, d), got {values.shape}.")
+    if values.shape[0] < 2:
+        raise ValueError("samples must contain at least two points.")
+    if not np.all(np.isfinite(values)):
+        raise ValueError("samples must contain only finite values.")
+    centered = values if assume_centered else values - values.mean(axis=0, keepdims=True)
+    cov = centered.T @ centered / (centered.shape[0] - 1)
+    eigenvalues, eigenvectors = np.linalg.eigh(cov)
+    return eigenvectors, eigenvalues
+
+
+def floor_covariance_eigenvalues(eigenvalues, floor_ratio: float):
+    """sampling.py:109-127."""
+
+    values = np.asarray(eigenvalues, dtype=float).reshape(-1)
+    if values.size == 0:
+        raise ValueError("eigenvalues must contain at least one value.")
+    if not np.all(np.isfinite(values)):
+        raise ValueError("eigenvalues must be finite.")
+    if not np.isfinite(floor_ratio) or floor_ratio <= 0.0:
+        raise ValueError("floor_ratio must be positive.")
+    mean = float(np.mean(values))
+    if mean <= 0.0:
+        raise ValueError("eigenvalues must have a positive mean before flooring.")
+    floor = float(floor_ratio * mean)
+    return np.maximum(values, floor), floor
+
+
+def infer_box_bounds(region: PolytopeRegion, tol: float = 1e-12):
+    """sampling.py:145-167."""
+
+    lows = np.full(region.dimension, -np.inf)
+    highs = np.full(region.dimension, np.inf)
+    for row, bound in zip(region.A, region.b):
+        nz = np.flatnonzero(np.abs(row) > tol)
+        if nz.size != 1:
+            continue
+        i = int(nz[0])
+        coef = row[i]
+        if coef > 0:
+            highs[i] = min(highs[i], bound / coef)
+        else:
+            lows[i] = max(lows[i], bound / coef)
+    if np.any(~np.isfinite(lows)) or np.any(~np.isfinite(highs)) or np.any(lows >= highs):
+        return None
+    return np.column_stack([lows, highs])
+
+
+def find_feasible_point(region: PolytopeRegion, bounds=None, max_tries: int = 20000,
+                        random_state: RandomState = None, tol: float = 1e-10) -> np.ndarray:
+    """sampling.py:170-190 (host rejection sampling for a chain start)."""
+
+    if bounds is None:
+        bounds = infer_box_bounds(region)
+    if bounds is None:
+        raise ValueError("bounds are required when they cannot be inferred from the region.")
+    rng = as_rng(random_state)
+    for _ in range(max_tries):
+        x = sample_uniform_box(bounds, 1, random_state=rng)[0]
+        if bool(region.contains(x, tol=tol)[0]):
+            return x
+    raise RuntimeError("Could not find a feasible point inside the region.")
+
+
+def autocorrelation_by_lag(series: np.ndarray, lags: Sequence[int]) -> np.ndarray:
+    """Signed autocorrelation per lag and series (sampling.py:214-256; host diagnostic)."""
+
+    values = np.asarray(series, dtype=float)
+    if values.ndim == 1:
+        values = values.reshape(-1, 1)
+    if values.ndim != 2:
+        raise ValueError("series must have shape (n_steps,) or (n_steps, n_series).")
+    if values.shape[0] < 2:
+        raise ValueError("series must contain at least two states.")
+    if not np.all(np.isfinite(values)):
+        raise ValueError("series must contain only finite values.")
+    lags_array = np.asarray(lags, dtype=int).reshape(-1)
+    if lags_array.size == 0:
+        raise ValueError("lags must contain at least one value.")
+    if np.any(lags_array < 1) or np.any(lags_array >= values.shape[0]):
+        raise ValueError("lags must lie in [1, n_steps).")
+    centered = values - np.mean(values, axis=0, keepdims=True)
+    scales = np.max(np.abs(centered), axis=0)
+    nonconstant = scales > 0.0
+    normalized = np.zeros_like(centered)
+    np.divide(centered, scales, out=normalized, where=nonconstant)
+    variance = np.mean(normalized * normalized, axis=0)
+    out = np.zeros((lags_array.size, values.shape[1]))
+    for i, lag in enumerate(lags_array):
+        cov = np.mean(normalized[:-lag] * normalized[lag:], axis=0)
+        out[i] = np.divide(cov, variance, out=np.zeros_like(cov), where=nonconstant)
+    return out
+
+
+# ------------------------------------------------------------------ device
+@dataclass
+class DevicePolytopes:
+    """Polytopes in the kernel layout: box bounds + oblique CSR rows (torch CUDA)."""
+
+    dim: int
+    lo: object
+    hi: object
+    row_offsets: object
+    A: object
+    b: object
+    max_rows: int
+
+    @property
+    def count(self) -> int:
+        return int(self.lo.shape[0])
+
+
+def split_box_rows(A: np.ndarray, b: np.ndarray):
+    """Separate exact +-e_i rows (box bounds) from the other (oblique) rows.
+
+    A row equal to +e_i bounds x_i <= b, a row equal to -e_i bounds
+    x_i >= -b; for those rows A u = +-u_i exactly, so structural handling is
+    bit-identical to the dense product.  Later duplicates stay oblique.
+    """
+
+    A = np.asarray(A, float)
+    b = np.asarray(b, float)
+    d = A.shape[1]
+    lo = np.full(d, -np.inf)
+    hi = np.full(d, np.inf)
+    has_lo = np.zeros(d, bool)
+    has_hi = np.zeros(d, bool)
+    keep = np.ones(A.shape[0], bool)
+    for r in range(A.shape[0]):
+        nz = np.flatnonzero(A[r])
+        if nz.size != 1:
+            continue
+        i = int(nz[0])
+        if A[r, i] == 1.0 and not has_hi[i]:
+            hi[i], has_hi[i], keep[r] = b[r], True, False
+        elif A[r, i] == -1.0 and not has_lo[i]:
+            lo[i], has_lo[i], keep[r] = -b[r], True, False
+    return lo, hi, A[keep], b[keep]
+
+
+def device_polytopes(regions: Sequence[PolytopeRegion] | Sequence[tuple]) -> DevicePolytopes:
+    """Pack regions (or (A, b) pairs) for ``art_hit_and_run``."""
+
+    t = torch()
+    dev = require_cuda()
+    los, his, As, bs, offs = [], [], [], [], [0]
+    d = None
+    for reg in regions:
+        A, b = (reg.A, reg.b) if isinstance(reg, PolytopeRegion) else reg
+        lo, hi, Ao, bo = split_box_rows(A, b)
+        d = A.shape[1] if d is None else d
+        if A.shape[1] != d:
+            raise ValueError("all polytopes of one call must share the dimension")
+        los.append(lo)
+        his.append(hi)
+        As.append(Ao)
+        bs.append(bo)
+        offs.append(offs[-1] + Ao.shape[0])
+    max_rows = max((a.shape[0] for a in As), default=0)
+    if max_rows > 32:
+        raise ValueError("at most 32 non-box rows per polytope are supported")
+    Acat = np.concatenate(As) if offs[-1] else np.zeros((1, d))
+    bcat = np.concatenate(bs) if offs[-1] else np.zeros(1)
+    return DevicePolytopes(
+        d, to_device(np.stack(los), t.float64, dev), to_device(np.stack(his), t.float64, dev),
+        to_device(np.asarray(offs, np.int64), t.int64, dev), to_device(Acat, t.float64, dev),
+        to_device(bcat, t.float64, dev), max_rows)
+
+
+def hit_and_run_device(polys: DevicePolytopes, chain_polytope, x0, *, burn_in: int, thinning: int,
+                       n_rounds: int, mode: str = "batched", seeds=None, directions=None,
+                       uniforms=None, counter_base: int = 0, stream=None):
+    """Advance chains on the device.  Returns (samples[n_rounds, C, d], last x[C, d], status[C])."""
+
+    t = torch()
+    lib = N.load_library()
+    dev = require_cuda()
+    x = to_device(x0, t.float64, dev).clone()
+    Cn = int(x.shape[0])
+    cp = to_device(chain_polytope, t.int32, dev)
+    samples = t.empty((max(n_rounds, 0), Cn, polys.dim), dtype=t.float64, device=dev)
+    status = t.empty(Cn, dtype=t.int32, device=dev)
+    sd = None if seeds is None else to_device(np.asarray(seeds, dtype=np.uint64).view(np.int64) if not isinstance(seeds, t.Tensor) else seeds, t.int64, dev)
+    dr = None if directions is None else to_device(directions, t.float64, dev)
+    un = None if uniforms is None else to_device(uniforms, t.float64, dev)
+    P = N.ArtPolytopes(polys.count, polys.dim, ptr(polys.lo), ptr(polys.hi), ptr(polys.row_offsets),
+                       ptr(polys.A), ptr(polys.b), polys.max_rows, 0)
+    Ch = N.ArtChains(Cn, ptr(cp), ptr(x), ptr(sd), ptr(dr), ptr(un),
+                     N.HAR_SCALAR if mode == "scalar" else N.HAR_BATCHED, int(burn_in), int(thinning),
+                     int(n_rounds), int(counter_base), ptr(samples), ptr(status))
+    N.check(lib.art_hit_and_run(C.byref(P), C.byref(Ch), stream_handle(stream)), "art_hit_and_run")
+    samples._keepalive = (cp, sd, dr, un)
+    return samples, x, status
+
+
+_STATUS_TEXT = {1: "Empty hit-and-run step interval.", 2: "x0 is not feasible for the region.",
+                3: "too many polytope rows for the compiled kernel"}
+
+
+def _raise_status(status):
+    st = np.asarray(status)
+    bad = st[st != 0]
+    if bad.size:
+        code = int(bad[0])
+        exc = ValueError if code == 2 else RuntimeError
+        raise exc(_STATUS_TEXT.get(code, f"hit-and-run status {code}"))
+
+
+@dataclass
+class HitAndRunSampler:
+    """Hit-and-run sampler for convex polytopes A x <= b (sampling.py:432-564)."""
+
+    burn_in: int = 500
+    thinning: int = 10
+    feasibility_tol: float = 1e-10
+    max_feasible_tries: int = 20000
+    bounds: np.ndarray | None = None
+    direction_eigenvectors: np.ndarray | None = None
+    direction_eigenvalues: np.ndarray | None = None
+    direction_eigenvalue_floor: float = 1e-4
+    rng_mode: RngMode = "reference"
+
+    def sample(self, region: PolytopeRegion, n: int, random_state: RandomState = None,
+               x0: np.ndarray | None = None) -> np.ndarray:
+        if n < 0:
+            raise ValueError("n must be nonnegative.")
+        if self.burn_in < 0:
+            raise ValueError("burn_in must be nonnegative.")
+        if self.thinning < 1:
+            raise ValueError("thinning must be at least 1.")
+        rng = as_rng(random_state)
+        vecs, sqrt_vals = self._direction_spectrum(region.dimension)
+        if x0 is None:
+            x = find_feasible_point(region, bounds=self.bounds, max_tries=self.max_feasible_tries,
+                                    random_state=rng, tol=self.feasibility_tol)
+        else:
+            x = np.asarray(x0, dtype=float).reshape(-1)
+            if x.shape[0] != region.dimension:
+                raise ValueError(f"x0 must have shape ({region.dimension},), got {x.shape}.")
+            if not bool(region.contains(x, tol=self.feasibility_tol)[0]):
+                raise ValueError("x0 is not feasible for the region.")
+        n = int(n)
+        d = region.dimension
+        total = self.burn_in + n * self.thinning
+        if n == 0:
+            return np.empty((0, d))
+        polys = device_polytopes([region])
+        if self.rng_mode == "reference":
+            # the reference interleaves normal(size=d) and uniform() per step
+            dirs = np.empty((total, d))
+            unif = np.zeros(total)
+            u_i = 0
+            for step in range(total):
+                z = rng.normal(size=d)
+                if vecs is not None:
+                    z = vecs @ (sqrt_vals * z)
+                dirs[step] = z
+                if np.linalg.norm(z) != 0.0:
+                    unif[u_i] = rng.uniform(0.0, 1.0)
+                    u_i += 1
+            samples, _, status = hit_and_run_device(
+                polys, [0], x[None, :], burn_in=self.burn_in, thinning=self.thinning, n_rounds=n,
+                mode="scalar", directions=dirs[None], uniforms=unif[None])
+        else:
+            if vecs is not None:
+                raise NotImplementedError("covariance-shaped directions need rng_mode='reference'")
+            seed = int(rng.integers(0, 2**63 - 1))
+            samples, _, status = hit_and_run_device(
+                polys, [0], x[None, :], burn_in=self.burn_in, thinning=self.thinning, n_rounds=n,
+                mode="scalar", seeds=[seed])
+        _raise_status(status.cpu().numpy())
+        return samples[:, 0, :].cpu().numpy()
+
+    def _direction_spectrum(self, dimension: int):
+        vecs, vals = self.direction_eigenvectors, self.direction_eigenvalues
+        if vecs is None and vals is None:
+            return None, None
+        if vecs is None or vals is None:
+            raise ValueError("direction_eigenvectors and direction_eigenvalues must be provided together.")
+        vecs = np.asarray(vecs, dtype=float)
+        vals = np.asarray(vals, dtype=float).reshape(-1)
+        if vecs.shape != (dimension, dimension) or vals.shape != (dimension,):
+            raise ValueError("direction spectrum shape mismatch")
+        if not np.allclose(vecs.T @ vecs, np.eye(dimension), rtol=1e-8, atol=1e-10):
+            raise ValueError("direction_eigenvectors must be orthonormal.")
+        safe, _ = floor_covariance_eigenvalues(vals, self.direction_eigenvalue_floor)
+        s = np.sqrt(safe)
+        return vecs, s / np.max(s)
+
+
+@dataclass
+class BatchedHitAndRunSampler(HitAndRunSampler):
+    """Several chains with incremental slacks (sampling.py:601-962), on the GPU.
+
+    Chains advance together; ``n`` samples are taken round-robin over the
+    chains exactly as the reference lays them out (round-major).
+    """
+
+    n_chains: int = 20
+    rng_mode: RngMode = "device"
+
+    def sample(self, region: PolytopeRegion, n: int, random_state: RandomState = None,
+               x0: np.ndarray | None = None) -> np.ndarray:
+        if n < 0:
+            raise ValueError("n must be nonnegative.")
+        if self.n_chains < 1:
+            raise ValueError("n_chains must be at least 1.")
+        n = int(n)
+        d = region.dimension
+        if n == 0:
+            return np.empty((0, d))
+        rng = as_rng(random_state)
+        n_chains = min(self.n_chains, n)
+        points = self._initial_points(region, n_chains, rng, x0)
+        stride = max(1, self.thinning)
+        full_rounds, remainder = divmod(n, n_chains)
+        polys = device_polytopes([region])
+        if self.rng_mode == "reference":
+            raise NotImplementedError("batched chains use device draws; inject draws via hit_and_run_device")
+        vecs, _ = self._direction_spectrum(d)
+        if vecs is not None:
+            raise NotImplementedError("covariance-shaped directions need the scalar sampler in reference mode")
+        seeds = rng.integers(0, 2**63 - 1, size=n_chains, dtype=np.int64).astype(np.uint64)
+        rounds = full_rounds + (1 if remainder else 0)
+        samples, _, status = hit_and_run_device(
+            polys, np.zeros(n_chains, np.int32), points, burn_in=self.burn_in, thinning=stride,
+            n_rounds=rounds, mode="batched", seeds=seeds)
+        _raise_status(status.cpu().numpy())
+        return samples.reshape(-1, d)[:n].cpu().numpy()
+
+    def _initial_points(self, region, n_chains, rng, x0):
+        """sampling.py:826-862."""
+
+        if x0 is None:
+            seed = find_feasible_point(region, bounds=self.bounds, max_tries=self.max_feasible_tries,
+                                       random_state=rng, tol=self.feasibility_tol)
+            return np.repeat(seed[None, :], n_chains, axis=0)
+        cands = np.asarray(x0, dtype=float)
+        if cands.ndim == 1:
+            cands = cands[None, :]
+        if cands.ndim != 2 or cands.shape[1] != region.dimension:
+            raise ValueError("x0 must have shape (d,) or (n_points, d)")
+        if cands.shape[0] == 0:
+            raise ValueError("x0 must contain at least one starting point.")
+        if not np.all(region.contains(cands, tol=self.feasibility_tol)):
+            raise ValueError("All x0 candidates must be feasible for the region.")
+        idx = rng.choice(cands.shape[0], size=n_chains, replace=cands.shape[0] < n_chains)
+        return cands[idx].copy()
+
+
+@dataclass
+class NumbaBatchedHitAndRunSampler(BatchedHitAndRunSampler):
+    """Name kept from the reference (sampling.py:965-970); runs the same GPU chains."""
+
+
+@dataclass
+class ParallelNumbaBatchedHitAndRunSampler(NumbaBatchedHitAndRunSampler):
+    """Name kept from the reference (sampling.py:973-1025); runs the same GPU chains."""
+
+    n_chains: int = 50
+    parallel_random: bool = True
+    random_threads: int = 10
+
+
+@dataclass
+class UniformBoxSampler:
+    """Exact uniform sampler for axis-aligned boxes (sampling.py:130-142)."""
+
+    def sample(self, domain: BoxDomain, n: int, random_state: RandomState = None, x0=None) -> np.ndarray:
+        del x0
+        return sample_uniform_box(domain.bounds, n, random_state=random_state)

@@ -27,6 +27,7 @@ namespace art {
 // ====================================================================== plan
 __device__ __forceinline__ int plan_class(const RidgeArgs& a, int p) {
   if (a.precision == ART_PRECISION_MIXED && p >= kTensorMinP) return CLS_TENSOR;
+  if (a.gram_out) return -1;  // Gram-only calls cover tensor-class systems only
   return (p + 1 <= kSmallMaxAug) ? CLS_SMALL : CLS_LARGE;
 }
 
@@ -52,7 +53,12 @@ __global__ void ridge_plan_hist(RidgeArgs a, RidgeLists L) {
     for (int i = 0; i < a.pmax; ++i) a.beta[k * a.beta_stride + i] = nan;
     return;
   }
-  atomicAdd(&L.hist[plan_class(a, p) * kBuckets + plan_bucket(n, p)], 1);
+  const int c = plan_class(a, p);
+  if (c < 0) {
+    a.status[k] = -4;
+    return;
+  }
+  atomicAdd(&L.hist[c * kBuckets + plan_bucket(n, p)], 1);
 }
 
 __global__ void ridge_plan_scan(RidgeLists L) {
@@ -82,6 +88,7 @@ __global__ void ridge_plan_scatter(RidgeArgs a, RidgeLists L) {
   const int64_t n = a.row_offsets[k + 1] - a.row_offsets[k];
   if (d < 1 || d > a.dmax || p < 1 || p > a.pmax || n < 0) return;
   const int c = plan_class(a, p), b = plan_bucket(n, p);
+  if (c < 0) return;
   const int slot = atomicSub(&L.hist[c * kBuckets + b], 1) - 1;
   L.list[(int64_t)c * a.K + L.start[c * kBuckets + b] + slot] = (int32_t)k;
 }
@@ -508,8 +515,8 @@ extern "C" size_t art_ridge_workspace_size(int64_t count, int32_t max_features) 
   return ws_layout(count).total;
 }
 
-extern "C" int art_ridge_batched(const ArtRidgeProblem* pr, const ArtRidgeResult* res,
-                                 void* workspace, size_t ws_bytes, art_stream_t stream) {
+static int ridge_entry(const ArtRidgeProblem* pr, const ArtRidgeResult* res, float* gram_out,
+                       int64_t gram_stride, void* workspace, size_t ws_bytes, art_stream_t stream) {
   if (!pr || !res) { set_error("art_ridge_batched: null problem/result"); return ART_E_INVALID; }
   const int64_t K = pr->seg.count;
   if (K < 0) { set_error("art_ridge_batched: negative count"); return ART_E_INVALID; }
@@ -574,6 +581,10 @@ extern "C" int art_ridge_batched(const ArtRidgeProblem* pr, const ArtRidgeResult
   a.beta = res->beta; a.beta_stride = res->beta_stride;
   a.ridge_eff = res->ridge_effective; a.cond = res->cond_estimate;
   a.status = res->status; a.info = res->info;
+  a.options = pr->options;
+  a.gram_out = gram_out;
+  a.gram_stride = gram_stride;
+  if (gram_out) a.precision = ART_PRECISION_MIXED;
   RidgeLists L;
   L.count = (int32_t*)(ws + wl.off_count);
   L.cursor = (int32_t*)(ws + wl.off_cursor);
@@ -598,6 +609,7 @@ extern "C" int art_ridge_batched(const ArtRidgeProblem* pr, const ArtRidgeResult
     rc = launch_ridge_tensor(a, L, s);
     if (rc) return rc;
   }
+  if (gram_out) return ART_OK;
   {
     const int pcap = std::min(a.pmax, kSmallMaxAug - 1);
     const size_t sm = fp64_layout(pcap, a.dmax, 4, 64).total;
@@ -637,4 +649,30 @@ extern "C" int art_ridge_batched(const ArtRidgeProblem* pr, const ArtRidgeResult
     if (rc) return rc;
   }
   return ART_OK;
+}
+
+extern "C" int art_ridge_batched(const ArtRidgeProblem* pr, const ArtRidgeResult* res,
+                                 void* workspace, size_t ws_bytes, art_stream_t stream) {
+  return ridge_entry(pr, res, nullptr, 0, workspace, ws_bytes, stream);
+}
+
+extern "C" int art_ridge_gram(const ArtRidgeProblem* pr, float* gram, int64_t gram_stride,
+                              int32_t* status, void* workspace, size_t ws_bytes,
+                              art_stream_t stream) {
+  if (!pr || !gram || !status) { set_error("art_ridge_gram: null argument"); return ART_E_INVALID; }
+  if (pr->max_dim > ART_MAX_DIM || pr->max_features > ART_MAX_FEATURES) {
+    set_error("art_ridge_gram: max_dim <= %d and max_features <= %d required", ART_MAX_DIM,
+              ART_MAX_FEATURES);
+    return ART_E_UNSUPPORTED;
+  }
+  if (gram_stride < (int64_t)pr->max_features * (pr->max_features + 1) / 2) {
+    set_error("art_ridge_gram: gram_stride below p(p+1)/2");
+    return ART_E_INVALID;
+  }
+  // beta is not written by a Gram-only call; any non-null pointer satisfies validation
+  ArtRidgeResult res{};
+  res.beta = (double*)gram;
+  res.beta_stride = pr->max_features;
+  res.status = status;
+  return ridge_entry(pr, &res, gram, gram_stride, workspace, ws_bytes, stream);
 }

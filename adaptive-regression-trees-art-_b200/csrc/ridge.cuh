@@ -45,6 +45,9 @@ struct RidgeArgs {
   double* cond;
   int32_t* status;
   uint32_t* info;
+  uint32_t options;
+  float* gram_out;        // art_ridge_gram: packed tensor-core Grams
+  int64_t gram_stride;
 };
 
 struct RidgeLists {

@@ -107,7 +107,7 @@ struct TcLayout {
   size_t x[2], y[2], w[2], q, sq, op, bars, tmem, gram, vec, fidx, total;
 };
 __host__ __device__ inline size_t a16(size_t v) { return (v + 15) & ~(size_t)15; }
-__host__ __device__ inline TcLayout tc_layout(int pmax, int dmax) {
+__host__ __device__ inline TcLayout tc_layout(int pmax, int dmax, int factor_bytes) {
   TcLayout L;
   size_t o = 0;
   for (int s = 0; s < 2; ++s) {
@@ -121,7 +121,7 @@ __host__ __device__ inline TcLayout tc_layout(int pmax, int dmax) {
   L.op = o; o = a16(o + (size_t)4 * kOpBytes);     // 2 stages x (hi, lo)
   L.bars = o; o = a16(o + 4 * 8);
   L.tmem = o; o = a16(o + 16);
-  L.gram = o; o = a16(o + (size_t)pmax * (pmax + 1) / 2 * 4);
+  L.gram = o; o = a16(o + (size_t)pmax * (pmax + 1) / 2 * factor_bytes);
   L.vec = o; o = a16(o + (size_t)7 * (pmax + 1) * 8);
   L.fidx = o; o = a16(o + (size_t)kPmax * 4);
   L.total = o;
@@ -138,16 +138,17 @@ struct TcState {
   uint32_t mma_waits[2];
 };
 
-__global__ void __launch_bounds__(kTcThreads, 2) ridge_tc_kernel(RidgeArgs a, RidgeLists L,
+template <typename TF>
+__global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_kernel(RidgeArgs a, RidgeLists L,
                                                                  uint32_t tmem_cols) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ int s_item, s_fail, s_flag;
   __shared__ double s_scalar[8];
-  const TcLayout lay = tc_layout(a.pmax, a.dmax);
+  const TcLayout lay = tc_layout(a.pmax, a.dmax, (int)sizeof(TF));
   uint64_t* load_bar = (uint64_t*)(smem + lay.bars);
   uint64_t* mma_bar = load_bar + 2;
   uint32_t* s_tmem = (uint32_t*)(smem + lay.tmem);
-  float* Gf = (float*)(smem + lay.gram);
+  TF* Gf = (TF*)(smem + lay.gram);
   double* vec = (double*)(smem + lay.vec);
   int16_t* fidx = (int16_t*)(smem + lay.fidx);
   double* sq_q = (double*)(smem + lay.q);
@@ -337,7 +338,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) ridge_tc_kernel(RidgeArgs a, Ri
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           const int col = cb + j;
-          if (row < p && col <= row) Gf[pk(row, col)] = v[j];
+          if (row < p && col <= row) Gf[pk(row, col)] = (TF)v[j];
         }
       }
       if (two) {
@@ -348,12 +349,20 @@ __global__ void __launch_bounds__(kTcThreads, 2) ridge_tc_kernel(RidgeArgs a, Ri
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
             const int col = 128 + cb + j;
-            if (frow >= 128 && frow < p && col <= frow) Gf[pk(frow, col)] = v[j];
+            if (frow >= 128 && frow < p && col <= frow) Gf[pk(frow, col)] = (TF)v[j];
           }
         }
       }
     }
     tc_fence_before();
+    if (a.gram_out) {  // Gram-only call: dump the tensor-core Gram and move on
+      __syncthreads();
+      const int E = p * (p + 1) / 2;
+      for (int e = tid; e < E; e += kTcThreads) a.gram_out[(int64_t)k * a.gram_stride + e] = (float)Gf[e];
+      if (tid == 0) a.status[k] = 0;
+      __syncthreads();
+      continue;
+    }
     // ---- reduce exact h and diag over the row octets (fixed order)
     double* red = (double*)op;  // operand buffers are idle now
     const int nitems = P16 * (kKC / 8);
@@ -399,14 +408,14 @@ __global__ void __launch_bounds__(kTcThreads, 2) ridge_tc_kernel(RidgeArgs a, Ri
       if (tid == 0) push_list(L, a.K, CLS_RESOLVE, k);
       continue;
     }
-    for (int f = tid; f < p; f += kTcThreads) Gf[pk(f, f)] = (float)(dg[f] + lam);
+    for (int f = tid; f < p; f += kTcThreads) Gf[pk(f, f)] = (TF)(dg[f] + lam);
     __syncthreads();
     const bool want_cond = (a.cond != nullptr) || (a.solver == ART_SOLVER_AUTO);
     if (want_cond && warp == 0) {
       const double an = warp_sym_norm1(Gf, p);
       if (lane == 0) s_scalar[1] = an;
     }
-    const int fail = chol_packed<float, 8>(Gf, p, &s_fail);
+    const int fail = chol_packed<TF, 8>(Gf, p, &s_fail);
     if (fail) {
       if (tid == 0) push_list(L, a.K, CLS_RESOLVE, k);
       continue;
@@ -422,7 +431,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) ridge_tc_kernel(RidgeArgs a, Ri
     double nd_prev = 0.0;
     int outcome = 0;  // 1 converged, 2 stalled/failed
     uint32_t info = 0;
+    int passes = 0;
     for (int iter = 0; iter < kMaxRefine && outcome == 0; ++iter) {
+      passes = iter;
       if (iter > 0) {
         // r = h - lambda beta - sum_k q_k (phi_k . beta) phi_k, in FP64 from the rows.
         // Phase 1: one warp per row, lane l owns features l + 32 m (m < 5).
@@ -474,8 +485,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) ridge_tc_kernel(RidgeArgs a, Ri
       if (warp == 0) {
         for (int f = lane; f < p; f += 32) v1[f] = r[f];
         __syncwarp();
-        warp_forward<float, double>(Gf, v1, p);
-        warp_backward<float, double>(Gf, v1, p);
+        warp_forward<TF, double>(Gf, v1, p);
+        warp_backward<TF, double>(Gf, v1, p);
         double nd = 0.0, nb = 0.0;
         for (int f = lane; f < p; f += 32) {
           const double b = beta[f] + v1[f];
@@ -499,14 +510,18 @@ __global__ void __launch_bounds__(kTcThreads, 2) ridge_tc_kernel(RidgeArgs a, Ri
       outcome = s_flag;
       if (outcome == 3) { outcome = 1; info |= ART_INFO_REFINE_CAP; }
     }
+    info |= (uint32_t)min(passes, 255) << ART_INFO_REFINE_SHIFT;
     if (outcome != 1) {
-      if (tid == 0) push_list(L, a.K, CLS_RESOLVE, k);
+      if (tid == 0) {
+        push_list(L, a.K, CLS_RESOLVE, k);
+        if (a.info) a.info[k] = info;  // the FP64 form ORs its own bits in
+      }
       continue;
     }
     double cond = __longlong_as_double(0x7ff8000000000000ll);
     if (want_cond) {
       if (warp == 0) {
-        const double est = warp_inv_norm1_estimate<float>(Gf, p, v1, v2);
+        const double est = warp_inv_norm1_estimate<TF>(Gf, p, v1, v2);
         if (lane == 0) {
           const double an = s_scalar[1];
           s_scalar[2] = (est > 0.0 && isfinite(est) && an > 0.0) ? 1.0 / (an * est) : 0.0;
@@ -542,31 +557,26 @@ __global__ void __launch_bounds__(kTcThreads, 2) ridge_tc_kernel(RidgeArgs a, Ri
   if (warp == 0) tmem_dealloc(tmem, tmem_cols);
 }
 
-}  // namespace
-
-int launch_ridge_tensor(const RidgeArgs& a, const RidgeLists& L, cudaStream_t s) {
-  if (a.dmax > ART_MAX_DIM) {
-    set_error("mixed precision requires max_dim <= %d", ART_MAX_DIM);
-    return ART_E_UNSUPPORTED;
-  }
+template <typename TF>
+int launch_tc(const RidgeArgs& a, const RidgeLists& L, cudaStream_t s, const char* name) {
+  auto kern = ridge_tc_kernel<TF>;
   const int P16 = (std::min(a.pmax, kPmax) + 15) & ~15;
   const int cols_needed = P16 + (P16 > 128 ? P16 - 128 : 0);
   uint32_t cols = 32;
   while ((int)cols < cols_needed) cols <<= 1;
-  size_t smem = tc_layout(a.pmax, a.dmax).total;
+  size_t smem = tc_layout(a.pmax, a.dmax, (int)sizeof(TF)).total;
   // TMEM: CTAs resident on one SM must fit 512 columns together; widen the
   // shared-memory request if occupancy would allow more CTAs than that.
   const int max_ctas = (int)(512 / cols);
   int occ = 0;
   for (;;) {
-    if (cudaFuncSetAttribute(ridge_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess) {
       cudaGetLastError();
-      set_error("ridge_tc: cannot reserve %zu bytes of shared memory", smem);
+      set_error("%s: cannot reserve %zu bytes of shared memory", name, smem);
       return ART_E_UNSUPPORTED;
     }
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ridge_tc_kernel, kTcThreads, smem) !=
-        cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kTcThreads, smem) != cudaSuccess) {
       cudaGetLastError();
       occ = 0;
     }
@@ -574,15 +584,27 @@ int launch_ridge_tensor(const RidgeArgs& a, const RidgeLists& L, cudaStream_t s)
     smem += 8 * 1024;
   }
   if (occ > max_ctas || occ < 1) {
-    set_error("ridge_tc: cannot place CTAs within TMEM capacity (occ %d, cols %u)", occ, cols);
+    set_error("%s: cannot place CTAs within TMEM capacity (occ %d, cols %u)", name, occ, cols);
     return ART_E_UNSUPPORTED;
   }
   const int64_t grid = std::min<int64_t>((int64_t)device_sm_count() * occ, a.K);
-  prof_begin("ridge_tc", s);
-  ridge_tc_kernel<<<(unsigned)std::max<int64_t>(grid, 1), kTcThreads, smem, s>>>(a, L, cols);
+  prof_begin(name, s);
+  kern<<<(unsigned)std::max<int64_t>(grid, 1), kTcThreads, smem, s>>>(a, L, cols);
   prof_end(s);
   count_launch();
-  return check_launch("ridge_tc");
+  return check_launch(name);
+}
+
+}  // namespace
+
+int launch_ridge_tensor(const RidgeArgs& a, const RidgeLists& L, cudaStream_t s) {
+  if (a.dmax > ART_MAX_DIM) {
+    set_error("mixed precision requires max_dim <= %d", ART_MAX_DIM);
+    return ART_E_UNSUPPORTED;
+  }
+  if ((a.options & ART_RIDGE_OPT_FP64_FACTOR) && !a.gram_out)
+    return launch_tc<double>(a, L, s, "ridge_tc<f64 factor>");
+  return launch_tc<float>(a, L, s, "ridge_tc");
 }
 
 }  // namespace art

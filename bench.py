@@ -49,6 +49,10 @@ def parse():
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--cpu-per-class", type=int, default=48,
                     help="systems per feature class in the timed CPU sample")
+    ap.add_argument("--fp64-factor", action="store_true",
+                    help="mixed form factors the tensor-core Gram in FP64")
+    ap.add_argument("--variants", action="store_true",
+                    help="also time the other mixed-form factorisation variant")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -282,20 +286,21 @@ def run_b200(args):
     ridge = torch.from_numpy(wl.ridge).to(dev)
     stream = torch.cuda.current_stream()
 
-    def solve(precision, out=None):
+    def solve(precision, out=None, fp64_factor=None):
         return solve_weighted_ridge_batched(
             wl.x, wl.y, wl.w, ro, dims, kinds, ridge, x_offsets=xo, precision=precision,
-            max_features=wl.max_features, max_dim=wl.max_dim, out=out)
+            max_features=wl.max_features, max_dim=wl.max_dim, out=out,
+            fp64_factor=args.fp64_factor if fp64_factor is None else fp64_factor)
 
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
 
-    def timed(precision):
+    def timed(precision, fp64_factor=None):
         out = None
         for _ in range(args.warmup):
-            out = solve(precision, out)
+            out = solve(precision, out, fp64_factor)
         barrier()
         N.profile_reset()
         N.profile_enable(True)
@@ -303,7 +308,7 @@ def run_b200(args):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(args.steps):
-            out = solve(precision, out)
+            out = solve(precision, out, fp64_factor)
         e1.record(stream)
         barrier()
         N.profile_enable(False)
@@ -318,6 +323,13 @@ def run_b200(args):
 
     # plain FP64 form (the >=5x comparison point), then the headline form
     plain_ms, _, plain_prof, plain_out = timed("fp64")
+    variants = {}
+    if args.variants and args.precision == "mixed":
+        v_ms, _, v_prof, v_out = timed("mixed", not args.fp64_factor)
+        v_info = v_out.info.cpu().numpy()
+        variants["fp64_factor" if not args.fp64_factor else "fp32_factor"] = {
+            "ms_per_step": v_ms, "resolve_fraction": float(np.mean((v_info & N.INFO_FP64_RESOLVE) != 0)),
+            "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in v_prof.items()}}
     with Clocks(gpu_id_for(local)) as clocks:
         ms, launches, prof, out = timed(args.precision)
     clk = clocks.summary()
@@ -417,6 +429,10 @@ def run_b200(args):
                        "speedup_of_headline": plain_ms / ms},
         "status_ok_fraction": ok,
         "fp64_resolve_fraction": float(np.mean((info & N.INFO_FP64_RESOLVE) != 0)),
+        "mean_refine_passes_tensor_class": float(np.mean(((info >> N.INFO_REFINE_SHIFT) & 255)[p_all >= 33])),
+        "fp64_factor": bool(args.fp64_factor),
+        "variants": variants,
+        "plain_kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in plain_prof.items()},
         "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()},
         "clocks": clk,
         "e2e": e2e,

@@ -86,6 +86,8 @@ typedef struct CUstream_st* art_stream_t; /* == cudaStream_t */
 #define ART_INFO_FP64_RESOLVE 8u       /* mixed form re-solved in FP64         */
 #define ART_INFO_REFINE_CAP 16u        /* refinement hit its iteration cap     */
 #define ART_INFO_COND_FAILED 32u       /* condition estimate failed            */
+/* bits 8..15: FP64 refinement passes used by the mixed form (0 otherwise)  */
+#define ART_INFO_REFINE_SHIFT 8
 
 /* ---- limits ------------------------------------------------------------- */
 #define ART_MAX_FEATURES 160   /* p = features per system (ridge, split fits) */
@@ -123,7 +125,14 @@ typedef struct ArtRidgeProblem {
   double auto_rcond_threshold; /* models.py:20 default 1e-10                */
   int32_t max_features;   /* host-known upper bound of p over the batch     */
   int32_t max_dim;        /* host-known upper bound of d (0: use max_features) */
+  uint32_t options;       /* ART_RIDGE_OPT_* bits                           */
+  int32_t reserved;
 } ArtRidgeProblem;
+
+/* Mixed form: factor the tensor-core Gram in FP64 instead of FP32 (fewer
+   systems fall back to the FP64 form on ill-conditioned data; one CTA per
+   SM instead of two).                                                        */
+#define ART_RIDGE_OPT_FP64_FACTOR 1u
 
 typedef struct ArtRidgeResult {
   double* beta;            /* device [K * beta_stride]; NaN on failure     */
@@ -135,6 +144,16 @@ typedef struct ArtRidgeResult {
 } ArtRidgeResult;
 
 ART_API size_t art_ridge_workspace_size(int64_t count, int32_t max_features);
+/* Weighted Grams only, by the mixed form's tensor-core path: for every system
+ * with 33 <= p <= 160 and d <= ART_MAX_DIM, G' = sum_k q_k phi_k phi_k^T from
+ * BF16 hi/lo split products accumulated in FP32, written as the packed lower
+ * triangle (row i holds G'[i][0..i]) at gram + k * gram_stride (floats), with
+ * status[k] = 0; other systems get status -4.  The GPU Gram / host solve
+ * split of the reference's hybrid optimizer (art/_cuda_hybrid_gram.py:115-169)
+ * and the accuracy probe of the mixed form.                                  */
+ART_API int art_ridge_gram(const ArtRidgeProblem* problem, float* gram, int64_t gram_stride,
+                           int32_t* status, void* workspace, size_t workspace_bytes,
+                           art_stream_t stream);
 ART_API int art_ridge_batched(const ArtRidgeProblem* problem, const ArtRidgeResult* result,
                       void* workspace, size_t workspace_bytes, art_stream_t stream);
 

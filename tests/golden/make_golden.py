@@ -164,6 +164,101 @@ def split_cases(ref):
     print("split cases:", len(SPLIT_SPECS))
 
 
+def har_polytope(rng, d, k):
+    """Box [-1,1]^d cut by k halfspaces a.x <= a.c + r with a Chebyshev ball at c."""
+    c = rng.uniform(-0.5, 0.5, d)
+    A = rng.normal(size=(k, d))
+    A /= np.linalg.norm(A, axis=1, keepdims=True)
+    r = rng.uniform(0.05, 0.5, k)
+    return A, A @ c + r, c
+
+
+class FixedStream:
+    """Serves injected draws through the Generator calls HitAndRunSampler makes."""
+
+    def __init__(self, directions, uniforms):
+        self.directions, self.uniforms = directions, uniforms
+        self.i = self.j = 0
+
+    def normal(self, size):
+        v = self.directions[self.i].copy()
+        self.i += 1
+        return v
+
+    def uniform(self, low, high):
+        v = self.uniforms[self.j]
+        self.j += 1
+        return float(low + v * (high - low))
+
+
+def har_cases(ref):
+    import importlib
+
+    from oracle import sampling as H
+
+    numba_sampling = importlib.import_module("art_ref._numba_sampling")
+    out = {}
+    # numba batched form, chain-major injected draws
+    specs = [(201, 2, 3, 16, 5, 2, 7), (202, 8, 6, 12, 3, 4, 9), (203, 16, 10, 8, 0, 5, 6),
+             (204, 32, 12, 4, 2, 3, 5)]
+    for i, (seed, d, k, C, burn, thin, rounds) in enumerate(specs):
+        rng = np.random.default_rng(seed)
+        Ao, bo, c = har_polytope(rng, d, k)
+        Ab, bb = H.box_rows(-np.ones(d), np.ones(d))
+        A = np.vstack([Ab, Ao])
+        b = np.concatenate([bb, bo])
+        steps = burn + thin * rounds
+        x0 = np.repeat(c[None, :], C, axis=0) + 0.01 * rng.uniform(-1, 1, (C, d))
+        dirs = rng.normal(size=(C, steps, d))
+        unif = rng.random(size=(C, steps))
+        pts = x0.copy()
+        slack = b[None, :] - pts @ A.T
+        cp = (dirs.reshape(-1, d) @ np.ascontiguousarray(A.T)).reshape(C, steps, -1)
+        samples = np.empty((rounds * C, d))
+        numba_sampling.sample_precomputed_chains_parallel(pts, slack, dirs, cp, unif, burn, thin, samples)
+        mine, last = H.chains_batched(A, b, x0, dirs, unif, burn, thin, rounds)
+        np.testing.assert_allclose(mine.reshape(-1, d), samples, rtol=1e-13, atol=1e-13)
+        out[f"b{i}_meta"] = np.array([d, k, C, burn, thin, rounds])
+        out[f"b{i}_Ao"], out[f"b{i}_bo"], out[f"b{i}_x0"] = Ao, bo, x0
+        out[f"b{i}_dirs"], out[f"b{i}_unif"] = dirs, unif
+        out[f"b{i}_samples"] = samples.reshape(rounds, C, d)
+    # scalar HitAndRunSampler with injected draws
+    sspecs = [(301, 2, 2, 3, 2, 12), (302, 5, 4, 0, 4, 10), (303, 12, 8, 6, 3, 8)]
+    for i, (seed, d, k, burn, thin, n) in enumerate(sspecs):
+        rng = np.random.default_rng(seed)
+        Ao, bo, c = har_polytope(rng, d, k)
+        Ab, bb = H.box_rows(-np.ones(d), np.ones(d))
+        A = np.vstack([Ab, Ao])
+        b = np.concatenate([bb, bo])
+        region = ref.domain.PolytopeRegion(A, b)
+        steps = burn + thin * n
+        dirs = rng.normal(size=(steps, d))
+        unif = rng.random(size=steps)
+        stream = FixedStream(dirs, unif)
+        old = ref.sampling.as_rng
+        ref.sampling.as_rng = lambda _: stream
+        try:
+            samples = ref.sampling.HitAndRunSampler(burn_in=burn, thinning=thin).sample(region, n, x0=c)
+        finally:
+            ref.sampling.as_rng = old
+        mine = H.chain_scalar(A, b, c, dirs, unif, burn, thin, n)
+        np.testing.assert_allclose(mine, samples, rtol=1e-13, atol=1e-13)
+        out[f"s{i}_meta"] = np.array([d, k, burn, thin, n])
+        out[f"s{i}_Ao"], out[f"s{i}_bo"], out[f"s{i}_x0"] = Ao, bo, c
+        out[f"s{i}_dirs"], out[f"s{i}_unif"] = dirs, unif
+        out[f"s{i}_samples"] = samples
+    # autocorrelation estimator
+    series = np.cumsum(np.random.default_rng(7).normal(size=(300, 3)), axis=0)
+    lags = (1, 2, 5, 10, 50)
+    acf = ref.sampling.autocorrelation_by_lag(series, lags)
+    np.testing.assert_allclose(H.autocorrelation_by_lag(series, lags), acf, rtol=1e-13, atol=1e-13)
+    out["acf_series"], out["acf_lags"], out["acf"] = series, np.array(lags), acf
+    out["batched_count"] = np.array(len(specs))
+    out["scalar_count"] = np.array(len(sspecs))
+    np.savez_compressed(HERE / "har_golden.npz", **out)
+    print("har cases:", len(specs), len(sspecs))
+
+
 def main():
     root = Path(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ART_REFERENCE", ""))
     if not (root / "art" / "__init__.py").exists():
