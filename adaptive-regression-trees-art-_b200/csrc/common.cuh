@@ -20,6 +20,7 @@ int check_launch(const char* what);
 // Profiling brackets around one kernel launch (no-ops unless enabled).
 void prof_begin(const char* name, cudaStream_t s);
 void prof_end(cudaStream_t s);
+int device_sm_count();
 
 constexpr int kWarp = 32;
 

@@ -38,7 +38,12 @@ constexpr int kGroups = kPmax / 8;         // 8-feature core-matrix groups
 constexpr int kLBO = 128;                  // bytes between K-adjacent core matrices
 constexpr int kSBO = (kKC / 8) * 128;      // bytes between 8-feature groups
 constexpr int kOpBytes = kGroups * kSBO;   // one operand array (hi or lo)
-constexpr int kMaxRefine = 10;
+constexpr int kMaxRefine = 14;
+// TMEM accumulation chains are restarted every kDrainChunks stages: the
+// FP32 accumulator of the tensor core loses low bits on every step, so the
+// chain length bounds the Gram error (~steps * 2^-24 relative); drained
+// partial Grams are summed in shared memory with round-to-nearest adds.
+constexpr int kDrainChunks = 8;
 
 // ------------------------------------------------------------- PTX wrappers
 __device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t ncols) {
@@ -303,7 +308,7 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
           for (int prod = 0; prod < 3; ++prod) {
             const uint32_t A = (prod == 2) ? lb : hb;
             const uint32_t B = (prod == 1) ? lb : hb;
-            const uint32_t acc = (c == 0 && s == 0 && prod == 0) ? 0u : 1u;
+            const uint32_t acc = ((c % kDrainChunks) == 0 && s == 0 && prod == 0) ? 0u : 1u;
             mma_bf16(tmem, smem_desc(A + ko), smem_desc(B + ko), id1, acc);
             if (two)
               mma_bf16(tmem + (uint32_t)N1, smem_desc(A + (uint32_t)g0 * kSBO + ko),
@@ -313,46 +318,58 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
         mma_commit(&mma_bar[st]);
       }
       S.mma_commits[st]++;
-    }
-    // all MMAs of this system complete
-    bool ok = !abort;
-    for (int st = 0; st < 2; ++st)
-      while (S.mma_waits[st] < S.mma_commits[st]) {
-        ok = mbar_wait(&mma_bar[st], S.mma_waits[st] & 1) && ok;
-        S.mma_waits[st]++;
-      }
-    if (!__syncthreads_and(ok) || abort) {
-      abort = true;
-      if (tid == 0) { atomicExch(L.err, 1); a.status[k] = -5; }
-      break;
-    }
-    tc_fence_after();
-    // ---- drain the FP32 Gram from TMEM into packed lower storage
-    {
-      const int sp = warp & 3, half = warp >> 2;
-      const int row = 32 * sp + lane;
-      const uint32_t lane_base = tmem + ((uint32_t)(32 * sp) << 16);
-      for (int cb = half * 16; cb < N1; cb += 32) {
-        float v[16];
-        tmem_ld16(lane_base + (uint32_t)cb, v);
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int col = cb + j;
-          if (row < p && col <= row) Gf[pk(row, col)] = (TF)v[j];
-        }
-      }
-      if (two) {
-        const int frow = g0 * 8 + row;
-        for (int cb = half * 16; cb < N2; cb += 32) {
+      const bool seg_end = ((c + 1) % kDrainChunks) == 0 || c + 1 == nchunks;
+      if (seg_end) {
+        // wait for every MMA of this segment, then add the partial Gram from TMEM
+        bool okw = true;
+        for (int s2 = 0; s2 < 2; ++s2)
+          while (S.mma_waits[s2] < S.mma_commits[s2]) {
+            okw = mbar_wait(&mma_bar[s2], S.mma_waits[s2] & 1) && okw;
+            S.mma_waits[s2]++;
+          }
+        if (!__syncthreads_and(okw)) { abort = true; break; }
+        tc_fence_after();
+        const bool first = c < kDrainChunks;
+        const int sp = warp & 3, half = warp >> 2;
+        const int row = 32 * sp + lane;
+        const uint32_t lane_base = tmem + ((uint32_t)(32 * sp) << 16);
+        for (int cb = half * 16; cb < N1; cb += 32) {
           float v[16];
-          tmem_ld16(lane_base + (uint32_t)(N1 + cb), v);
+          tmem_ld16(lane_base + (uint32_t)cb, v);
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
-            const int col = 128 + cb + j;
-            if (frow >= 128 && frow < p && col <= frow) Gf[pk(frow, col)] = (TF)v[j];
+            const int col = cb + j;
+            // lower entries of tile 1, plus its upper block G[row < 128][col >= 128],
+            // which is the transpose of the lower-left block of features >= 128
+            if (row < p && col < p && (col <= row || col >= 128)) {
+              TF* gp = (col <= row) ? &Gf[pk(row, col)] : &Gf[pk(col, row)];
+              *gp = first ? (TF)v[j] : *gp + (TF)v[j];
+            }
           }
         }
+        if (two) {
+          const int frow = g0 * 8 + row;
+          for (int cb = half * 16; cb < N2; cb += 32) {
+            float v[16];
+            tmem_ld16(lane_base + (uint32_t)(N1 + cb), v);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              const int col = 128 + cb + j;
+              if (frow >= 128 && frow < p && col <= frow) {
+                TF* gp = &Gf[pk(frow, col)];
+                *gp = first ? (TF)v[j] : *gp + (TF)v[j];
+              }
+            }
+          }
+        }
+        tc_fence_before();
+        __syncthreads();
       }
+    }
+    if (abort || !__syncthreads_and(!abort)) {
+      if (tid == 0) { atomicExch(L.err, 1); a.status[k] = -5; }
+      abort = true;
+      break;
     }
     tc_fence_before();
     if (a.gram_out) {  // Gram-only call: dump the tensor-core Gram and move on
@@ -446,39 +463,41 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
           fb_r[m] = f < p ? fidx[2 * f + 1] : -1;
           b_r[m] = f < p ? beta[f] : 0.0;
         }
-        const int ia2 = tid < p ? fidx[2 * tid] : -3, ib2 = tid < p ? fidx[2 * tid + 1] : -1;
-        double accf = 0.0;
+        // per-lane accumulators of sum_k q_k e_k phi_f for the lane's features
+        double acc_r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
         for (int64_t c0 = 0; c0 < it.n; c0 += KR) {
           const int rows = (int)min((int64_t)KR, it.n - c0);
           for (int e = tid; e < rows * d; e += kTcThreads) {
             const int rr = e / d, cc = e - rr * d;
             xr[rr * dp + cc] = a.x[it.xoff + (c0 + rr) * d + cc];
           }
+          for (int rr = tid; rr < rows; rr += kTcThreads)
+            se[rr] = fmax(a.w ? a.w[it.r0 + c0 + rr] : 1.0, a.weight_floor);
           __syncthreads();
           for (int rr = warp; rr < rows; rr += kTcThreads / 32) {
             const double* xk = xr + rr * dp;
+            double ph[5];
             double e_ = 0.0;
 #pragma unroll
             for (int m = 0; m < 5; ++m) {
-              if (fa_r[m] != -3)
-                e_ = fma((fa_r[m] < 0 ? 1.0 : xk[fa_r[m]]) * (fb_r[m] < 0 ? 1.0 : xk[fb_r[m]]),
-                         b_r[m], e_);
+              ph[m] = fa_r[m] == -3 ? 0.0
+                                    : (fa_r[m] < 0 ? 1.0 : xk[fa_r[m]]) * (fb_r[m] < 0 ? 1.0 : xk[fb_r[m]]);
+              e_ = fma(ph[m], b_r[m], e_);
             }
-            e_ = warp_sum(e_);
-            if (lane == 0) {
-              const double wv = a.w ? a.w[it.r0 + c0 + rr] : 1.0;
-              se[rr] = fmax(wv, a.weight_floor) * e_;
-            }
-          }
-          __syncthreads();
-          if (tid < p) {
-            for (int rr = 0; rr < rows; ++rr) {
-              const double* xk = xr + rr * dp;
-              accf = fma(se[rr], (ia2 < 0 ? 1.0 : xk[ia2]) * (ib2 < 0 ? 1.0 : xk[ib2]), accf);
-            }
+            e_ = warp_sum(e_) * se[rr];
+#pragma unroll
+            for (int m = 0; m < 5; ++m) acc_r[m] = fma(e_, ph[m], acc_r[m]);
           }
           __syncthreads();
         }
+        // reduce the 8 warps' partial sums in a fixed order
+        double* part = xr;  // reuse: [warp][160]
+#pragma unroll
+        for (int m = 0; m < 5; ++m) part[warp * kPmax + lane + 32 * m] = acc_r[m];
+        __syncthreads();
+        double accf = 0.0;
+        if (tid < p)
+          for (int ww = 0; ww < kTcThreads / 32; ++ww) accf += part[ww * kPmax + tid];
         if (tid < p) r[tid] = h[tid] - lam * beta[tid] - accf;
         __syncthreads();
       }
@@ -500,7 +519,7 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
           int out = 0;
           if (!(nd <= 1e300) || !(nb <= 1e300)) out = 2;           // non-finite
           else if (nd <= 2.3e-16 * nb) out = 1;                     // at working precision
-          else if (iter >= 1 && nd > 0.5 * nd_prev) out = (nd <= 1e-12 * nb) ? 1 : 2;
+          else if (iter >= 1 && nd > 0.75 * nd_prev) out = (nd <= 1e-12 * nb) ? 1 : 2;
           else if (iter == kMaxRefine - 1) out = (nd <= 1e-12 * nb) ? 3 : 2;
           s_flag = out;
         }

@@ -1,0 +1,1130 @@
+// split.cu -- soft oblique split search for a whole tree level in one launch.
+//
+// Device form of SoftObliqueSplitter.split (art/splitters.py:252-363) and
+// _optimize_from_initialization (365-601) with the objective of
+// SoftObliqueRidgeObjective (objectives.py:132-340), Armijo backtracking
+// (optimizers.py:72-121), AdaptiveAlpha (optimizers.py:20-69) and the hard
+// result (_make_hard_result, splitters.py:603-690).  The host reads results
+// once per level; every control decision (stop rules, line-search retries,
+// step-size control, last-feasible tracking, min-side fallback) is made on
+// the device.
+//
+// Work item = (node, group of Rg restarts); one CTA per item (persistent
+// queue, largest nodes first).  The restarts of a group share every pass
+// over the node's rows:
+//   gram pass   : gates pi_r = sigmoid((x.w_r - z_r)/T) and, for all 2*Rg
+//                 (restart, side) systems at once, the augmented weighted
+//                 Grams sum_k Q[k][c] P[k][e] with P = vech([phi;y][phi;y]^T)
+//                 -- one outer-product accumulation in register tiles;
+//   solve       : trace-scaled ridge + Cholesky per system (one warp each);
+//   resid pass  : loss, envelope gradient [X^T a / T, -sum a / T], n_right;
+//   trial pass  : H speculative Armijo step sizes per restart evaluated with
+//                 the frozen child models (objectives.py:145-156), accepted in
+//                 the reference's order (first passing step of the sequence
+//                 alpha0 * rho^k built by repeated multiplication).
+// A select kernel then keeps, per node, the best restart as split() does.
+#include <algorithm>
+
+#include "common.cuh"
+#include "linalg.cuh"
+
+namespace art {
+namespace {
+
+constexpr int kSplitThreads = 256;
+constexpr int kWarps = kSplitThreads / 32;
+constexpr int kCH = 32;          // rows per chunk
+constexpr int kMaxP = 64;        // child model features
+constexpr int kMaxRg = 16;       // restarts per work item
+constexpr int kRedSlots = 5;     // (restart, component) accumulators per thread
+constexpr int kBuckets = 64;
+
+struct SplitArgs {
+  int64_t K;
+  const int64_t* row_offsets;
+  const int64_t* x_offsets;
+  const int32_t* dims;
+  const int32_t* features;
+  const double* x;
+  const double* y;
+  const double* temperature;
+  const double* ridge;
+  const double* parent_loss;
+  const int8_t* fallback;
+  const double* theta0;
+  int64_t theta0_stride;
+  ArtSplitParams prm;
+  int R, Rg, groups, dmax, pmax, H, TC;
+  // per (node, restart) results, index k * R + r
+  double* r_theta;   // [.. ][dmax + 1]
+  double* r_loss;
+  double* r_beta;    // [..][2][pmax]
+  double* r_child;   // [..][2]
+  double* r_ridge;   // [..][2]
+  int32_t* r_nright;
+  int32_t* r_iters;
+  int32_t* r_stop;
+  int32_t* r_fail;
+  int32_t* r_flags;
+  int32_t* r_fbiter;
+  double* r_alpha;
+  double* tr_loss;
+  double* tr_step;
+  int32_t* tr_back;
+  double* tr_gnorm;
+  // work queue
+  int32_t* counts;   // [0] items, [1] cursor, [2..2+64) hist, [66..130) start
+  int32_t* items;    // [K * groups]
+};
+
+// Shared-memory layout for a given (dmax, pmax, Rg, H).
+struct SLayout {
+  size_t x, y, phi, q, G, cache, theta, dirn, grad, lastf, bl, br, trial, red, chol, eidx, rs,
+      total;
+};
+__host__ __device__ inline size_t al(size_t v) { return (v + 15) & ~(size_t)15; }
+__host__ __device__ inline SLayout split_layout(int dmax, int pmax, int Rg, int H) {
+  SLayout L;
+  const int pa = pmax + 1, E = pa * (pa + 1) / 2, dt = dmax + 1;
+  size_t o = 0;
+  L.x = o; o = al(o + (size_t)kCH * dmax * 8);
+  L.y = o; o = al(o + (size_t)kCH * 8);
+  L.phi = o; o = al(o + (size_t)kCH * pa * 8);
+  L.q = o; o = al(o + (size_t)kCH * 2 * Rg * 8);
+  L.G = o; o = al(o + (size_t)E * 2 * Rg * 8);
+  L.cache = o; o = al(o + (size_t)kCH * Rg * 4 * 8);
+  L.theta = o; o = al(o + (size_t)Rg * dt * 8);
+  L.dirn = o; o = al(o + (size_t)Rg * dt * 8);
+  L.grad = o; o = al(o + (size_t)Rg * dt * 8);
+  L.lastf = o; o = al(o + (size_t)Rg * dt * 8);
+  L.bl = o; o = al(o + (size_t)Rg * pmax * 8);
+  L.br = o; o = al(o + (size_t)Rg * pmax * 8);
+  L.trial = o; o = al(o + (size_t)Rg * H * 3 * 8);
+  L.red = o; o = al(o + (size_t)Rg * (dmax + 3) * 8);
+  L.chol = o; o = al(o + (size_t)kWarps * (E + 2 * pa) * 8);
+  L.eidx = o; o = al(o + (size_t)E * 2 * 2);
+  L.rs = o; o = al(o + (size_t)Rg * 32 * 8);  // per-restart scalar state
+  L.total = o;
+  return L;
+}
+
+// Per-restart scalar state, stored as doubles in smem (slot index below).
+enum RS {
+  RS_LOSS = 0, RS_DD, RS_TOL, RS_GNORM, RS_T, RS_ALPHA, RS_ASTART, RS_STEP, RS_LSVAL,
+  RS_LAML, RS_LAMR, RS_NRIGHT, RS_ACTIVE, RS_ITERS, RS_STOP, RS_FAIL, RS_FAILURES, RS_NBBASE,
+  RS_SEARCH, RS_ACCEPT, RS_NB, RS_FEASIT, RS_HASFEAS, RS_CONV, RS_FB, RS_CHOLBAD, RS_HLOSSL,
+  RS_HLOSSR, RS_PARENT, RS_COUNT_
+};
+
+struct Item {
+  int64_t r0, n, xoff;
+  int d, kind, p, pa, E;
+  double T0, ridge;
+  int k, g, rbase, rn;  // node, group, first restart, restarts in this item
+};
+
+__device__ __forceinline__ double sigm(double s) {
+  s = fmin(fmax(s, -50.0), 50.0);  // objectives.py:49-51
+  return 1.0 / (1.0 + exp(-s));
+}
+
+// Entry e of the packed lower triangle -> (i, j), i >= j.
+__device__ __forceinline__ void entry_ij(int e, int& i, int& j) {
+  i = (int)((sqrtf(8.0f * e + 1.0f) - 1.0f) * 0.5f);
+  while (i * (i + 1) / 2 > e) --i;
+  while ((i + 1) * (i + 2) / 2 <= e) ++i;
+  j = e - i * (i + 1) / 2;
+}
+
+// =========================================================== plan (LPT order)
+__global__ void split_plan_hist(SplitArgs a) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.K * a.groups) return;
+  const int64_t k = t / a.groups;
+  const int64_t n = a.row_offsets[k + 1] - a.row_offsets[k];
+  const int b = kBuckets - 1 - max(0, min(kBuckets - 1, ilogb((double)(n + 1))));
+  atomicAdd(&a.counts[2 + b], 1);
+}
+__global__ void split_plan_scan(SplitArgs a) {
+  if (threadIdx.x != 0) return;
+  int c = 0;
+  for (int b = 0; b < kBuckets; ++b) {
+    a.counts[2 + kBuckets + b] = c;
+    c += a.counts[2 + b];
+  }
+  a.counts[0] = c;
+  a.counts[1] = 0;
+}
+__global__ void split_plan_scatter(SplitArgs a) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.K * a.groups) return;
+  const int64_t k = t / a.groups;
+  const int64_t n = a.row_offsets[k + 1] - a.row_offsets[k];
+  const int b = kBuckets - 1 - max(0, min(kBuckets - 1, ilogb((double)(n + 1))));
+  const int slot = atomicSub(&a.counts[2 + b], 1) - 1;
+  a.items[a.counts[2 + kBuckets + b] + slot] = (int32_t)t;
+}
+
+// ================================================================ kernel
+template <int TC>
+struct SplitCta {
+  static constexpr int TE = 32 / TC;
+  const SplitArgs& a;
+  unsigned char* sm;
+  SLayout L;
+  Item it;
+  double *xs, *ys, *phi, *Q, *G, *cache, *th, *dn, *gr, *lf, *bl, *br, *trial, *red, *chol, *rs;
+  int16_t* eidx;
+  int tid, lane, warp;
+
+  __device__ SplitCta(const SplitArgs& a_, unsigned char* sm_) : a(a_), sm(sm_) {
+    L = split_layout(a.dmax, a.pmax, a.Rg, a.H);
+    xs = (double*)(sm + L.x); ys = (double*)(sm + L.y); phi = (double*)(sm + L.phi);
+    Q = (double*)(sm + L.q); G = (double*)(sm + L.G); cache = (double*)(sm + L.cache);
+    th = (double*)(sm + L.theta); dn = (double*)(sm + L.dirn); gr = (double*)(sm + L.grad);
+    lf = (double*)(sm + L.lastf); bl = (double*)(sm + L.bl); br = (double*)(sm + L.br);
+    trial = (double*)(sm + L.trial); red = (double*)(sm + L.red); chol = (double*)(sm + L.chol);
+    eidx = (int16_t*)(sm + L.eidx); rs = (double*)(sm + L.rs);
+    tid = threadIdx.x; lane = tid & 31; warp = tid >> 5;
+  }
+  __device__ double& S(int r, int slot) { return rs[r * 32 + slot]; }
+  __device__ int dt() const { return it.d + 1; }
+
+  // Stage rows [c0, c0 + rows) of x and y, then the augmented features.
+  __device__ int load_chunk(int64_t c0) {
+    const int rows = (int)min((int64_t)kCH, it.n - c0);
+    const int d = it.d;
+    for (int e = tid; e < rows * d; e += kSplitThreads) xs[e] = a.x[it.xoff + c0 * d + e];
+    for (int r = tid; r < rows; r += kSplitThreads) ys[r] = a.y[it.r0 + c0 + r];
+    __syncthreads();
+    const int pa = it.pa;
+    for (int e = tid; e < rows * pa; e += kSplitThreads) {
+      const int r = e / pa, f = e - r * pa;
+      double v;
+      if (f == it.p) v = ys[r];
+      else {
+        int ia, ib;
+        feature_factors(d, it.kind, f, ia, ib);
+        const double* xr = xs + r * d;
+        v = (ia < 0 ? 1.0 : xr[ia]) * (ib < 0 ? 1.0 : xr[ib]);
+      }
+      phi[r * pa + f] = v;
+    }
+    __syncthreads();
+    return rows;
+  }
+
+  __device__ double score(int r, int row) {  // x . w_r
+    const double* xr = xs + row * it.d;
+    const double* w = th + r * dt();
+    double u = 0.0;
+    for (int i = 0; i < it.d; ++i) u = fma(xr[i], w[i], u);
+    return u;
+  }
+  __device__ double fitted(const double* beta, int row) {
+    const double* pr = phi + row * it.pa;
+    double s = 0.0;
+    for (int f = 0; f < it.p; ++f) s = fma(pr[f], beta[f], s);
+    return s;
+  }
+
+  // ---- Gram pass: G[e][c] = sum_k Q[k][c] P[k][e]; hard = gates from the
+  // exact side of each row (weights 1/0, no floor), else soft gates.
+  __device__ void gram_pass(bool hard) {
+    const int E = it.E, C2 = 2 * a.Rg;
+    const int nct = (C2 + TC - 1) / TC, net = (E + TE - 1) / TE;
+    const bool mine = tid < nct * net;
+    const int ct = tid % nct, et = tid / nct;
+    int ei[TE], ej[TE];
+#pragma unroll
+    for (int u = 0; u < TE; ++u) {
+      const int e = et * TE + u;
+      if (mine && e < E) { ei[u] = eidx[2 * e]; ej[u] = eidx[2 * e + 1]; }
+      else { ei[u] = 0; ej[u] = 0; }
+    }
+    double acc[TE][TC];
+#pragma unroll
+    for (int u = 0; u < TE; ++u)
+#pragma unroll
+      for (int v = 0; v < TC; ++v) acc[u][v] = 0.0;
+    for (int64_t c0 = 0; c0 < it.n; c0 += kCH) {
+      const int rows = load_chunk(c0);
+      for (int pr = tid; pr < rows * a.Rg; pr += kSplitThreads) {
+        const int row = pr / a.Rg, r = pr - row * a.Rg;
+        double qL = 0.0, qR = 0.0;
+        if (r < it.rn && S(r, RS_ACTIVE) != 0.0) {
+          if (hard) {
+            const double* w = th + r * dt();
+            const bool right = dot2_score(xs + row * it.d, w, it.d, w[it.d]) >= 0.0;
+            qL = right ? 0.0 : 1.0;
+            qR = right ? 1.0 : 0.0;
+            // integer-valued sums below 2^53 are exact in any order
+            if (right) atomicAdd(&S(r, RS_NRIGHT), 1.0);
+          } else {
+            const double pi = sigm((score(r, row) - th[r * dt() + it.d]) / S(r, RS_T));
+            qL = fmax(1.0 - pi, a.prm.weight_floor);
+            qR = fmax(pi, a.prm.weight_floor);
+          }
+        }
+        Q[row * C2 + 2 * r] = qL;
+        Q[row * C2 + 2 * r + 1] = qR;
+      }
+      __syncthreads();
+      if (mine) {
+        for (int row = 0; row < rows; ++row) {
+          const double* pr = phi + row * it.pa;
+          const double* qr = Q + row * C2 + ct * TC;
+          double pv[TE], qv[TC];
+#pragma unroll
+          for (int u = 0; u < TE; ++u) pv[u] = pr[ei[u]] * pr[ej[u]];
+#pragma unroll
+          for (int v = 0; v < TC; ++v) qv[v] = (ct * TC + v < C2) ? qr[v] : 0.0;
+#pragma unroll
+          for (int u = 0; u < TE; ++u)
+#pragma unroll
+            for (int v = 0; v < TC; ++v) acc[u][v] = fma(pv[u], qv[v], acc[u][v]);
+        }
+      }
+      __syncthreads();
+    }
+    if (mine) {
+#pragma unroll
+      for (int u = 0; u < TE; ++u)
+#pragma unroll
+        for (int v = 0; v < TC; ++v) {
+          const int e = et * TE + u, c = ct * TC + v;
+          if (e < E && c < C2) G[(size_t)e * C2 + c] = acc[u][v];
+        }
+    }
+    __syncthreads();
+  }
+
+  // ---- trace-scaled ridge + Cholesky + solve for every (restart, side).
+  // One warp per system; a failed factorisation marks the restart.
+  __device__ void solve_all() {
+    const int p = it.p, pa = it.pa, E = it.E, C2 = 2 * a.Rg;
+    double* A = chol + (size_t)warp * (E + 2 * pa);
+    double* z = A + E;
+    for (int c = warp; c < 2 * it.rn; c += kWarps) {
+      const int r = c >> 1, side = c & 1;
+      if (S(r, RS_ACTIVE) == 0.0) continue;
+      for (int e = lane; e < E; e += 32) A[e] = G[(size_t)e * C2 + c];
+      __syncwarp();
+      double tr = 0.0;
+      if (lane == 0)
+        for (int i = 0; i < p; ++i) tr += A[pk(i, i)];
+      tr = __shfl_sync(0xffffffffu, tr, 0);
+      const double lam = it.ridge * tr / p;  // models.py:271
+      for (int i = lane; i < p; i += 32) A[pk(i, i)] += lam;
+      __syncwarp();
+      // left-looking Cholesky, lanes over rows
+      int fail = 0;
+      for (int j = 0; j < p && !fail; ++j) {
+        double s = 0.0;
+        for (int k2 = lane; k2 < j; k2 += 32) s += A[pk(j, k2)] * A[pk(j, k2)];
+        s = warp_sum(s);
+        const double djj = A[pk(j, j)] - s;
+        if (!(djj > 0.0) || !isfinite(djj)) { fail = j + 1; break; }
+        const double ljj = sqrt(djj);
+        __syncwarp();
+        if (lane == 0) A[pk(j, j)] = ljj;
+        for (int i = j + 1 + lane; i < p; i += 32) {
+          double t2 = A[pk(i, j)];
+          for (int k2 = 0; k2 < j; ++k2) t2 -= A[pk(i, k2)] * A[pk(j, k2)];
+          A[pk(i, j)] = t2 / ljj;
+        }
+        __syncwarp();
+      }
+      if (fail) {
+        if (lane == 0) S(r, RS_CHOLBAD) = 1.0;
+        __syncwarp();
+        continue;
+      }
+      for (int i = lane; i < p; i += 32) z[i] = A[pk(p, i)];  // h
+      __syncwarp();
+      warp_forward<double, double>(A, z, p);
+      warp_backward<double, double>(A, z, p);
+      double* beta = (side ? br : bl) + r * a.pmax;
+      for (int i = lane; i < p; i += 32) beta[i] = z[i];
+      if (lane == 0) S(r, side ? RS_LAMR : RS_LAML) = lam;
+      __syncwarp();
+    }
+    __syncthreads();
+  }
+
+  // ---- soft residual pass: loss, gradient, n_right for active restarts.
+  __device__ void resid_pass() {
+    const int d = it.d, comps = d + 3;  // grad_w (d), sum a, loss, n_right
+    const int pairs = a.Rg * comps;
+    double accs[kRedSlots];
+#pragma unroll
+    for (int s = 0; s < kRedSlots; ++s) accs[s] = 0.0;
+    double* coef = cache;                      // [row][r]: a_k
+    double* wl = cache + kCH * a.Rg;           // [row][r]: weighted loss term
+    double* nr = cache + 2 * kCH * a.Rg;       // [row][r]: pi >= 0.5
+    for (int64_t c0 = 0; c0 < it.n; c0 += kCH) {
+      const int rows = load_chunk(c0);
+      for (int pr = tid; pr < rows * a.Rg; pr += kSplitThreads) {
+        const int row = pr / a.Rg, r = pr - row * a.Rg;
+        double cf = 0.0, lw = 0.0, ge = 0.0;
+        if (r < it.rn && S(r, RS_ACTIVE) != 0.0) {
+          const double pi = sigm((score(r, row) - th[r * dt() + d]) / S(r, RS_T));
+          const double yv = ys[row];
+          const double eL = yv - fitted(bl + r * a.pmax, row);
+          const double eR = yv - fitted(br + r * a.pmax, row);
+          const double eL2 = eL * eL, eR2 = eR * eR;
+          lw = (1.0 - pi) * eL2 + pi * eR2;
+          cf = (eR2 - eL2) * pi * (1.0 - pi) / (double)it.n;
+          ge = pi >= 0.5 ? 1.0 : 0.0;
+        }
+        coef[row * a.Rg + r] = cf;
+        wl[row * a.Rg + r] = lw;
+        nr[row * a.Rg + r] = ge;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int s = 0; s < kRedSlots; ++s) {
+        const int q = tid + s * kSplitThreads;
+        if (q < pairs) {
+          const int r = q / comps, cp = q - r * comps;
+          double acc = accs[s];
+          for (int row = 0; row < rows; ++row) {
+            const double cv = coef[row * a.Rg + r];
+            if (cp < d) acc = fma(cv, xs[row * d + cp], acc);
+            else if (cp == d) acc += cv;
+            else if (cp == d + 1) acc += wl[row * a.Rg + r];
+            else acc += nr[row * a.Rg + r];
+          }
+          accs[s] = acc;
+        }
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int s = 0; s < kRedSlots; ++s) {
+      const int q = tid + s * kSplitThreads;
+      if (q < pairs) red[q] = accs[s];
+    }
+    __syncthreads();
+    // finalize per restart (one thread each)
+    if (tid < it.rn && S(tid, RS_ACTIVE) != 0.0) {
+      const int r = tid;
+      const double T = S(r, RS_T);
+      const double* rr = red + r * comps;
+      double* g = gr + r * dt();
+      for (int i = 0; i < d; ++i) g[i] = rr[i] / T;
+      g[d] = -rr[d] / T;
+      S(r, RS_LOSS) = rr[d + 1] / (double)it.n;
+      S(r, RS_NRIGHT) = rr[d + 2];
+      // projected gradient and its norm (splitters.py:86-98)
+      const double* w = th + r * dt();
+      double gw = 0.0;
+      for (int i = 0; i < d; ++i) gw += g[i] * w[i];
+      double* pd = dn + r * dt();
+      double nrm2 = 0.0;
+      for (int i = 0; i < d; ++i) {
+        const double pg = g[i] - gw * w[i];
+        pd[i] = -pg;
+        nrm2 += pg * pg;
+      }
+      pd[d] = -g[d];
+      nrm2 += g[d] * g[d];
+      S(r, RS_GNORM) = sqrt(nrm2);
+      double dd = 0.0;
+      for (int i = 0; i <= d; ++i) dd += g[i] * pd[i];
+      S(r, RS_DD) = dd;
+    }
+    __syncthreads();
+  }
+
+  // ---- trial pass: frozen-model losses of H step sizes per searching restart.
+  __device__ void trial_pass() {
+    const int d = it.d, H = a.H;
+    double* tal = trial;                       // [r][H] alpha
+    double* tnr = trial + a.Rg * H;            // [r][H] ||w + alpha p_w||
+    double* tf = trial + 2 * a.Rg * H;         // [r][H] accumulated loss
+    const bool mine = tid < a.Rg * H;
+    const int r = tid / H, j = tid - (tid / H) * H;
+    double f = 0.0;
+    const bool on = mine && r < it.rn && S(r, RS_SEARCH) != 0.0;
+    double alpha = 0.0, nrm = 1.0, z = 0.0, pz = 0.0, T = 1.0;
+    if (on) {
+      alpha = tal[r * H + j];
+      nrm = tnr[r * H + j];
+      z = th[r * dt() + d];
+      pz = dn[r * dt() + d];
+      T = S(r, RS_T);
+    }
+    for (int64_t c0 = 0; c0 < it.n; c0 += kCH) {
+      const int rows = load_chunk(c0);
+      for (int pr = tid; pr < rows * a.Rg; pr += kSplitThreads) {
+        const int row = pr / a.Rg, rr = pr - row * a.Rg;
+        double* cp = cache + (row * a.Rg + rr) * 4;
+        if (rr < it.rn && S(rr, RS_SEARCH) != 0.0) {
+          const double* xr = xs + row * d;
+          const double* w = th + rr * dt();
+          const double* pw = dn + rr * dt();
+          double u = 0.0, v = 0.0;
+          for (int i = 0; i < d; ++i) { u = fma(xr[i], w[i], u); v = fma(xr[i], pw[i], v); }
+          const double yv = ys[row];
+          const double eL = yv - fitted(bl + rr * a.pmax, row);
+          const double eR = yv - fitted(br + rr * a.pmax, row);
+          cp[0] = u; cp[1] = v; cp[2] = eL * eL; cp[3] = eR * eR;
+        }
+      }
+      __syncthreads();
+      if (on) {
+        for (int row = 0; row < rows; ++row) {
+          const double* cp = cache + (row * a.Rg + r) * 4;
+          const double s = ((cp[0] + alpha * cp[1]) / nrm - (z + alpha * pz)) / T;
+          const double pi = sigm(s);
+          f += (1.0 - pi) * cp[2] + pi * cp[3];
+        }
+      }
+      __syncthreads();
+    }
+    if (on) tf[r * H + j] = f / (double)it.n;
+    __syncthreads();
+  }
+
+  __device__ void record_trace(int r, int iter) {
+    const int64_t kr = (int64_t)it.k * a.R + it.rbase + r;
+    const int M = a.prm.max_iters;
+    if (a.tr_loss) a.tr_loss[kr * (M + 1) + iter] = S(r, RS_LOSS);
+    if (a.tr_gnorm) a.tr_gnorm[kr * (M + 1) + iter] = S(r, RS_GNORM);
+  }
+
+  __device__ void run(int item_id);
+};
+
+template <int TC>
+__device__ void SplitCta<TC>::run(int item_id) {
+  const ArtSplitParams& P = a.prm;
+  // ---------------------------------------------------------------- setup
+  const int k = item_id / a.groups, g = item_id - (item_id / a.groups) * a.groups;
+  it.k = k;
+  it.g = g;
+  it.r0 = a.row_offsets[k];
+  it.n = a.row_offsets[k + 1] - it.r0;
+  it.xoff = a.x_offsets[k];
+  it.d = a.dims[k];
+  it.kind = a.features[k];
+  it.p = feature_count(it.d, it.kind);
+  it.pa = it.p + 1;
+  it.E = it.pa * (it.pa + 1) / 2;
+  it.T0 = a.temperature[k];
+  it.ridge = a.ridge[k];
+  it.rbase = g * a.Rg;
+  it.rn = min(a.Rg, a.R - it.rbase);
+  const int d = it.d, n = (int)it.n;
+  const int req = max(P.min_side_points, (int)ceil(P.min_side_fraction * (double)n));
+  const bool fb_allowed = a.fallback ? a.fallback[k] != 0 : false;
+  for (int e = tid; e < it.E; e += kSplitThreads) {
+    int i, j;
+    entry_ij(e, i, j);
+    eidx[2 * e] = (int16_t)i;
+    eidx[2 * e + 1] = (int16_t)j;
+  }
+  for (int q = tid; q < a.Rg * 32; q += kSplitThreads) rs[q] = 0.0;
+  __syncthreads();
+  // initial theta: projected theta0 (splitters.py:379)
+  if (tid < it.rn) {
+    const int r = tid;
+    const int64_t kr = (int64_t)k * a.R + it.rbase + r;
+    const double* t0 = a.theta0 + kr * a.theta0_stride;
+    double* t = th + r * dt();
+    double nrm2 = 0.0;
+    for (int i = 0; i < d; ++i) nrm2 += t0[i] * t0[i];
+    const double nrm = sqrt(nrm2);
+    S(r, RS_ACTIVE) = 1.0;
+    if (!(nrm > 1e-12) || !isfinite(nrm)) {
+      S(r, RS_ACTIVE) = 0.0;
+      S(r, RS_FAIL) = ART_SPLIT_INVALID;
+    }
+    for (int i = 0; i < d; ++i) t[i] = t0[i] / nrm;
+    t[d] = t0[d];
+    S(r, RS_T) = it.T0;
+    S(r, RS_ALPHA) = fmin(fmax(P.alpha0, P.alpha_min), P.alpha_max);
+    S(r, RS_STOP) = ART_STOP_MAX_ITERS;
+    S(r, RS_FEASIT) = -1.0;
+  }
+  __syncthreads();
+  if (n == 0) {  // nothing to split
+    if (tid < it.rn) { S(tid, RS_ACTIVE) = 0.0; S(tid, RS_FAIL) = ART_SPLIT_MIN_SIDE_POINTS; }
+    __syncthreads();
+  }
+  // ---------------------------------------------------------- evaluate(theta)
+  auto evaluate = [&]() {
+    gram_pass(false);
+    solve_all();
+    if (tid < it.rn && S(tid, RS_ACTIVE) != 0.0 && S(tid, RS_CHOLBAD) != 0.0) {
+      S(tid, RS_ACTIVE) = 0.0;
+      S(tid, RS_FAIL) = ART_SPLIT_CHOLESKY_FAILURE;
+    }
+    __syncthreads();
+    resid_pass();
+  };
+  evaluate();
+  if (tid < it.rn && S(tid, RS_ACTIVE) != 0.0) {
+    const int r = tid;
+    const double g0 = S(r, RS_GNORM);
+    S(r, RS_TOL) = P.grad_atol + P.grad_rtol * g0;
+    const int nr = (int)S(r, RS_NRIGHT);
+    if (min(nr, n - nr) >= req) {
+      S(r, RS_HASFEAS) = 1.0;
+      S(r, RS_FEASIT) = 0.0;
+      for (int i = 0; i <= d; ++i) lf[r * dt() + i] = th[r * dt() + i];
+    }
+    record_trace(r, 0);
+  }
+  __syncthreads();
+  // ------------------------------------------------------------------ loop
+  for (int iter = 0; iter < P.max_iters; ++iter) {
+    // stop checks (splitters.py:424-437)
+    if (tid < it.rn) {
+      const int r = tid;
+      S(r, RS_SEARCH) = 0.0;
+      S(r, RS_ACCEPT) = 0.0;
+      if (S(r, RS_ACTIVE) != 0.0) {
+        if (S(r, RS_GNORM) <= S(r, RS_TOL)) {
+          S(r, RS_CONV) = 1.0;
+          S(r, RS_STOP) = ART_STOP_GRADIENT_TOLERANCE;
+          S(r, RS_ACTIVE) = 0.0;
+        } else if (S(r, RS_DD) >= 0.0) {
+          S(r, RS_STOP) = ART_STOP_NON_DESCENT;
+          S(r, RS_ACTIVE) = 0.0;
+        } else {
+          S(r, RS_SEARCH) = 1.0;
+          S(r, RS_FAILURES) = 0.0;
+          S(r, RS_NBBASE) = 0.0;
+          S(r, RS_ASTART) = P.adaptive_alpha ? S(r, RS_ALPHA) : P.alpha0;
+        }
+      }
+    }
+    __syncthreads();
+    // ---------------------------------------------------- line search
+    const int max_batches = (P.max_backtracks + 1 + a.H - 1) / a.H * P.max_line_search_failures + 1;
+    for (int batch = 0; batch < max_batches; ++batch) {
+      int any = 0;
+      if (tid < it.rn) any = S(tid, RS_SEARCH) != 0.0;
+      if (!__syncthreads_or(any)) break;
+      // step sizes alpha0 * rho^k by repeated multiplication (optimizers.py:104-107)
+      if (tid < it.rn && S(tid, RS_SEARCH) != 0.0) {
+        const int r = tid, H = a.H;
+        double al = S(r, RS_ASTART);
+        const int base = (int)S(r, RS_NBBASE);
+        for (int q = 0; q < base; ++q) al *= P.rho;
+        const double* w = th + r * dt();
+        const double* pw = dn + r * dt();
+        for (int j = 0; j < H; ++j) {
+          if (j > 0) al *= P.rho;
+          double nrm2 = 0.0;
+          for (int i = 0; i < d; ++i) {
+            const double v = w[i] + al * pw[i];
+            nrm2 += v * v;
+          }
+          trial[r * H + j] = al;
+          trial[a.Rg * H + r * H + j] = sqrt(nrm2);
+        }
+      }
+      __syncthreads();
+      trial_pass();
+      if (tid < it.rn && S(tid, RS_SEARCH) != 0.0) {
+        const int r = tid, H = a.H;
+        const int base = (int)S(r, RS_NBBASE);
+        const double f0 = S(r, RS_LOSS), dd = S(r, RS_DD);
+        int acc_j = -1;
+        for (int j = 0; j < H && base + j <= P.max_backtracks; ++j) {
+          const double al = trial[r * H + j];
+          const double rhs = __dadd_rn(f0, __dmul_rn(__dmul_rn(P.armijo_c, al), dd));
+          if (trial[2 * a.Rg * H + r * H + j] <= rhs) { acc_j = j; break; }
+        }
+        bool attempt_done = false, success = false;
+        double step = 0.0;
+        int nb = 0;
+        if (acc_j >= 0) {
+          attempt_done = true;
+          success = true;
+          step = trial[r * H + acc_j];
+          nb = base + acc_j;
+          S(r, RS_LSVAL) = trial[2 * a.Rg * H + r * H + acc_j];
+        } else if (base + H > P.max_backtracks) {
+          attempt_done = true;
+          const int last = P.max_backtracks - base;
+          step = trial[r * H + last];
+          nb = P.max_backtracks;
+        } else {
+          S(r, RS_NBBASE) = base + H;
+        }
+        if (attempt_done) {
+          if (P.adaptive_alpha) {  // AdaptiveAlpha.update (optimizers.py:49-66)
+            double na;
+            if (!success) na = step * P.rho;
+            else if (nb == 0) na = step * P.alpha_grow;
+            else if (nb >= P.heavy_backtrack_threshold) na = step * P.alpha_recovery;
+            else na = step / P.rho;
+            S(r, RS_ALPHA) = fmin(fmax(na, P.alpha_min), P.alpha_max);
+          }
+          if (success) {
+            S(r, RS_SEARCH) = 0.0;
+            S(r, RS_ACCEPT) = 1.0;
+            S(r, RS_STEP) = step;
+            S(r, RS_NB) = nb;
+          } else {
+            const double fails = S(r, RS_FAILURES) + 1.0;
+            S(r, RS_FAILURES) = fails;
+            int stop = -1;
+            if (!P.adaptive_alpha) stop = ART_STOP_LINE_SEARCH_FAILED;
+            else if (fails >= P.max_line_search_failures) stop = ART_STOP_MAX_LINE_SEARCH_FAILURES;
+            else if (S(r, RS_ALPHA) <= P.alpha_min) stop = ART_STOP_ALPHA_MIN_REACHED;
+            if (stop >= 0) {
+              S(r, RS_STOP) = stop;
+              S(r, RS_SEARCH) = 0.0;
+              S(r, RS_ACTIVE) = 0.0;
+            } else {
+              S(r, RS_NBBASE) = 0.0;
+              S(r, RS_ASTART) = S(r, RS_ALPHA);
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+    // restarts still searching after the batch cap stop (cannot happen with
+    // the cap above; kept as a bound on device work)
+    if (tid < it.rn && S(tid, RS_SEARCH) != 0.0) {
+      S(tid, RS_SEARCH) = 0.0;
+      S(tid, RS_ACTIVE) = 0.0;
+      S(tid, RS_STOP) = ART_STOP_MAX_LINE_SEARCH_FAILURES;
+    }
+    // commit accepted steps: theta <- project(theta + alpha d) (splitters.py:451, 497)
+    int any_acc = 0;
+    if (tid < it.rn && S(tid, RS_ACCEPT) != 0.0) {
+      any_acc = 1;
+      const int r = tid;
+      const double al = S(r, RS_STEP);
+      double* t = th + r * dt();
+      const double* pd = dn + r * dt();
+      double nrm2 = 0.0;
+      for (int i = 0; i < d; ++i) {
+        const double v = t[i] + al * pd[i];
+        t[i] = v;
+        nrm2 += v * v;
+      }
+      const double nrm = sqrt(nrm2);
+      for (int i = 0; i < d; ++i) t[i] = t[i] / nrm;
+      t[d] = t[d] + al * pd[d];
+      if (P.anneal_ratio != 1.0 && P.max_iters > 1)
+        S(r, RS_T) = it.T0 * pow(P.anneal_ratio, (double)(iter + 1) / (double)(P.max_iters - 1));
+      S(r, RS_ITERS) = iter + 1;
+      const int64_t kr = (int64_t)k * a.R + it.rbase + r;
+      if (a.tr_step) a.tr_step[kr * P.max_iters + iter] = al;
+      if (a.tr_back) a.tr_back[kr * P.max_iters + iter] = (int)S(r, RS_NB);
+    } else if (tid < it.rn) {
+      S(tid, RS_ACTIVE) = 0.0;  // stopped this iteration (reason already set)
+    }
+    if (!__syncthreads_or(any_acc)) break;
+    evaluate();
+    if (tid < it.rn && S(tid, RS_ACCEPT) != 0.0 && S(tid, RS_ACTIVE) != 0.0) {
+      const int r = tid;
+      const int nr = (int)S(r, RS_NRIGHT);
+      if (min(nr, n - nr) >= req) {
+        S(r, RS_HASFEAS) = 1.0;
+        S(r, RS_FEASIT) = (double)(iter + 1);
+        for (int i = 0; i <= d; ++i) lf[r * dt() + i] = th[r * dt() + i];
+      }
+      record_trace(r, iter + 1);
+    }
+    __syncthreads();
+  }
+  // ------------------------------------------------ finish (splitters.py:584-601)
+  if (tid < it.rn) {
+    const int r = tid;
+    if (S(r, RS_FAIL) == 0.0) {
+      S(r, RS_ACTIVE) = 1.0;  // participate in the hard passes
+      const int nr = (int)S(r, RS_NRIGHT);
+      const bool final_ok = min(nr, n - nr) >= req;
+      if (!final_ok && fb_allowed && S(r, RS_HASFEAS) != 0.0) {
+        for (int i = 0; i <= d; ++i) th[r * dt() + i] = lf[r * dt() + i];
+        S(r, RS_FB) = 1.0;
+      }
+      // re-project (splitters.py:614)
+      double* t = th + r * dt();
+      double nrm2 = 0.0;
+      for (int i = 0; i < d; ++i) nrm2 += t[i] * t[i];
+      const double nrm = sqrt(nrm2);
+      for (int i = 0; i < d; ++i) t[i] = t[i] / nrm;
+    } else {
+      S(r, RS_ACTIVE) = 0.0;
+    }
+    S(r, RS_CHOLBAD) = 0.0;
+  }
+  __syncthreads();
+  // hard partition: exact sides, right-side counts and (for refits) the hard Grams
+  if (tid < it.rn) S(tid, RS_NRIGHT) = 0.0;
+  __syncthreads();
+  gram_pass(true);
+  if (tid < it.rn && S(tid, RS_ACTIVE) != 0.0) {
+    const int nr = (int)S(tid, RS_NRIGHT);
+    if (nr < req || n - nr < req) {
+      S(tid, RS_ACTIVE) = 0.0;
+      S(tid, RS_FAIL) = ART_SPLIT_MIN_SIDE_POINTS;
+    }
+  }
+  __syncthreads();
+  if (P.hard_refit) {
+    solve_all();  // hard child models from the hard Grams
+    if (tid < it.rn && S(tid, RS_ACTIVE) != 0.0 && S(tid, RS_CHOLBAD) != 0.0) {
+      S(tid, RS_ACTIVE) = 0.0;
+      S(tid, RS_FAIL) = ART_SPLIT_CHOLESKY_FAILURE;
+    }
+    __syncthreads();
+    // hard losses: mean squared residual on each side, reduced per (restart,
+    // side) in row order
+    double sl = 0.0;
+    for (int64_t c0 = 0; c0 < it.n; c0 += kCH) {
+      const int rows = load_chunk(c0);
+      for (int pr = tid; pr < rows * a.Rg; pr += kSplitThreads) {
+        const int row = pr / a.Rg, r = pr - row * a.Rg;
+        double eL2 = 0.0, eR2 = 0.0;
+        if (r < it.rn && S(r, RS_ACTIVE) != 0.0) {
+          const double* w = th + r * dt();
+          const bool right = dot2_score(xs + row * d, w, d, w[d]) >= 0.0;
+          const double e = ys[row] - fitted((right ? br : bl) + r * a.pmax, row);
+          (right ? eR2 : eL2) = e * e;
+        }
+        cache[(row * a.Rg + r) * 2] = eL2;
+        cache[(row * a.Rg + r) * 2 + 1] = eR2;
+      }
+      __syncthreads();
+      if (tid < 2 * it.rn) {
+        const int r = tid >> 1, side = tid & 1;
+        for (int row = 0; row < rows; ++row) sl += cache[(row * a.Rg + r) * 2 + side];
+      }
+      __syncthreads();
+    }
+    if (tid < 2 * it.rn) red[tid] = sl;
+    __syncthreads();
+    if (tid < it.rn && S(tid, RS_ACTIVE) != 0.0) {
+      const int r = tid;
+      const int nr = (int)S(r, RS_NRIGHT), nl = n - nr;
+      const double ll = red[2 * r] / nl, lr = red[2 * r + 1] / nr;
+      S(r, RS_HLOSSL) = ll;
+      S(r, RS_HLOSSR) = lr;
+      S(r, RS_LOSS) = (double)nl / n * ll + (double)nr / n * lr;
+    }
+    __syncthreads();
+  }
+  // ----------------------------------------------------------- write results
+  if (tid < it.rn) {
+    const int r = tid;
+    const int64_t kr = (int64_t)k * a.R + it.rbase + r;
+    const int dts = a.dmax + 1;
+    for (int i = 0; i <= d; ++i) a.r_theta[kr * dts + i] = th[r * dt() + i];
+    a.r_fail[kr] = (int)S(r, RS_FAIL);
+    a.r_stop[kr] = (int)S(r, RS_STOP);
+    a.r_iters[kr] = (int)S(r, RS_ITERS);
+    a.r_nright[kr] = (int)S(r, RS_NRIGHT);
+    a.r_flags[kr] = (S(r, RS_CONV) != 0.0 ? 1 : 0) | (S(r, RS_FB) != 0.0 ? 2 : 0);
+    a.r_fbiter[kr] = (int)S(r, RS_FEASIT);
+    a.r_alpha[kr] = P.adaptive_alpha ? S(r, RS_ALPHA) : P.alpha0;
+    const double nan = __longlong_as_double(0x7ff8000000000000ll);
+    a.r_loss[kr] = (P.hard_refit && S(r, RS_FAIL) == 0.0) ? S(r, RS_LOSS) : nan;
+    a.r_child[kr * 2] = P.hard_refit ? S(r, RS_HLOSSL) : nan;
+    a.r_child[kr * 2 + 1] = P.hard_refit ? S(r, RS_HLOSSR) : nan;
+    a.r_ridge[kr * 2] = S(r, RS_LAML);
+    a.r_ridge[kr * 2 + 1] = S(r, RS_LAMR);
+    const bool have = P.hard_refit && S(r, RS_FAIL) == 0.0;
+    for (int f = 0; f < it.p; ++f) {
+      a.r_beta[(kr * 2) * a.pmax + f] = have ? bl[r * a.pmax + f] : nan;
+      a.r_beta[(kr * 2 + 1) * a.pmax + f] = have ? br[r * a.pmax + f] : nan;
+    }
+  }
+  __syncthreads();
+}
+
+template <int TC>
+__global__ void __launch_bounds__(kSplitThreads, 1) split_kernel(SplitArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_item;
+  SplitCta<TC> cta(a, smem);
+  const int count = a.counts[0];
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(&a.counts[1], 1);
+    __syncthreads();
+    const int q = s_item;
+    __syncthreads();
+    if (q >= count) break;
+    cta.run(a.items[q]);
+  }
+}
+
+// Per node: best non-fallback restart by hard loss, else best fallback,
+// else the last failure (splitters.py:354-363); copy it to the outputs.
+__global__ void split_select(SplitArgs a, ArtSplitResult out) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.K) return;
+  const int d = a.dims[k], p = feature_count(d, a.features[k]);
+  int best = -1, best_fb = -1, last_fail = -1;
+  for (int r = 0; r < a.R; ++r) {
+    const int64_t kr = k * a.R + r;
+    if (a.r_fail[kr] != 0) { last_fail = r; continue; }
+    const bool fb = (a.r_flags[kr] & 2) != 0;
+    const double l = a.r_loss[kr];
+    if (!a.prm.hard_refit) { if (best < 0) best = r; continue; }
+    if (fb) { if (best_fb < 0 || l < a.r_loss[k * a.R + best_fb]) best_fb = r; }
+    else if (best < 0 || l < a.r_loss[k * a.R + best]) best = r;
+  }
+  int pick = best >= 0 ? best : (best_fb >= 0 ? best_fb : last_fail);
+  if (pick < 0) pick = 0;
+  const int64_t kr = k * a.R + pick;
+  const int dts = a.dmax + 1;
+  for (int i = 0; i <= d; ++i) out.theta[k * out.theta_stride + i] = a.r_theta[kr * dts + i];
+  if (out.beta)
+    for (int f = 0; f < p; ++f) {
+      out.beta[(k * 2) * out.beta_stride + f] = a.r_beta[(kr * 2) * a.pmax + f];
+      out.beta[(k * 2 + 1) * out.beta_stride + f] = a.r_beta[(kr * 2 + 1) * a.pmax + f];
+    }
+  if (out.loss) out.loss[k] = a.r_loss[kr];
+  if (out.child_loss) { out.child_loss[2 * k] = a.r_child[2 * kr]; out.child_loss[2 * k + 1] = a.r_child[2 * kr + 1]; }
+  if (out.ridge_effective) { out.ridge_effective[2 * k] = a.r_ridge[2 * kr]; out.ridge_effective[2 * k + 1] = a.r_ridge[2 * kr + 1]; }
+  if (out.n_right) out.n_right[k] = a.r_nright[kr];
+  if (out.n_iters) out.n_iters[k] = a.r_iters[kr];
+  if (out.stop_reason) out.stop_reason[k] = a.r_stop[kr];
+  if (out.failure) out.failure[k] = (best >= 0 || best_fb >= 0) ? 0 : a.r_fail[kr];
+  if (out.flags) out.flags[k] = a.r_flags[kr] | (pick << 8);
+  if (out.fallback_iteration) out.fallback_iteration[k] = a.r_fbiter[kr];
+  if (out.final_alpha) out.final_alpha[k] = a.r_alpha[kr];
+}
+
+// Device initialisation of theta0 when none is supplied: w ~ N(0, I) from
+// Philox keyed by (seed, node, restart), normalised; z = median(X w) by
+// selection (numpy's median: mean of the two middle values for even n).
+__global__ void split_init_theta(SplitArgs a, double* theta0, int64_t stride) {
+  const int64_t kr = blockIdx.x;
+  if (kr >= a.K * a.R) return;
+  const int64_t k = kr / a.R;
+  const int d = a.dims[k];
+  const int64_t r0 = a.row_offsets[k], n = a.row_offsets[k + 1] - r0;
+  const int64_t xoff = a.x_offsets[k];
+  __shared__ double w[ART_MAX_DIM + 1];
+  __shared__ double s_lo, s_hi;
+  if (threadIdx.x == 0) {
+    double nrm2 = 0.0;
+    for (int i = 0; i < d; i += 2) {
+      Philox4 r = philox4x32_10((uint32_t)kr, (uint32_t)(kr >> 32), (uint32_t)i, 0x5eedu,
+                                (uint32_t)a.prm.seed, (uint32_t)(a.prm.seed >> 32));
+      double z0, z1;
+      normal_pair(r, z0, z1);
+      w[i] = z0;
+      if (i + 1 < d) w[i + 1] = z1;
+    }
+    for (int i = 0; i < d; ++i) nrm2 += w[i] * w[i];
+    double nrm = sqrt(nrm2);
+    if (nrm <= 1e-12) { w[0] = 1.0; for (int i = 1; i < d; ++i) w[i] = 0.0; nrm = 1.0; }
+    for (int i = 0; i < d; ++i) w[i] /= nrm;
+  }
+  __syncthreads();
+  // median of u = X w: order statistics by bisection on the ordered 64-bit
+  // keys of the doubles (count(key(u) <= t) is monotone; <= 64 passes)
+  __shared__ long long red_c[32];
+  // monotone map of doubles to int64: +x -> bits, -x (magnitude bits m) -> -m - 1
+  auto key = [](double v) -> long long {
+    const long long b = __double_as_longlong(v);
+    return b >= 0 ? b : -(b & 0x7FFFFFFFFFFFFFFFll) - 1;
+  };
+  auto kth = [&](long long m) {
+    long long lo = key(-INFINITY), hi = key(INFINITY);
+    for (int it = 0; it < 70 && lo < hi; ++it) {
+      const long long mid = lo + (long long)(((unsigned long long)hi - (unsigned long long)lo) >> 1);
+      long long c = 0;
+      for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        double u = 0.0;
+        for (int cc = 0; cc < d; ++cc) u = fma(a.x[xoff + i * d + cc], w[cc], u);
+        c += (key(u) <= mid);
+      }
+      for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+      if ((threadIdx.x & 31) == 0) red_c[threadIdx.x >> 5] = c;
+      __syncthreads();
+      long long tot = 0;
+      for (int i = 0; i < (int)(blockDim.x >> 5); ++i) tot += red_c[i];
+      __syncthreads();
+      if (tot > m) hi = mid; else lo = mid + 1;
+    }
+    const long long b = lo;
+    return __longlong_as_double(b >= 0 ? b : ((-(b + 1)) | (long long)0x8000000000000000ull));
+  };
+  if (n == 0) {
+    if (threadIdx.x == 0) { for (int i = 0; i < d; ++i) theta0[kr * stride + i] = w[i]; theta0[kr * stride + d] = 0.0; }
+    return;
+  }
+  const double v1 = kth((n - 1) / 2);
+  const double v2 = (n % 2 == 0) ? kth(n / 2) : v1;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < d; ++i) theta0[kr * stride + i] = w[i];
+    theta0[kr * stride + d] = (n % 2 == 0) ? 0.5 * (v1 + v2) : v1;
+  }
+}
+
+struct SplitWs {
+  size_t counts, items, theta0, r_theta, r_loss, r_beta, r_child, r_ridge, r_i, r_alpha, total;
+};
+SplitWs split_ws(int64_t K, int R, int dmax, int pmax) {
+  SplitWs w;
+  size_t o = 0;
+  auto take = [&](size_t bytes) { size_t at = o; o = (o + bytes + 255) & ~(size_t)255; return at; };
+  w.counts = take(4 * (2 + 2 * kBuckets));
+  w.items = take(4 * (size_t)K * R);
+  w.theta0 = take(8 * (size_t)K * R * (ART_MAX_DIM + 1));
+  w.r_theta = take(8 * (size_t)K * R * (dmax + 1));
+  w.r_loss = take(8 * (size_t)K * R);
+  w.r_beta = take(8 * (size_t)K * R * 2 * pmax);
+  w.r_child = take(8 * (size_t)K * R * 2);
+  w.r_ridge = take(8 * (size_t)K * R * 2);
+  w.r_i = take(4 * (size_t)K * R * 6);
+  w.r_alpha = take(8 * (size_t)K * R);
+  w.total = o;
+  return w;
+}
+
+int choose_rg(int R, int pa, int& TC) {
+  // largest group (<= 16 restarts) whose Gram tiles fit 256 threads and the
+  // accumulators a modest shared-memory budget
+  const int E = pa * (pa + 1) / 2;
+  for (int rg = std::min(R, kMaxRg); rg >= 1; --rg) {
+    const int c2 = 2 * rg;
+    const int tc = c2 >= 8 ? 8 : (c2 >= 4 ? 4 : 2);
+    const int te = 32 / tc;
+    const int tiles = ((E + te - 1) / te) * ((c2 + tc - 1) / tc);
+    if (tiles <= kSplitThreads && (size_t)E * c2 * 8 <= 64 * 1024) { TC = tc; return rg; }
+  }
+  TC = 2;
+  return 0;
+}
+
+}  // namespace
+}  // namespace art
+
+using namespace art;
+
+extern "C" size_t art_split_workspace_size(int64_t count, int32_t n_restarts, int32_t max_dim,
+                                           int32_t max_features) {
+  if (count < 0 || n_restarts < 1) return 0;
+  return split_ws(count, n_restarts, std::max(max_dim, 1), std::max(max_features, 1)).total;
+}
+
+extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* prm,
+                               const ArtSplitResult* out, void* workspace, size_t ws_bytes,
+                               art_stream_t stream) {
+  cudaGetLastError();
+  if (!pr || !prm || !out) { set_error("art_split_level: null argument"); return ART_E_INVALID; }
+  const int64_t K = pr->seg.count;
+  if (K < 0) { set_error("art_split_level: negative count"); return ART_E_INVALID; }
+  if (K == 0) return ART_OK;
+  if (!pr->seg.row_offsets || !pr->seg.x_offsets || !pr->seg.dims || !pr->seg.features || !pr->x ||
+      !pr->y || !pr->temperature || !pr->ridge || !out->theta) {
+    set_error("art_split_level: null device pointer");
+    return ART_E_INVALID;
+  }
+  if (pr->max_dim < 1 || pr->max_dim > ART_MAX_DIM || pr->max_features < 1 || pr->max_features > kMaxP) {
+    set_error("art_split_level: max_dim in [1, %d] and max_features in [1, %d] required", ART_MAX_DIM, kMaxP);
+    return ART_E_UNSUPPORTED;
+  }
+  if (prm->n_restarts < 1 || prm->max_iters < 0 || prm->max_backtracks < 0 ||
+      prm->max_line_search_failures < 1 || !(prm->rho > 0.0 && prm->rho < 1.0) ||
+      !(prm->armijo_c > 0.0 && prm->armijo_c < 1.0) || !(prm->alpha0 > 0.0) ||
+      !(prm->alpha_min > 0.0) || prm->alpha_max < prm->alpha_min || prm->min_side_points < 1 ||
+      !(prm->min_side_fraction >= 0.0 && prm->min_side_fraction < 0.5) || !(prm->anneal_ratio > 0.0)) {
+    set_error("art_split_level: invalid splitter parameters");
+    return ART_E_INVALID;
+  }
+  if (prm->precision != ART_PRECISION_FP64) {
+    set_error("art_split_level: only the FP64 form is built");
+    return ART_E_UNSUPPORTED;
+  }
+  if (out->theta_stride < pr->max_dim + 1 || (out->beta && out->beta_stride < pr->max_features)) {
+    set_error("art_split_level: output strides too small");
+    return ART_E_INVALID;
+  }
+  const int R = prm->n_restarts;
+  int TC = 2;
+  const int Rg = choose_rg(R, pr->max_features + 1, TC);
+  if (Rg < 1) { set_error("art_split_level: model too large for the split kernel"); return ART_E_UNSUPPORTED; }
+  const SplitWs wl = split_ws(K, R, pr->max_dim, pr->max_features);
+  if (!workspace || ws_bytes < wl.total) {
+    set_error("art_split_level: workspace %zu bytes < required %zu", ws_bytes, wl.total);
+    return ART_E_WORKSPACE;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned char* ws = (unsigned char*)workspace;
+  SplitArgs a{};
+  a.K = K;
+  a.row_offsets = pr->seg.row_offsets; a.x_offsets = pr->seg.x_offsets;
+  a.dims = pr->seg.dims; a.features = pr->seg.features;
+  a.x = pr->x; a.y = pr->y; a.temperature = pr->temperature; a.ridge = pr->ridge;
+  a.parent_loss = pr->parent_loss; a.fallback = pr->min_side_fallback;
+  a.prm = *prm;
+  a.R = R; a.Rg = Rg; a.groups = (R + Rg - 1) / Rg;
+  a.dmax = pr->max_dim; a.pmax = pr->max_features; a.TC = TC;
+  a.H = std::min(32, std::max(1, kSplitThreads / Rg));
+  a.H = std::min(a.H, prm->max_backtracks + 1);
+  a.r_theta = (double*)(ws + wl.r_theta); a.r_loss = (double*)(ws + wl.r_loss);
+  a.r_beta = (double*)(ws + wl.r_beta); a.r_child = (double*)(ws + wl.r_child);
+  a.r_ridge = (double*)(ws + wl.r_ridge);
+  int32_t* ri = (int32_t*)(ws + wl.r_i);
+  a.r_nright = ri; a.r_iters = ri + K * R; a.r_stop = ri + 2 * K * R; a.r_fail = ri + 3 * K * R;
+  a.r_flags = ri + 4 * K * R; a.r_fbiter = ri + 5 * K * R;
+  a.r_alpha = (double*)(ws + wl.r_alpha);
+  a.tr_loss = out->trace_loss; a.tr_step = out->trace_step; a.tr_back = out->trace_backtracks;
+  a.tr_gnorm = out->trace_grad_norm;
+  a.counts = (int32_t*)(ws + wl.counts); a.items = (int32_t*)(ws + wl.items);
+  if (pr->theta0) {
+    a.theta0 = pr->theta0;
+    a.theta0_stride = pr->theta_stride;
+  } else {
+    a.theta0 = (double*)(ws + wl.theta0);
+    a.theta0_stride = ART_MAX_DIM + 1;
+    prof_begin("split_init_theta", s);
+    split_init_theta<<<(unsigned)(K * R), 256, 0, s>>>(a, (double*)(ws + wl.theta0), ART_MAX_DIM + 1);
+    prof_end(s);
+    count_launch();
+  }
+  if (cudaMemsetAsync(a.counts, 0, 4 * (2 + 2 * kBuckets), s) != cudaSuccess) return check_launch("memset");
+  const unsigned pg = (unsigned)((K * a.groups + 255) / 256);
+  prof_begin("split_plan", s);
+  split_plan_hist<<<pg, 256, 0, s>>>(a);
+  split_plan_scan<<<1, 32, 0, s>>>(a);
+  split_plan_scatter<<<pg, 256, 0, s>>>(a);
+  prof_end(s);
+  count_launch(); count_launch(); count_launch();
+  const size_t smem = split_layout(a.dmax, a.pmax, a.Rg, a.H).total;
+  if (smem > 227 * 1024) { set_error("art_split_level: shared memory %zu too large", smem); return ART_E_UNSUPPORTED; }
+  auto launch = [&](auto kern) -> int {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("art_split_level: cannot reserve %zu bytes of shared memory", smem);
+      return ART_E_UNSUPPORTED;
+    }
+    int occ = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kSplitThreads, smem) != cudaSuccess) {
+      cudaGetLastError();
+      occ = 1;
+    }
+    const int64_t grid = std::min<int64_t>((int64_t)device_sm_count() * std::max(occ, 1), K * a.groups);
+    prof_begin("split_level", s);
+    kern<<<(unsigned)std::max<int64_t>(grid, 1), kSplitThreads, smem, s>>>(a);
+    prof_end(s);
+    count_launch();
+    return check_launch("split_level");
+  };
+  int rc;
+  if (TC == 8) rc = launch(split_kernel<8>);
+  else if (TC == 4) rc = launch(split_kernel<4>);
+  else rc = launch(split_kernel<2>);
+  if (rc) return rc;
+  prof_begin("split_select", s);
+  split_select<<<(unsigned)((K + 127) / 128), 128, 0, s>>>(a, *out);
+  prof_end(s);
+  count_launch();
+  return check_launch("split_select");
+}

@@ -238,7 +238,8 @@ def test_batched_mixed_fp64_factor_matches_oracle(seed, K, n_max):
 
 
 def test_tensor_core_gram_accuracy():
-    """BF16 hi/lo split products with FP32 accumulation: ||G' - G||_F <= 2e-6 ||G||_F."""
+    """BF16 hi/lo split products, FP32 accumulation in chains of at most 256 rows
+    summed in FP32: ||G' - G||_F <= 3e-6 ||G||_F for every system."""
 
     from art.models import ridge_gram_batched
 
@@ -248,6 +249,7 @@ def test_tensor_core_gram_accuracy():
     gram = gram.cpu().numpy().astype(float)
     status = status.cpu().numpy()
     checked = 0
+    errs = []
     for k in range(wl.count):
         r0, r1 = wl.row_offsets[k], wl.row_offsets[k + 1]
         d = int(wl.dims[k])
@@ -271,9 +273,11 @@ def test_tensor_core_gram_accuracy():
         Gd = Gd + np.tril(Gd, -1).T
         err = np.linalg.norm(Gd - G) / np.linalg.norm(G)
         print(f"system {k} p={p} n={r1 - r0} rel Frobenius error {err:.2e}")
-        assert err <= 2e-6, (k, p, err)
+        errs.append((k, p, err))
         checked += 1
     assert checked >= 5
+    worst = max(errs, key=lambda e: e[2])
+    assert worst[2] <= 3e-6, worst
 
 
 def test_mixed_is_deterministic_and_alone_equals_batched():

@@ -1,0 +1,152 @@
+"""Soft oblique split search on the GPU vs the reference (golden fixtures) and the oracle.
+
+FP64 form tolerances: split parameters and soft-loss histories within 1e-9
+relative of the reference given identical initial theta; stop reasons,
+iteration counts, backtrack counts and partitions identical.
+"""
+
+import ast
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, gpu_available
+from oracle import ridge as O
+from oracle import split as S
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not gpu_available(), reason="needs a CUDA device")]
+SG = np.load(GOLDEN / "split_golden.npz")
+
+
+def splitter_for(kind, T, lam, R, iters, extra):
+    from art import AffineRidgeModel, PolynomialRidgeModel
+    from art.splitters import SoftObliqueSplitter
+
+    model = AffineRidgeModel(ridge=lam) if kind == O.AFFINE else PolynomialRidgeModel(
+        degree=2 if kind == O.POLY2 else 1, ridge=lam)
+    return SoftObliqueSplitter(model, T, max_iters=int(iters), n_restarts=int(R), **extra)
+
+
+@pytest.mark.parametrize("i", range(int(SG["count"])))
+def test_split_matches_reference_golden(i):
+    from art.splitters import level_result_to_split, split_level
+
+    kind, T, lam, R, iters, parent_loss = SG[f"s{i}_meta"]
+    extra = ast.literal_eval(str(SG[f"s{i}_extra"]))
+    s = splitter_for(int(kind), T, lam, R, iters, extra)
+    X, y = SG[f"s{i}_X"], SG[f"s{i}_y"]
+    res = split_level(s, X.reshape(-1), y, [0, len(y)], [X.shape[1]], [int(kind)], T, lam,
+                      parent_loss=[parent_loss], theta0=SG[f"s{i}_theta0"][None], traces=True)
+    out = level_result_to_split(s, res, 0, len(y), parent_loss, True)
+    np.testing.assert_allclose(np.r_[out.w, out.z], SG[f"s{i}_theta"], rtol=1e-9, atol=1e-11)
+    assert out.stop_reason == str(SG[f"s{i}_stop"])
+    assert out.n_iters == int(SG[f"s{i}_n_iters"])
+    assert out.n_right == int(SG[f"s{i}_n_right"])
+    np.testing.assert_allclose(out.metadata["soft_loss_history"], SG[f"s{i}_soft_losses"], rtol=1e-9, atol=1e-13)
+    np.testing.assert_allclose(out.metadata["step_size_history"], SG[f"s{i}_steps"], rtol=1e-12)
+    assert out.metadata["backtrack_history"] == [int(v) for v in SG[f"s{i}_backtracks"]]
+    np.testing.assert_allclose(out.loss, float(SG[f"s{i}_loss"]), rtol=1e-9)
+    np.testing.assert_allclose(out.left_model.coef_, SG[f"s{i}_beta_left"], rtol=1e-8, atol=1e-10)
+    np.testing.assert_allclose(out.right_model.coef_, SG[f"s{i}_beta_right"], rtol=1e-8, atol=1e-10)
+    assert bool(out.metadata.get("min_side_fallback", False)) == bool(SG[f"s{i}_fallback"])
+
+
+def random_level(seed, K=10, R=3, d=4, kinds=(O.AFFINE, O.POLY2)):
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(40, 600, K)
+    Xs, ys, th0, kd = [], [], [], []
+    for k in range(K):
+        X = rng.uniform(-1, 1, (ns[k], d))
+        a = rng.normal(size=d)
+        y = np.tanh(5 * (X @ a / np.linalg.norm(a) - 0.2)) + 0.2 * X[:, 0] ** 2
+        init = np.random.default_rng(seed * 100 + k)
+        th0.append([S.initialize_theta(X, init) for _ in range(R)])
+        Xs.append(X)
+        ys.append(y)
+        kd.append(kinds[k % len(kinds)])
+    return ns, Xs, ys, np.array(th0), np.array(kd)
+
+
+@pytest.mark.parametrize("anneal", [1.0, 0.1])
+def test_level_matches_oracle_per_node(anneal):
+    """Many nodes of uneven size and mixed feature kinds in one launch == per-node oracle."""
+
+    from art.splitters import level_result_to_split, split_level
+
+    ns, Xs, ys, th0, kd = random_level(3)
+    K, R = len(ns), th0.shape[1]
+    T, lam, iters = 0.15, 1e-6, 12
+    s = splitter_for(O.AFFINE, T, lam, R, iters, {"min_side_points": 5})
+    parent = []
+    for X, y, k in zip(Xs, ys, kd):
+        phi = O.features(X, int(k))
+        b = O.solve_weighted_ridge(phi, y, np.ones(len(y)), lam)["coefficients"]
+        parent.append(float(np.mean((y - phi @ b) ** 2)))
+    ro = np.concatenate([[0], np.cumsum(ns)])
+    res = split_level(s, np.concatenate([X.reshape(-1) for X in Xs]), np.concatenate(ys), ro, [4] * K, kd, T, lam,
+                      parent_loss=parent, theta0=th0, anneal_ratio=anneal, traces=True)
+    p = S.Params(max_iters=iters, n_restarts=R, min_side_points=5, anneal_ratio=anneal)
+    for k in range(K):
+        ref = S.split(Xs[k], ys[k], list(th0[k]), T, int(kd[k]), lam, parent[k], p)
+        s.model_template = splitter_for(int(kd[k]), T, lam, R, iters, {}).model_template
+        out = level_result_to_split(s, res, k, int(ns[k]), parent[k], True)
+        np.testing.assert_allclose(np.r_[out.w, out.z], np.r_[ref["w"], ref["z"]], rtol=1e-9, atol=1e-11)
+        assert out.n_iters == ref["n_iters"] and out.stop_reason == ref["stop_reason"]
+        assert out.n_right == ref["n_right"]
+        np.testing.assert_allclose(out.loss, ref["loss"], rtol=1e-9)
+
+
+def test_partition_only_mode_and_failures():
+    from art.splitters import SplitNotFoundError, level_result_to_split, split_level
+
+    rng = np.random.default_rng(8)
+    X = rng.uniform(-1, 1, (60, 2))
+    y = (X[:, 0] > 0).astype(float)
+    s = splitter_for(O.AFFINE, 0.1, 1e-6, 1, 10, {"min_side_points": 40, "min_side_fraction": 0.0})
+    th0 = np.array([[[1.0, 0.0, 0.0]]])
+    res = split_level(s, X.reshape(-1), y, [0, 60], [2], [O.AFFINE], 0.1, 1e-6, parent_loss=[0.25], theta0=th0,
+                      hard_refit=False)
+    with pytest.raises(SplitNotFoundError) as err:
+        level_result_to_split(s, res, 0, 60, 0.25, False)
+    assert err.value.reason == "min_side_points"
+    s.min_side_points = 5
+    res = split_level(s, X.reshape(-1), y, [0, 60], [2], [O.AFFINE], 0.1, 1e-6, parent_loss=[0.25], theta0=th0,
+                      hard_refit=False)
+    out = level_result_to_split(s, res, 0, 60, 0.25, False)
+    assert out.loss is None and out.left_model is None and out.n_left + out.n_right == 60
+    right = (X @ out.w - out.z) >= 0
+    assert right.sum() == out.n_right
+
+
+def test_device_initialisation_is_deterministic_and_valid():
+    from art.splitters import split_level
+
+    ns, Xs, ys, th0, kd = random_level(5, K=6, R=4)
+    s = splitter_for(O.AFFINE, 0.2, 1e-6, 4, 8, {"min_side_points": 3})
+    ro = np.concatenate([[0], np.cumsum(ns)])
+    args = (s, np.concatenate([X.reshape(-1) for X in Xs]), np.concatenate(ys), ro, [4] * 6, [O.AFFINE] * 6, 0.2, 1e-6)
+    a = split_level(*args, parent_loss=[1.0] * 6, seed=99)
+    b = split_level(*args, parent_loss=[1.0] * 6, seed=99)
+    np.testing.assert_array_equal(a.theta.cpu().numpy(), b.theta.cpu().numpy())
+    th = a.theta.cpu().numpy()
+    np.testing.assert_allclose(np.linalg.norm(th[:, :4], axis=1), 1.0, rtol=1e-12)
+
+
+def test_public_split_api_matches_oracle():
+    from art import AffineRidgeModel
+    from art.splitters import SoftObliqueSplitter
+
+    rng = np.random.default_rng(12)
+    X = rng.uniform(-1, 1, (300, 3))
+    y = np.where(X[:, 0] + 0.3 * X[:, 1] > 0.1, 1.0, -1.0) + 0.05 * rng.normal(size=300)
+    s = SoftObliqueSplitter(AffineRidgeModel(ridge=1e-6), 0.1, max_iters=20, n_restarts=2, random_state=4)
+    out = s.split(X, y)
+    init = np.random.default_rng(4)
+    th0 = [S.initialize_theta(X, init) for _ in range(2)]
+    phi = O.features(X, O.AFFINE)
+    b = O.solve_weighted_ridge(phi, y, np.ones(300), 1e-6)["coefficients"]
+    ref = S.split(X, y, th0, 0.1, O.AFFINE, 1e-6, float(np.mean((y - phi @ b) ** 2)),
+                  S.Params(max_iters=20, n_restarts=2))
+    np.testing.assert_allclose(np.r_[out.w, out.z], np.r_[ref["w"], ref["z"]], rtol=1e-9, atol=1e-11)
+    np.testing.assert_allclose(out.predict(X), np.where((X @ ref["w"] - ref["z"]) >= 0, phi @ ref["br"], phi @ ref["bl"]),
+                               rtol=1e-8, atol=1e-10)
