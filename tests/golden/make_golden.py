@@ -259,6 +259,74 @@ def har_cases(ref):
     print("har cases:", len(specs), len(sspecs))
 
 
+def c1_target(seed):
+    """Sum of 3 Gaussian bumps + tanh ridge (the C1 target family)."""
+    rng = np.random.default_rng(seed)
+    centres = rng.uniform(-0.8, 0.8, (3, 2))
+    widths = rng.uniform(0.2, 0.5, 3)
+    amps = rng.normal(size=3)
+    a = rng.normal(size=2)
+    a /= np.linalg.norm(a)
+    b = rng.uniform(-0.3, 0.3)
+
+    def f(X):
+        X = np.atleast_2d(X)
+        r2 = ((X[:, None, :] - centres[None]) ** 2).sum(-1)
+        return (amps * np.exp(-r2 / (2 * widths ** 2))).sum(1) + np.tanh(8 * (X @ a - b))
+
+    return f, (centres, widths, amps, a, b)
+
+
+def flatten_tree(ref, tree):
+    rows = []
+    for node in tree.iter_nodes():
+        if isinstance(node, ref.tree.SplitNode):
+            rows.append((node.node_id, node.status, np.r_[node.w, node.z], None,
+                         node.metadata.get("n_samples")))
+        else:
+            rows.append((node.node_id, node.status, None, np.asarray(node.model.coef_),
+                         node.metadata.get("n_samples")))
+    return rows
+
+
+TREE_SPECS = [
+    # (seed, traversal, sample_count, max_depth, isotropic, threshold, restarts)
+    (401, "dfs", 200, 3, False, 0.02, 1),
+    (402, "bfs", 160, 3, True, 0.02, 1),
+    (403, "dfs", 120, 2, True, 0.05, 2),
+]
+
+
+def tree_cases(ref):
+    out = {}
+    for i, (seed, trav, count, depth, iso, thr, R) in enumerate(TREE_SPECS):
+        f, params = c1_target(seed)
+        model = ref.models.AffineRidgeModel(ridge=1e-6, solver="normal")
+        splitter = ref.splitters.SoftObliqueSplitter(model, 0.05, max_iters=40, n_restarts=R, min_side_points=8,
+                                                     min_side_fraction=0.0)
+        builder = ref.builder.RegressionTreeBuilder(
+            domain=ref.domain.BoxDomain.hypercube(2, -1.0, 1.0), oracle=f, model_template=model,
+            splitter=splitter, error_threshold=thr, max_depth=depth, sample_count=count,
+            isotropic_sampling=iso, temperature_config=ref.temperature.TemperatureConfig(strategy="splitter"),
+            random_state=seed, oracle_vectorized=True, traversal=trav,
+            sampler=ref.sampling.HitAndRunSampler(burn_in=0, thinning=5))
+        res = builder.build()
+        rows = flatten_tree(ref, res.tree)
+        out[f"t{i}_ids"] = np.array([r[0] for r in rows])
+        out[f"t{i}_status"] = np.array([r[1] for r in rows])
+        out[f"t{i}_theta"] = np.array([r[2] if r[2] is not None else np.full(3, np.nan) for r in rows])
+        out[f"t{i}_coef"] = np.array([r[3] if r[3] is not None else np.full(3, np.nan) for r in rows])
+        out[f"t{i}_nsamples"] = np.array([-1 if r[4] is None else r[4] for r in rows])
+        out[f"t{i}_queries"] = np.array(res.oracle_queries)
+        out[f"t{i}_target"] = np.concatenate([np.ravel(p) for p in params[:4]] + [[params[4]]])
+        Xt = np.random.default_rng(seed + 1).uniform(-1, 1, (500, 2))
+        out[f"t{i}_Xtest"] = Xt
+        out[f"t{i}_pred"] = res.tree.predict(Xt)
+        print(f"tree {i}: {res.tree.num_nodes()} nodes, {res.oracle_queries} queries")
+    out["count"] = np.array(len(TREE_SPECS))
+    np.savez_compressed(HERE / "tree_golden.npz", **out)
+
+
 def main():
     root = Path(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ART_REFERENCE", ""))
     if not (root / "art" / "__init__.py").exists():

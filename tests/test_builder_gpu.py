@@ -1,0 +1,75 @@
+"""Tree builds on the GPU kernels reproduce the reference builder's trees.
+
+Same configuration and random_state as the reference run recorded in
+tests/golden/tree_golden.npz: identical node ids, statuses and oracle query
+counts; split planes and leaf coefficients within 1e-8; predictions on
+held-out points within 1e-8 relative.
+"""
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, gpu_available
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not gpu_available(), reason="needs a CUDA device")]
+TG = np.load(GOLDEN / "tree_golden.npz")
+SPECS = [(401, "dfs", 200, 3, False, 0.02, 1), (402, "bfs", 160, 3, True, 0.02, 1), (403, "dfs", 120, 2, True, 0.05, 2)]
+
+
+def target_from(params):
+    centres = params[:6].reshape(3, 2)
+    widths, amps, a, b = params[6:9], params[9:12], params[12:14], params[14]
+
+    def f(X):
+        X = np.atleast_2d(X)
+        r2 = ((X[:, None, :] - centres[None]) ** 2).sum(-1)
+        return (amps * np.exp(-r2 / (2 * widths ** 2))).sum(1) + np.tanh(8 * (X @ a - b))
+
+    return f
+
+
+@pytest.mark.parametrize("i", range(3))
+def test_build_matches_reference_tree(i):
+    from art import (AffineRidgeModel, BoxDomain, HitAndRunSampler, RegressionTreeBuilder, SoftObliqueSplitter,
+                     SplitNode, TemperatureConfig)
+
+    seed, trav, count, depth, iso, thr, R = SPECS[i]
+    f = target_from(TG[f"t{i}_target"])
+    model = AffineRidgeModel(ridge=1e-6, solver="normal")
+    splitter = SoftObliqueSplitter(model, 0.05, max_iters=40, n_restarts=R, min_side_points=8, min_side_fraction=0.0)
+    builder = RegressionTreeBuilder(
+        domain=BoxDomain.hypercube(2, -1.0, 1.0), oracle=f, model_template=model, splitter=splitter,
+        error_threshold=thr, max_depth=depth, sample_count=count, isotropic_sampling=iso,
+        temperature_config=TemperatureConfig(strategy="splitter"), random_state=seed, oracle_vectorized=True,
+        traversal=trav, sampler=HitAndRunSampler(burn_in=0, thinning=5))
+    res = builder.build()
+    nodes = list(res.tree.iter_nodes())
+    assert [n.node_id for n in nodes] == list(TG[f"t{i}_ids"])
+    assert [n.status for n in nodes] == list(TG[f"t{i}_status"])
+    assert res.oracle_queries == int(TG[f"t{i}_queries"])
+    for n, th, cf in zip(nodes, TG[f"t{i}_theta"], TG[f"t{i}_coef"]):
+        if isinstance(n, SplitNode):
+            np.testing.assert_allclose(np.r_[n.w, n.z], th, rtol=1e-8, atol=1e-10)
+        else:
+            np.testing.assert_allclose(n.model.coef_, cf, rtol=1e-8, atol=1e-10)
+    pred = res.tree.predict(TG[f"t{i}_Xtest"])
+    np.testing.assert_allclose(pred, TG[f"t{i}_pred"], rtol=1e-8, atol=1e-10)
+
+
+def test_tree_predict_device_routing_matches_host_walk():
+    from art import AffineRidgeModel, LeafNode, RegressionTree, SplitNode
+
+    rng = np.random.default_rng(2)
+
+    def leaf(c):
+        m = AffineRidgeModel()
+        m.coef_ = np.asarray(c, float)
+        return LeafNode(m)
+
+    inner = SplitNode(np.array([0.0, 1.0]), 0.1, leaf([1, 2, 3]), leaf([-1, 0, 2]), node_id="root/R")
+    root = SplitNode(np.array([0.6, 0.8]), -0.2, leaf([0.5, -0.5, 1.0]), inner)
+    tree = RegressionTree(root)
+    X = rng.uniform(-1, 1, (2000, 2))
+    X[0] = [0.0, 0.1]        # exactly on the inner plane: goes right
+    host = np.array([tree.leaf_for_point(x).predict_one(x) for x in X])
+    np.testing.assert_allclose(tree.predict(X), host, rtol=1e-13, atol=1e-13)
