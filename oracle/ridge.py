@@ -1,4 +1,4 @@
-"""Oracle: weighted trace-scaled ridge (reference art/models.py:200-448).
+"""Oracle: weighted trace-scaled ridge (reference art/models.py:200-448) -- test infrastructure only.
 
 Restates solve_weighted_ridge with the same scipy/LAPACK calls the reference
 makes (cho_factor, dpocon, cho_solve, lstsq with gelsy/gelsd), plus the
