@@ -43,6 +43,7 @@ INFO_REFINE_SHIFT = 8
 RIDGE_OPT_FP64_FACTOR = 1
 
 MAX_FEATURES = 160
+RIDGE_NOALLOC_MAX_COUNT = 65536
 MAX_DIM = 64
 
 HAR_BATCHED = 0
@@ -134,6 +135,8 @@ class ArtChains(C.Structure):
 SIGNATURES = {
     "art_ridge_workspace_size": (C.c_size_t, [I64, I32]),
     "art_ridge_batched": (C.c_int, [C.POINTER(ArtRidgeProblem), C.POINTER(ArtRidgeResult), P, C.c_size_t, P]),
+    "art_ridge_noalloc_scratch_bytes": (C.c_size_t, []),
+    "art_ridge_batched_noalloc": (C.c_int, [C.POINTER(ArtRidgeProblem), C.POINTER(ArtRidgeResult), P]),
     "art_ridge_gram": (C.c_int, [C.POINTER(ArtRidgeProblem), P, I64, P, P, C.c_size_t, P]),
     "art_split_workspace_size": (C.c_size_t, [I64, I32, I32, I32]),
     "art_split_level": (C.c_int, [C.POINTER(ArtSplitProblem), C.POINTER(ArtSplitParams),

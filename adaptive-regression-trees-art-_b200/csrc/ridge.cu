@@ -459,8 +459,8 @@ struct WsLayout {
   size_t off_count, off_cursor, off_hist, off_start, off_err, off_lambda, off_list, header,
       total;
 };
-static WsLayout ws_layout(int64_t K) {
-  WsLayout w;
+static constexpr WsLayout ws_layout(int64_t K) {
+  WsLayout w{};
   size_t o = 0;
   w.off_count = o; o += kClasses * 4;
   w.off_cursor = o; o += kClasses * 4;
@@ -654,6 +654,41 @@ static int ridge_entry(const ArtRidgeProblem* pr, const ArtRidgeResult* res, flo
 extern "C" int art_ridge_batched(const ArtRidgeProblem* pr, const ArtRidgeResult* res,
                                  void* workspace, size_t ws_bytes, art_stream_t stream) {
   return ridge_entry(pr, res, nullptr, 0, workspace, ws_bytes, stream);
+}
+
+// Fixed scratch of art_ridge_batched_noalloc: the workspace layout for
+// ART_RIDGE_NOALLOC_MAX_COUNT systems (about 1.8 MiB), a file-scope device
+// array so that the call itself allocates nothing.
+static constexpr size_t kNoallocBytes = ws_layout(ART_RIDGE_NOALLOC_MAX_COUNT).total;
+static __device__ __align__(256) unsigned char g_ridge_noalloc_ws[kNoallocBytes];
+static void* g_noalloc_addr[64];
+
+extern "C" size_t art_ridge_noalloc_scratch_bytes(void) { return kNoallocBytes; }
+
+extern "C" int art_ridge_batched_noalloc(const ArtRidgeProblem* pr, const ArtRidgeResult* res,
+                                         art_stream_t stream) {
+  if (pr && pr->seg.count > ART_RIDGE_NOALLOC_MAX_COUNT) {
+    set_error("art_ridge_batched_noalloc: %lld systems exceed the fixed scratch limit of %d",
+              (long long)pr->seg.count, ART_RIDGE_NOALLOC_MAX_COUNT);
+    return ART_E_UNSUPPORTED;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    set_error("art_ridge_batched_noalloc: no usable current device");
+    return ART_E_DEVICE;
+  }
+  // Resolved once per device; the first call on a device may load the module.
+  if (!g_noalloc_addr[dev]) {
+    void* addr = nullptr;
+    if (cudaGetSymbolAddress(&addr, g_ridge_noalloc_ws) != cudaSuccess || !addr) {
+      cudaGetLastError();
+      set_error("art_ridge_batched_noalloc: cannot resolve the scratch address");
+      return ART_E_LAUNCH;
+    }
+    g_noalloc_addr[dev] = addr;
+  }
+  return ridge_entry(pr, res, nullptr, 0, g_noalloc_addr[dev], kNoallocBytes, stream);
 }
 
 extern "C" int art_ridge_gram(const ArtRidgeProblem* pr, float* gram, int64_t gram_stride,

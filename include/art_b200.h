@@ -157,6 +157,23 @@ ART_API int art_ridge_gram(const ArtRidgeProblem* problem, float* gram, int64_t 
 ART_API int art_ridge_batched(const ArtRidgeProblem* problem, const ArtRidgeResult* result,
                       void* workspace, size_t workspace_bytes, art_stream_t stream);
 
+/* art_ridge_batched without a caller workspace (no counterpart in the
+ * reference, which solves on the host).  For callers that cannot allocate
+ * device memory at solve time -- a host loop embedded in another runtime's
+ * memory pool, or a C/FFI caller with no device allocator of its own -- the
+ * call uses a fixed scratch array compiled into the library and makes no
+ * allocation.  At most ART_RIDGE_NOALLOC_MAX_COUNT systems per call
+ * (ART_E_UNSUPPORTED beyond); results equal art_ridge_batched's.  The scratch
+ * is shared by every call on a device: calls that may overlap (different
+ * streams, or host threads, on the same device) race and must be ordered by
+ * the caller.  The first call on each device resolves the scratch address and
+ * may load the module, so make it before any stream capture.  Every
+ * zero-initialised part of the scratch is cleared on the stream by each call. */
+#define ART_RIDGE_NOALLOC_MAX_COUNT 65536
+ART_API size_t art_ridge_noalloc_scratch_bytes(void);
+ART_API int art_ridge_batched_noalloc(const ArtRidgeProblem* problem, const ArtRidgeResult* result,
+                                      art_stream_t stream);
+
 /* ======================================================================== */
 /*  Soft oblique split search, one launch per tree level                     */
 /*  Replaces BatchedOptimizerWorkspace.optimize                              */
