@@ -312,7 +312,7 @@ def solve_weighted_ridge_batched(
 def ridge_gram_batched(x, y, weights, row_offsets, dims, features, *, x_offsets=None,
                        weight_floor: float = 1e-12, max_features: int | None = None,
                        max_dim: int | None = None, stream=None):
-    """Tensor-core weighted Grams (BF16 hi/lo split products, FP32 accumulation).
+    """Tensor-core weighted Grams (TF32 hi/lo split products, FP32 accumulation).
 
     Returns (packed lower-triangular Grams [K, pmax(pmax+1)/2] float32, status[K]);
     systems outside 33 <= p <= 160 get status -4.

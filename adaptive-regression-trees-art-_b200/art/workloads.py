@@ -213,3 +213,129 @@ def ridge_meta(wl: RidgeWorkload):
     """(row_offsets, dims, kinds) of the full mix a (possibly row-less) workload was drawn from."""
 
     return wl._full_meta
+
+
+@dataclass
+class SplitWorkload:
+    """Node-sorted split-search inputs: x (sum n_k * d,), y (sum n_k,), CSR offsets."""
+
+    x: object
+    y: object
+    row_offsets: np.ndarray
+    dims: np.ndarray
+    kinds: np.ndarray
+    theta0: object  # (K, R, d + 1) restart normals and thresholds
+    temperature: np.ndarray
+    ridge: np.ndarray
+    d: int
+
+    @property
+    def count(self) -> int:
+        return int(self.dims.size)
+
+    @property
+    def n_rows(self) -> int:
+        return int(self.row_offsets[-1])
+
+
+def split_nodes(count: int = 4096, seed: int = 3, d: int = 16, n_min: int = 256, n_max: int = 16384,
+                restarts: int = 16, temperature: float = 0.2, ridge: float = 1e-6,
+                device: str = "cuda") -> SplitWorkload:
+    """Batched split-search nodes: each node a random axis box inside [-1,1]^d
+    (side lengths U[0.25, 1] * 2), x uniform in the box, y = 8 Gaussian bumps
+    (widths U(0.1, 0.6), amplitudes N(0,1)) + a linear trend with N(0,1)
+    coefficients; R restart normals per node (unit Gaussian w, z = the median
+    of x.w over the node).  Node parameters come from numpy's PCG64 (seed);
+    rows are drawn on ``device`` by torch's Philox generator."""
+
+    import torch
+
+    rng = np.random.default_rng(seed)
+    K = int(count)
+    n = np.floor(np.exp(rng.uniform(np.log(n_min), np.log(n_max), K))).astype(np.int64)
+    side = rng.uniform(0.25, 1.0, (K, d)) * 2.0
+    lo = rng.uniform(-1.0, 1.0 - side)
+    centres = rng.uniform(-1.0, 1.0, (8, d))
+    widths = rng.uniform(0.1, 0.6, 8)
+    amps = rng.normal(size=8)
+    trend = rng.normal(size=d)
+    W0 = rng.normal(size=(K, restarts, d))
+    W0 /= np.linalg.norm(W0, axis=2, keepdims=True)
+    gen_seed = int(rng.integers(0, 2**62))
+    dev = torch.device(device)
+    g = torch.Generator(device=dev)
+    g.manual_seed(gen_seed)
+    ro = np.concatenate([[0], np.cumsum(n)]).astype(np.int64)
+    total = int(ro[-1])
+    nt = torch.from_numpy(n).to(dev)
+    node = torch.repeat_interleave(torch.arange(K, device=dev), nt)
+    lo_t = torch.from_numpy(lo).to(dev)
+    side_t = torch.from_numpy(side).to(dev)
+    x = torch.empty((total, d), dtype=torch.float64, device=dev)
+    y = torch.empty(total, dtype=torch.float64, device=dev)
+    C_t = torch.from_numpy(centres).to(dev)
+    Wd = torch.from_numpy(widths).to(dev)
+    Am = torch.from_numpy(amps).to(dev)
+    Tr = torch.from_numpy(trend).to(dev)
+    step = 1 << 21
+    for s in range(0, total, step):
+        e = min(total, s + step)
+        kk = node[s:e]
+        X = lo_t[kk] + side_t[kk] * torch.rand((e - s, d), generator=g, device=dev, dtype=torch.float64)
+        r2 = ((X[:, None, :] - C_t[None]) ** 2).sum(-1)
+        y[s:e] = (Am * torch.exp(-r2 / (2.0 * Wd ** 2))).sum(1) + X @ Tr
+        x[s:e] = X
+    theta0 = torch.empty((K, restarts, d + 1), dtype=torch.float64, device=dev)
+    W0_t = torch.from_numpy(W0).to(dev)
+    theta0[:, :, :d] = W0_t
+    for k0 in range(0, K, 256):
+        k1 = min(K, k0 + 256)
+        r0, r1 = int(ro[k0]), int(ro[k1])
+        proj = torch.einsum("nd,nrd->nr", x[r0:r1], W0_t[node[r0:r1]])
+        for k in range(k0, k1):
+            a, b = int(ro[k]) - r0, int(ro[k + 1]) - r0
+            theta0[k, :, d] = proj[a:b].median(dim=0).values if b > a else 0.0
+    return SplitWorkload(x.reshape(-1), y, ro, np.full(K, d, np.int32), np.full(K, N.FEATURES_AFFINE, np.int32),
+                         theta0, np.full(K, temperature), np.full(K, ridge), d)
+
+
+@dataclass
+class PolytopeWorkload:
+    """Chains in per-chain polytopes [-1,1]^d cut by k oblique halfspaces."""
+
+    lo: object
+    hi: object
+    row_offsets: object
+    A: object
+    b: object
+    max_rows: int
+    x0: object
+    chain_polytope: object
+    seeds: object
+    d: int
+
+
+def polytopes(count: int = 16384, d: int = 8, seed: int = 4, k_min: int = 4, k_max: int = 12,
+              device: str = "cuda") -> PolytopeWorkload:
+    """One polytope per chain: box [-1,1]^d and k ~ U{k_min..k_max} unit
+    halfspaces a.x <= b with b = a.c + r, c ~ U[-0.5,0.5]^d, r ~ U[0.05, 0.5],
+    so a ball of radius >= 0.05 around the start c is feasible."""
+
+    import torch
+
+    rng = np.random.default_rng([seed, d])
+    Cn = int(count)
+    k = rng.integers(k_min, k_max + 1, Cn)
+    c = rng.uniform(-0.5, 0.5, (Cn, d))
+    ro = np.concatenate([[0], np.cumsum(k)]).astype(np.int64)
+    A = rng.normal(size=(int(ro[-1]), d))
+    A /= np.linalg.norm(A, axis=1, keepdims=True)
+    owner = np.repeat(np.arange(Cn), k)
+    r = rng.uniform(0.05, 0.5, owner.size)
+    b = np.einsum("ij,ij->i", A, c[owner]) + r
+    dev = torch.device(device)
+    to = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a)).to(device=dev, dtype=dt)
+    return PolytopeWorkload(to(np.full((Cn, d), -1.0), torch.float64), to(np.full((Cn, d), 1.0), torch.float64),
+                            to(ro, torch.int64), to(A, torch.float64), to(b, torch.float64), int(k_max),
+                            to(c, torch.float64), to(np.arange(Cn), torch.int32),
+                            to((np.uint64(seed) << np.uint64(32)) + np.arange(Cn, dtype=np.uint64), torch.int64), d)

@@ -1,14 +1,21 @@
 // bulk.cuh -- mbarrier + cp.async.bulk (1-D TMA) staging helpers, sm_90+/sm_100a.
 //
-// Every wait is bounded: try_wait loops give up after kSpinLimit polls and
-// report failure to the caller, which records an error status and skips the
-// item instead of hanging the GPU.
+// Every wait is bounded: a try_wait loop gives up after kWaitNs nanoseconds
+// of %globaltimer (or kSpinLimit polls) and reports failure to the caller,
+// which records an error status and stops instead of hanging the GPU.
 #pragma once
 #include <stdint.h>
 
 namespace art {
 
 constexpr uint32_t kSpinLimit = 1u << 26;
+constexpr uint64_t kWaitNs = 1000000000ull;  // 1 s
+
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -53,8 +60,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 // Bounded wait; returns false if the barrier did not complete in time.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (uint32_t i = 0; i < kSpinLimit; ++i)
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (uint32_t i = 0; i < kSpinLimit; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 63u) == 63u && globaltimer_ns() - t0 > kWaitNs) return false;
+  }
   return false;
 }
 

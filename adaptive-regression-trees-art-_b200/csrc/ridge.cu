@@ -12,6 +12,7 @@
 //   plan_hist -> plan_scan -> plan_scatter : per-class work lists, largest
 //       cost first (log2 buckets of n*(p+1)^2), built on the device;
 //   [mixed] ridge_tc_kernel                : tcgen05 Gram + refinement;
+//   ridge_warp_kernel                      : FP64, (p+1) <= 24, warp per system;
 //   ridge_fp64_kernel<4>, <8>              : persistent FP64 work queues;
 //   ridge_fp64_kernel<8> on the resolve list (mixed systems that did not
 //       converge); ridge_qr_kernel on the auto-solver fallback list.
@@ -28,6 +29,7 @@ namespace art {
 __device__ __forceinline__ int plan_class(const RidgeArgs& a, int p) {
   if (a.precision == ART_PRECISION_MIXED && p >= kTensorMinP) return CLS_TENSOR;
   if (a.gram_out) return -1;  // Gram-only calls cover tensor-class systems only
+  if (p + 1 <= kWarpMaxAug) return CLS_WARP;
   return (p + 1 <= kSmallMaxAug) ? CLS_SMALL : CLS_LARGE;
 }
 
@@ -126,13 +128,6 @@ __host__ __device__ inline Fp64Layout fp64_layout(int pmax, int dmax, int ts, in
   return L;
 }
 
-__device__ __forceinline__ int tile_row(int t) {
-  int I = (int)((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
-  while (I * (I + 1) / 2 > t) --I;
-  while ((I + 1) * (I + 2) / 2 <= t) ++I;
-  return I;
-}
-
 // Issue the bulk copies of chunk c (x rows, y, w) into stage st.
 __device__ __forceinline__ void issue_chunk(const RidgeArgs& a, const RidgeItem& it, int chunk,
                                             int64_t c, unsigned char* smem, const Fp64Layout& lay,
@@ -208,12 +203,13 @@ __global__ void __launch_bounds__(kRidgeThreads) ridge_fp64_kernel(RidgeArgs a, 
     }
     __syncthreads();  // fa/fb visible
     bool timed_out = false;
+    int64_t timed_c = 0;
     for (int64_t c = 0; c < nchunks; ++c) {
       const int st = (int)(c & 1);
       const uint32_t par = st ? (uses1 & 1) : (uses0 & 1);
       const bool ok = mbar_wait(&bars[st], par);
+      if (!__syncthreads_and(ok)) { timed_out = true; timed_c = c; break; }
       if (st) ++uses1; else ++uses0;
-      if (!__syncthreads_and(ok)) { timed_out = true; break; }
       const int rows = (int)min((int64_t)CHUNK, it.n - c * CHUNK);
       const double* xs =
           (const double*)(smem + lay.off_x[st] +
@@ -270,6 +266,12 @@ __global__ void __launch_bounds__(kRidgeThreads) ridge_fp64_kernel(RidgeArgs a, 
       if (tid == 0) {
         atomicExch(L.err, 1);
         a.status[k] = -5;
+        // bounded waits for this CTA's own copies still in flight
+        for (int64_t c2 = timed_c; c2 < min(timed_c + 2, nchunks); ++c2) {
+          const int s2 = (int)(c2 & 1);
+          mbar_wait(&bars[s2], s2 ? (uses1 & 1) : (uses0 & 1));
+          if (s2) ++uses1; else ++uses0;
+        }
       }
       return;  // barrier phases are no longer consistent: stop this CTA
     }
@@ -610,7 +612,9 @@ static int ridge_entry(const ArtRidgeProblem* pr, const ArtRidgeResult* res, flo
     if (rc) return rc;
   }
   if (gram_out) return ART_OK;
-  {
+  rc = launch_ridge_warp(a, L, s);
+  if (rc) return rc;
+  if (a.pmax + 1 > kWarpMaxAug) {
     const int pcap = std::min(a.pmax, kSmallMaxAug - 1);
     const size_t sm = fp64_layout(pcap, a.dmax, 4, 64).total;
     rc = launch_persistent(ridge_fp64_kernel<4, 64>, sm, K, s, a, L, CLS_SMALL, pcap,

@@ -12,14 +12,16 @@ constexpr int kBuckets = 64;
 // Work lists.  The plan kernels fill the first three; solve kernels append
 // to the last two.
 enum RidgeClass {
-  CLS_SMALL = 0,    // FP64, (p+1) <= 48: 4x4 register tiles + row slices
+  CLS_SMALL = 0,    // FP64, 24 < (p+1) <= 48: 4x4 register tiles + row slices
   CLS_LARGE = 1,    // FP64, (p+1) > 48: 8x8 register tiles
   CLS_TENSOR = 2,   // mixed form, p > 32: tcgen05 split-product Gram
-  CLS_QR = 3,       // auto solver fallback: Householder QR
-  CLS_RESOLVE = 4,  // mixed form systems re-solved by the FP64 form
-  kClasses = 5
+  CLS_WARP = 3,     // FP64, (p+1) <= 24: one warp per system
+  CLS_QR = 4,       // auto solver fallback: Householder QR
+  CLS_RESOLVE = 5,  // mixed form systems re-solved by the FP64 form
+  kClasses = 6
 };
-constexpr int kPlanClasses = 3;
+constexpr int kPlanClasses = 4;
+constexpr int kWarpMaxAug = 24;
 constexpr int kSmallMaxAug = 48;
 constexpr int kTensorMinP = 33;
 
@@ -216,8 +218,17 @@ __device__ inline bool finish_fp64(const RidgeArgs& a, const RidgeLists& L, int 
   return false;
 }
 
-// Host-side launch helpers (ridge.cu / ridge_tc.cu).
+// Row of the lower-triangular tile grid holding linear tile index t.
+__device__ __forceinline__ int tile_row(int t) {
+  int I = (int)((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
+  while (I * (I + 1) / 2 > t) --I;
+  while ((I + 1) * (I + 2) / 2 <= t) ++I;
+  return I;
+}
+
+// Host-side launch helpers (ridge.cu / ridge_tc.cu / ridge_warp.cu).
 int launch_ridge_tensor(const RidgeArgs& a, const RidgeLists& L, cudaStream_t stream);
+int launch_ridge_warp(const RidgeArgs& a, const RidgeLists& L, cudaStream_t stream);
 int device_sm_count();
 
 }  // namespace art

@@ -4,11 +4,12 @@
 // Per system (one CTA, persistent work queue over the CLS_TENSOR list):
 //  1. Rows stream into shared memory by 1-D bulk copies (2 stages of 32 rows).
 //     256 threads generate v = sqrt(q) * phi(x) for every feature and row,
-//     split it into BF16 hi + lo parts and store both in the K-major
+//     split it into TF32 hi + lo parts (hi = rna(v), lo = rna(v - hi): about
+//     22 significant bits together) and store both in the K-major
 //     core-matrix layout (8 rows x 16 bytes per core matrix, no swizzle).
 //     The same threads accumulate the exact FP64 h = Phi^T (q y) and
 //     diag(G) = sum q phi^2 (for the trace-scaled ridge, models.py:271).
-//  2. One thread issues tcgen05.mma kind::f16 (BF16 x BF16 -> FP32 in TMEM):
+//  2. One thread issues tcgen05.mma kind::tf32 (TF32 x TF32 -> FP32 in TMEM):
 //     G' = Hi Hi^T + Hi Lo^T + Lo Hi^T with M = 128 feature rows per tile
 //     (tile 1: features 0..127 x 0..P16-1; tile 2 covers features >= 128),
 //     committed to an mbarrier per stage so operand buffers recycle.
@@ -24,8 +25,6 @@
 // always released before the CTA exits.
 #include <algorithm>
 
-#include <cuda_bf16.h>
-
 #include "ridge.cuh"
 
 namespace art {
@@ -35,8 +34,10 @@ constexpr int kTcThreads = 256;
 constexpr int kKC = 32;                    // data rows per stage (MMA K per stage)
 constexpr int kPmax = 160;
 constexpr int kGroups = kPmax / 8;         // 8-feature core-matrix groups
+constexpr int kKE = 4;                     // TF32 elements per 16-byte core-matrix row
+constexpr int kKM = 8;                     // MMA K of kind::tf32
 constexpr int kLBO = 128;                  // bytes between K-adjacent core matrices
-constexpr int kSBO = (kKC / 8) * 128;      // bytes between 8-feature groups
+constexpr int kSBO = (kKC / kKE) * 128;    // bytes between 8-feature groups
 constexpr int kOpBytes = kGroups * kSBO;   // one operand array (hi or lo)
 constexpr int kMaxRefine = 14;
 // TMEM accumulation chains are restarted every kDrainChunks stages: the
@@ -65,12 +66,12 @@ __device__ __forceinline__ void tc_fence_before() {
 __device__ __forceinline__ void tc_fence_after() {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
-__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
                                          uint32_t idesc, uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
@@ -101,9 +102,10 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
   return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)(kLBO >> 4) << 16) |
          ((uint64_t)(kSBO >> 4) << 32) | (1ull << 46);
 }
-// Instruction descriptor, kind::f16: D = F32, A = B = BF16, both K-major.
-__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+// Instruction descriptor, kind::tf32: D = F32 (bits 4-5 = 1), A = B = TF32
+// (format 2 at bits 7-9 and 10-12), both K-major, N >> 3 at bit 17, M >> 4 at 24.
+__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) |
          ((uint32_t)(M >> 4) << 24);
 }
 
@@ -133,11 +135,15 @@ __host__ __device__ inline TcLayout tc_layout(int pmax, int dmax, int factor_byt
   return L;
 }
 
-__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 a, __nv_bfloat16 b) {
-  return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
+// FP32 -> TF32 bit pattern, round to nearest (ties away), low 13 bits zero.
+__device__ __forceinline__ uint32_t to_tf32(float v) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
+  return r;
 }
 
 struct TcState {
+  uint32_t load_issued[2];
   uint32_t load_uses[2];
   uint32_t mma_commits[2];
   uint32_t mma_waits[2];
@@ -173,7 +179,7 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *s_tmem;
-  TcState S = {{0, 0}, {0, 0}, {0, 0}};
+  TcState S = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
   bool abort = false;
   const int count = L.count[CLS_TENSOR];
 
@@ -217,17 +223,19 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
         if (a.w) bulk_g2s(smem + lay.w[c], gw.base, gw.bytes, &load_bar[c]);
       }
     }
+    for (int64_t c = 0; c < min((int64_t)2, nchunks); ++c) S.load_issued[c]++;
     __syncthreads();
-    const uint32_t id1 = idesc_bf16(128, N1), id2 = idesc_bf16(128, two ? N2 : 16);
+    const uint32_t id1 = idesc_tf32(128, N1), id2 = idesc_tf32(128, two ? N2 : 16);
     for (int64_t c = 0; c < nchunks && !abort; ++c) {
       const int st = (int)(c & 1);
-      bool ok = mbar_wait(&load_bar[st], S.load_uses[st] & 1);
+      const bool okl = mbar_wait(&load_bar[st], S.load_uses[st] & 1);
+      // the MMAs that last read this stage's operands (two chunks back) must be
+      // done; a drain since then has already consumed their commit
+      const bool mpend = S.mma_waits[st] < S.mma_commits[st];
+      const bool okm = mpend ? mbar_wait(&mma_bar[st], S.mma_waits[st] & 1) : true;
+      if (!__syncthreads_and(okl && okm)) { abort = true; break; }
       S.load_uses[st]++;
-      if (c >= 2) {
-        ok = ok && mbar_wait(&mma_bar[st], S.mma_waits[st] & 1);
-        S.mma_waits[st]++;
-      }
-      if (!__syncthreads_and(ok)) { abort = true; break; }
+      if (mpend) S.mma_waits[st]++;
       const int rows = (int)min((int64_t)kKC, it.n - c * kKC);
       const double* xs = (const double*)(smem + lay.x[st] +
                                          (((uintptr_t)(a.x + it.xoff + c * kKC * d)) & 15));
@@ -258,35 +266,33 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
         if (j < nitems) {
           const int f = j % P16, oct = j / P16;
           const int ia = fidx[2 * f], ib = fidx[2 * f + 1];
-          uint32_t ph[4], pl[4];
+          uint32_t ph[8], pl[8];
 #pragma unroll
-          for (int e = 0; e < 8; e += 2) {
-            __nv_bfloat16 h2[2], l2[2];
-#pragma unroll
-            for (int u = 0; u < 2; ++u) {
-              const int r = oct * 8 + e + u;
-              float v = 0.0f;
-              if (r < rows && ia != -3) {
-                const double* xr = xs + (int64_t)r * d;
-                const double phi = (ia < 0 ? 1.0 : xr[ia]) * (ib < 0 ? 1.0 : xr[ib]);
-                const double qphi = sq_q[r] * phi;
-                hacc[s] = fma(qphi, ys[r], hacc[s]);
-                dacc[s] = fma(qphi, phi, dacc[s]);
-                v = (float)(sq_s[r] * phi);
-              }
-              h2[u] = __float2bfloat16_rn(v);
-              l2[u] = __float2bfloat16_rn(v - __bfloat162float(h2[u]));
+          for (int e = 0; e < 8; ++e) {
+            const int r = oct * 8 + e;
+            float v = 0.0f;
+            if (r < rows && ia != -3) {
+              const double* xr = xs + (int64_t)r * d;
+              const double phi = (ia < 0 ? 1.0 : xr[ia]) * (ib < 0 ? 1.0 : xr[ib]);
+              const double qphi = sq_q[r] * phi;
+              hacc[s] = fma(qphi, ys[r], hacc[s]);
+              dacc[s] = fma(qphi, phi, dacc[s]);
+              v = (float)(sq_s[r] * phi);
             }
-            ph[e >> 1] = pack_bf16(h2[0], h2[1]);
-            pl[e >> 1] = pack_bf16(l2[0], l2[1]);
+            ph[e] = to_tf32(v);
+            pl[e] = to_tf32(v - __uint_as_float(ph[e]));
           }
-          const size_t off = (size_t)(f >> 3) * kSBO + (size_t)oct * 128 + (size_t)(f & 7) * 16;
+          // rows 8*oct .. 8*oct+7 span two K-adjacent core matrices (4 rows each)
+          const size_t off = (size_t)(f >> 3) * kSBO + (size_t)(2 * oct) * 128 + (size_t)(f & 7) * 16;
           *(uint4*)(hi + off) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
+          *(uint4*)(hi + off + 128) = make_uint4(ph[4], ph[5], ph[6], ph[7]);
           *(uint4*)(lo + off) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+          *(uint4*)(lo + off + 128) = make_uint4(pl[4], pl[5], pl[6], pl[7]);
         }
       }
       fence_proxy_async();  // operand writes -> visible to the tensor core
       __syncthreads();
+      if (c + 2 < nchunks) S.load_issued[st]++;
       if (tid == 0) {
         if (c + 2 < nchunks) {
           const int64_t rr = (c + 2) * kKC;
@@ -302,16 +308,16 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
         tc_fence_after();
         const uint32_t hb = smem_u32(hi), lb = smem_u32(lo);
 #pragma unroll
-        for (int s = 0; s < kKC / 16; ++s) {
-          const uint32_t ko = (uint32_t)s * 2 * kLBO;
+        for (int s = 0; s < kKC / kKM; ++s) {
+          const uint32_t ko = (uint32_t)s * (kKM / kKE) * kLBO;
 #pragma unroll
           for (int prod = 0; prod < 3; ++prod) {
             const uint32_t A = (prod == 2) ? lb : hb;
             const uint32_t B = (prod == 1) ? lb : hb;
             const uint32_t acc = ((c % kDrainChunks) == 0 && s == 0 && prod == 0) ? 0u : 1u;
-            mma_bf16(tmem, smem_desc(A + ko), smem_desc(B + ko), id1, acc);
+            mma_tf32(tmem, smem_desc(A + ko), smem_desc(B + ko), id1, acc);
             if (two)
-              mma_bf16(tmem + (uint32_t)N1, smem_desc(A + (uint32_t)g0 * kSBO + ko),
+              mma_tf32(tmem + (uint32_t)N1, smem_desc(A + (uint32_t)g0 * kSBO + ko),
                        smem_desc(B + 16u * kSBO + ko), id2, acc);
           }
         }
@@ -322,9 +328,9 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
       if (seg_end) {
         // wait for every MMA of this segment, then add the partial Gram from TMEM
         bool okw = true;
-        for (int s2 = 0; s2 < 2; ++s2)
+        for (int s2 = 0; s2 < 2 && okw; ++s2)
           while (S.mma_waits[s2] < S.mma_commits[s2]) {
-            okw = mbar_wait(&mma_bar[s2], S.mma_waits[s2] & 1) && okw;
+            if (!mbar_wait(&mma_bar[s2], S.mma_waits[s2] & 1)) { okw = false; break; }
             S.mma_waits[s2]++;
           }
         if (!__syncthreads_and(okw)) { abort = true; break; }
@@ -564,12 +570,17 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
     }
     __syncthreads();
   }
-  // release TMEM (after a bounded wait for any MMA still in flight)
-  for (int st = 0; st < 2; ++st)
+  // release TMEM after bounded waits for this CTA's MMAs and bulk copies in flight
+  for (int st = 0; st < 2; ++st) {
     while (S.mma_waits[st] < S.mma_commits[st]) {
-      mbar_wait(&mma_bar[st], S.mma_waits[st] & 1);
+      if (!mbar_wait(&mma_bar[st], S.mma_waits[st] & 1)) break;
       S.mma_waits[st]++;
     }
+    while (S.load_uses[st] < S.load_issued[st]) {
+      if (!mbar_wait(&load_bar[st], S.load_uses[st] & 1)) break;
+      S.load_uses[st]++;
+    }
+  }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();

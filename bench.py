@@ -53,7 +53,12 @@ def parse():
                     help="mixed form factors the tensor-core Gram in FP64")
     ap.add_argument("--variants", action="store_true",
                     help="also time the other mixed-form factorisation variant")
+    ap.add_argument("--per-node-per-class", type=int, default=64,
+                    help="systems per feature class in the per-node FP64 sample")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-legs", action="store_true", help="skip the split-search and hit-and-run legs")
+    ap.add_argument("--split-nodes", type=int, default=4096)
+    ap.add_argument("--har-chains", type=int, default=16384)
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
 
@@ -262,6 +267,139 @@ class _Meta:
         return {(int(a), int(b)): int(c) for (a, b), c in zip(keys, counts)}
 
 
+def per_node_rate(args, wl, ro, xo, dims, kinds, ridge, out, stream):
+    """Plain FP64 form called once per system (count 1 per C-ABI call, no
+    batching), on a stratified sample; the per-system device time is averaged
+    over the sample with the workload's class mix and reported as solves/s."""
+
+    import ctypes as C
+
+    import torch
+
+    from art import _native as N
+
+    lib = N.load_library()
+    idx = stratified_sample(wl, args.per_node_per_class)
+    x, y, w = wl.x, wl.y, wl.w
+    P = int(out.beta.shape[1])
+    ws = torch.empty(lib.art_ridge_workspace_size(1, P), dtype=torch.uint8, device=x.device)
+    h = C.c_void_p(stream.cuda_stream)
+
+    def addr(t, k):
+        return C.c_void_p(t.data_ptr() + k * t.element_size() * (t.shape[1] if t.dim() == 2 else 1))
+
+    def call(k):
+        seg = N.ArtSegments(1, addr(ro, k), addr(xo, k), addr(dims, k), addr(kinds, k))
+        prob = N.ArtRidgeProblem(seg, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), C.c_void_p(w.data_ptr()),
+                                 addr(ridge, k), 1e-12, N.SOLVER_NORMAL, N.PRECISION_FP64, 1e-10, P,
+                                 int(wl.max_dim), 0, 0)
+        res = N.ArtRidgeResult(addr(out.beta, k), P, addr(out.ridge_effective, k), None, addr(out.status, k),
+                               addr(out.info, k))
+        N.check(lib.art_ridge_batched(C.byref(prob), C.byref(res), C.c_void_p(ws.data_ptr()), ws.numel(), h),
+                "art_ridge_batched")
+
+    for k in idx[:8]:
+        call(int(k))
+    torch.cuda.synchronize()
+    cls = list(zip(wl.dims[idx].tolist(), wl.kinds[idx].tolist()))
+    per_cls = {}
+    for k, key in zip(idx, cls):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        call(int(k))
+        e1.record(stream)
+        per_cls.setdefault(key, []).append((e0, e1))
+    torch.cuda.synchronize()
+    mix = {key: int(np.sum((wl.dims == key[0]) & (wl.kinds == key[1]))) for key in per_cls}
+    total = sum(mix.values())
+    avg_ms = sum(mix[key] / total * np.mean([a.elapsed_time(b) for a, b in evs]) for key, evs in per_cls.items())
+    return {"value": 1000.0 / avg_ms, "unit": UNIT, "sample": f"{len(idx)} systems stratified by n over the "
+            f"feature classes, one art_ridge_batched call each, scaled to the class mix",
+            "ms_per_system": avg_ms}
+
+
+def _event_ms(fn, steps, warmup, stream):
+    import torch
+
+    out = None
+    for _ in range(warmup):
+        out = fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        out = fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps, out
+
+
+def leg_split(args, stream):
+    """Batched soft oblique split search: 4096 nodes, d = 16, n log-uniform in
+    [256, 16384], 16 restarts x 60 projected-gradient steps, affine child fits
+    (lambda = 1e-6), temperature annealed 0.2 -> 0.02; FP64 form."""
+
+    from art import _native as N
+    from art import workloads
+    from art.models import AffineRidgeModel
+    from art.splitters import SoftObliqueSplitter, split_level
+
+    wl = workloads.split_nodes(args.split_nodes, device="cuda")
+    sp = SoftObliqueSplitter(AffineRidgeModel(ridge=1e-6), 0.2, max_iters=60, grad_atol=0.0, grad_rtol=0.0,
+                             min_side_points=8, min_side_fraction=0.0, n_restarts=16)
+
+    def step():
+        return split_level(sp, wl.x, wl.y, wl.row_offsets, wl.dims, wl.kinds, wl.temperature, wl.ridge,
+                           theta0=wl.theta0, anneal_ratio=0.1, hard_refit=True, max_dim=wl.d,
+                           max_features=wl.d + 1, stream=stream)
+
+    N.profile_reset()
+    N.profile_enable(True)
+    ms, res = _event_ms(step, 1, 1, stream)
+    N.profile_enable(False)
+    prof = N.profile_report()
+    units = wl.count * 16 * 60
+    n = np.diff(wl.row_offsets).astype(float)
+    d, p, H = wl.d, wl.d + 1, 4
+    flops = float((n * (2 * d + p * (p + 1) + 8 * p + 2 * d + 12 + 6 * H)).sum()) * 16 * 60
+    top = max(prof.items(), key=lambda kv: kv[1][1])
+    return {"metric": "split restart-steps/s", "value": units / (ms / 1000.0), "unit": "restart-steps/s",
+            "ms_per_step": ms, "nodes": wl.count, "rows": wl.n_rows, "restarts": 16, "iterations": 60,
+            "precision": "fp64", "mean_iters_chosen": float(res.n_iters.double().mean().item()),
+            "failures": int((res.failure != 0).sum().item()),
+            "achieved_fp64_tflops": flops / (ms / 1000.0) / 1e12, "kernel": top[0],
+            "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()}}
+
+
+def leg_har(args, stream):
+    """Batched hit-and-run: 16,384 chains, one polytope each (box [-1,1]^d cut
+    by 4-12 oblique halfspaces), 2000 steps, thinning 10, device Philox draws,
+    FP64 chords; d in {8, 16, 32, 64}."""
+
+    from art import workloads
+    from art.sampling import DevicePolytopes, hit_and_run_device
+
+    out = {}
+    for d in (8, 16, 32, 64):
+        wl = workloads.polytopes(args.har_chains, d=d, device="cuda")
+        polys = DevicePolytopes(d, wl.lo, wl.hi, wl.row_offsets, wl.A, wl.b, wl.max_rows)
+
+        def step():
+            return hit_and_run_device(polys, wl.chain_polytope, wl.x0, burn_in=0, thinning=10, n_rounds=200,
+                                      seeds=wl.seeds, stream=stream)
+
+        ms, (samples, x, status) = _event_ms(step, 1, 1, stream)
+        steps = args.har_chains * 2000
+        k_mean = float((wl.row_offsets[1:] - wl.row_offsets[:-1]).double().mean().item())
+        flops = steps * (2 * k_mean * d + 7 * d + 6 * (2 * d + k_mean))
+        out[f"d{d}"] = {"value": steps / (ms / 1000.0), "unit": "chain-steps/s", "ms": ms,
+                        "samples_per_s": args.har_chains * 200 / (ms / 1000.0),
+                        "achieved_fp64_gflops": flops / (ms / 1000.0) / 1e9,
+                        "status_ok": bool((status == 0).all().item())}
+    return {"metric": "hit-and-run chain-steps/s", "chains": args.har_chains, "steps": 2000, "thinning": 10,
+            "by_dim": out}
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -321,8 +459,11 @@ def run_b200(args):
             ms = float(t.item())
         return ms / args.steps, launches // args.steps, prof, out
 
-    # plain FP64 form (the >=5x comparison point), then the headline form
+    # plain FP64 form, batched and per node (one call per system, the
+    # comparison point of the >=5x target), then the headline form
     plain_ms, _, plain_prof, plain_out = timed("fp64")
+    per_node = (per_node_rate(args, wl, ro, xo, dims, kinds, ridge, plain_out, stream)
+                if args.per_node_per_class > 0 else None)
     variants = {}
     if args.variants and args.precision == "mixed":
         v_ms, _, v_prof, v_out = timed("mixed", not args.fp64_factor)
@@ -345,8 +486,10 @@ def run_b200(args):
     from art.models import kind_feature_count
 
     p_all = np.array([kind_feature_count(int(a), int(b)) for a, b in zip(wl.dims, wl.kinds)])
-    if "fp64<4>" in name:
-        cls_idx = np.flatnonzero(p_all + 1 <= 48)
+    if name == "ridge_warp":
+        cls_idx = np.flatnonzero(p_all + 1 <= 24)
+    elif "fp64<4>" in name:
+        cls_idx = np.flatnonzero((p_all + 1 > 24) & (p_all + 1 <= 48) & ((p_all < 33) | (args.precision == "fp64")))
     elif "fp64<8>" in name:
         cls_idx = np.flatnonzero(p_all + 1 > 48) if args.precision == "fp64" else np.flatnonzero(info & N.INFO_FP64_RESOLVE)
     else:
@@ -398,6 +541,14 @@ def run_b200(args):
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms}
         del hx, hy, hw
 
+    legs = {}
+    if rank == 0 and not args.no_legs:
+        for name, fn in (("split_level", leg_split), ("hit_and_run", leg_har)):
+            try:
+                legs[name] = fn(args, stream)
+            except Exception as exc:  # a failing leg is reported, the headline stands
+                legs[name] = {"error": f"{type(exc).__name__}: {exc}"}
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         # the same systems the GPU solved: a stratified sample copied to the host
@@ -418,7 +569,7 @@ def run_b200(args):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "bf16x3+f32+f64" if args.precision == "mixed" else "f64",
+        "vs_baseline": None, "dtype": "tf32x3+f32+f64" if args.precision == "mixed" else "f64",
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "systems_per_gpu": args.systems, "precision": args.precision,
                    "rows_per_gpu": wl.n_rows, "l2": "inputs (~12 GB) larger than L2; no flush",
@@ -427,6 +578,8 @@ def run_b200(args):
         "roofline": roofline,
         "plain_fp64": {"ms_per_step": plain_ms, "value": world * args.systems / (plain_ms / 1000.0),
                        "speedup_of_headline": plain_ms / ms},
+        "plain_fp64_per_node": (dict(per_node, speedup_of_headline=value / (world * per_node["value"]))
+                                if per_node else None),
         "status_ok_fraction": ok,
         "fp64_resolve_fraction": float(np.mean((info & N.INFO_FP64_RESOLVE) != 0)),
         "mean_refine_passes_tensor_class": float(np.mean(((info >> N.INFO_REFINE_SHIFT) & 255)[p_all >= 33])),
@@ -437,6 +590,7 @@ def run_b200(args):
         "clocks": clk,
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "legs": legs,
     }
     print(json.dumps(line), flush=True)
 

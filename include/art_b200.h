@@ -73,7 +73,7 @@ typedef struct CUstream_st* art_stream_t; /* == cudaStream_t */
 
 /* ---- precision forms ---------------------------------------------------- */
 #define ART_PRECISION_FP64 0   /* plain form: FP64 Gram, FP64 Cholesky        */
-#define ART_PRECISION_MIXED 1  /* tcgen05 BF16 hi/lo split-product Gram with
+#define ART_PRECISION_MIXED 1  /* tcgen05 TF32 hi/lo split-product Gram with
                                   FP32 accumulation, FP32 Cholesky, FP64
                                   iterative refinement on residuals recomputed
                                   from the data in FP64; systems that do not
@@ -146,7 +146,7 @@ typedef struct ArtRidgeResult {
 ART_API size_t art_ridge_workspace_size(int64_t count, int32_t max_features);
 /* Weighted Grams only, by the mixed form's tensor-core path: for every system
  * with 33 <= p <= 160 and d <= ART_MAX_DIM, G' = sum_k q_k phi_k phi_k^T from
- * BF16 hi/lo split products accumulated in FP32, written as the packed lower
+ * TF32 hi/lo split products accumulated in FP32, written as the packed lower
  * triangle (row i holds G'[i][0..i]) at gram + k * gram_stride (floats), with
  * status[k] = 0; other systems get status -4.  The GPU Gram / host solve
  * split of the reference's hybrid optimizer (art/_cuda_hybrid_gram.py:115-169)

@@ -201,7 +201,7 @@ def _oracle_check(wl, out, solver="normal"):
 
 @pytest.mark.parametrize("seed,K,n_max", [(7, 96, 700), (8, 24, 5000)])
 def test_batched_mixed_matches_oracle(seed, K, n_max):
-    """Mixed form (tcgen05 BF16x3 Gram, FP32 Cholesky, FP64 refinement) meets the
+    """Mixed form (tcgen05 TF32x3 Gram, FP32 Cholesky, FP64 refinement) meets the
     same FP64 tolerance as the plain form; systems it cannot refine are re-solved."""
 
     from art import _native as N
@@ -238,7 +238,7 @@ def test_batched_mixed_fp64_factor_matches_oracle(seed, K, n_max):
 
 
 def test_tensor_core_gram_accuracy():
-    """BF16 hi/lo split products, FP32 accumulation in chains of at most 256 rows
+    """TF32 hi/lo split products, FP32 accumulation in chains of at most 256 rows
     summed in FP32: ||G' - G||_F <= 3e-6 ||G||_F for every system."""
 
     from art.models import ridge_gram_batched
