@@ -102,7 +102,7 @@ class ArtSplitProblem(C.Structure):
     _fields_ = [
         ("seg", ArtSegments), ("x", P), ("y", P), ("temperature", P), ("ridge", P),
         ("parent_loss", P), ("min_side_fallback", P), ("theta0", P), ("theta_stride", I64),
-        ("max_dim", I32), ("max_features", I32),
+        ("max_dim", I32), ("max_features", I32), ("node_keys", P),
     ]
 
 
@@ -143,6 +143,7 @@ SIGNATURES = {
                                   C.POINTER(ArtSplitResult), P, C.c_size_t, P]),
     "art_hit_and_run": (C.c_int, [C.POINTER(ArtPolytopes), C.POINTER(ArtChains), P]),
     "art_partition_rows": (C.c_int, [C.POINTER(ArtSegments), P, P, I64, P, P, P, P]),
+    "art_segment_residuals": (C.c_int, [C.POINTER(ArtSegments), P, P, P, I64, P, P, P]),
     "art_tree_predict": (C.c_int, [I32, I64, P, P, I64, P, I64, P, I64, P, P, P, P]),
     "art_last_error": (C.c_char_p, []),
     "art_abi_version": (C.c_int, []),

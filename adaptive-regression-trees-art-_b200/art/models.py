@@ -626,3 +626,32 @@ def _as_2d(X) -> np.ndarray:
     if X.ndim != 2:
         raise ValueError(f"X must have shape (n, d), got {X.shape}.")
     return X
+
+
+def segment_residuals(x, y, row_offsets, dims, features, beta, *, x_offsets=None, stream=None):
+    """Per segment k: (sum (y - phi(x) . beta_k)^2, sum y^2) on the device.
+
+    ``beta`` is (K, stride) with each segment's coefficients in its model's
+    feature order; returns two float64 tensors of length K.
+    """
+
+    t = torch()
+    lib = N.load_library()
+    dev = require_cuda()
+    x = to_device(x, t.float64, dev)
+    y = to_device(y, t.float64, dev)
+    ro = to_device(row_offsets, t.int64, dev)
+    dims_t = to_device(dims, t.int32, dev)
+    feats = to_device(features, t.int32, dev)
+    K = int(dims_t.numel())
+    if x_offsets is None:
+        x_offsets = ro[:-1] * dims_t.to(t.int64)
+    xo = to_device(x_offsets, t.int64, dev)
+    b = to_device(beta, t.float64, dev)
+    sse = t.empty(K, dtype=t.float64, device=dev)
+    ssy = t.empty(K, dtype=t.float64, device=dev)
+    seg = N.ArtSegments(K, ptr(ro), ptr(xo), ptr(dims_t), ptr(feats))
+    N.check(lib.art_segment_residuals(C.byref(seg), ptr(x), ptr(y), ptr(b), int(b.shape[1]), ptr(sse), ptr(ssy),
+                                      stream_handle(stream)), "art_segment_residuals")
+    sse._keepalive = (x, y, ro, xo, dims_t, feats, b)
+    return sse, ssy

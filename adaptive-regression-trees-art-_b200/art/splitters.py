@@ -171,11 +171,14 @@ def split_params(s: "SoftObliqueSplitter", hard_refit: bool, anneal_ratio: float
 def split_level(splitter: "SoftObliqueSplitter", x, y, row_offsets, dims, features, temperature, ridge,
                 *, x_offsets=None, parent_loss=None, min_side_fallback=None, theta0=None,
                 hard_refit: bool = True, anneal_ratio: float = 1.0, seed: int = 0, traces: bool = False,
-                max_dim: int | None = None, max_features: int | None = None, stream=None) -> LevelResult:
+                max_dim: int | None = None, max_features: int | None = None, node_keys=None,
+                stream=None) -> LevelResult:
     """Split K nodes in one launch sequence; arrays are numpy or torch (moved to the device).
 
     theta0, when given, is (K, R, d_max + 1); otherwise restarts start from
-    device draws keyed by ``seed`` (unit Gaussian w, z = median(X w)).
+    device draws keyed by ``seed`` and the node's position k (unit Gaussian w,
+    z = median(X w)), or by ``node_keys[k]`` (uint64 per node) when given, so
+    that a node's draws do not depend on the batch it is solved in.
     """
 
     t = torch()
@@ -225,8 +228,12 @@ def split_level(splitter: "SoftObliqueSplitter", x, y, row_offsets, dims, featur
         out.trace_step = t.full((K, R, max(M, 1)), float("nan"), dtype=t.float64, device=dev)
         out.trace_backtracks = t.full((K, R, max(M, 1)), -1, dtype=t.int32, device=dev)
     seg = N.ArtSegments(K, ptr(ro), ptr(xo), ptr(dims_t), ptr(feats))
+    nk = None
+    if node_keys is not None:
+        nk = to_device(np.asarray(node_keys, dtype=np.uint64).view(np.int64) if not isinstance(node_keys, t.Tensor)
+                       else node_keys, t.int64, dev)
     prob = N.ArtSplitProblem(seg, ptr(x), ptr(y), ptr(temp), ptr(rid), ptr(pl), ptr(fb), ptr(th0), stride,
-                             int(max_dim), int(max_features))
+                             int(max_dim), int(max_features), ptr(nk))
     prm = split_params(splitter, hard_refit, anneal_ratio, seed)
     res = N.ArtSplitResult(ptr(out.theta), max_dim + 1, ptr(out.beta), max_features, ptr(out.loss),
                            ptr(out.child_loss), ptr(out.ridge_effective), ptr(out.n_right), ptr(out.n_iters),
@@ -237,7 +244,7 @@ def split_level(splitter: "SoftObliqueSplitter", x, y, row_offsets, dims, featur
     ws = WORKSPACES.get(nbytes, stream)
     N.check(lib.art_split_level(C.byref(prob), C.byref(prm), C.byref(res), ptr(ws), ws.numel(),
                                 stream_handle(stream)), "art_split_level")
-    out._keepalive = (x, y, ro, xo, dims_t, feats, temp, rid, pl, fb, th0)
+    out._keepalive = (x, y, ro, xo, dims_t, feats, temp, rid, pl, fb, th0, nk)
     return out
 
 

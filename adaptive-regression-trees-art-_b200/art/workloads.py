@@ -339,3 +339,24 @@ def polytopes(count: int = 16384, d: int = 8, seed: int = 4, k_min: int = 4, k_m
                             to(ro, torch.int64), to(A, torch.float64), to(b, torch.float64), int(k_max),
                             to(c, torch.float64), to(np.arange(Cn), torch.int32),
                             to((np.uint64(seed) << np.uint64(32)) + np.arange(Cn, dtype=np.uint64), torch.int64), d)
+
+
+def bumps_ridge_2d(seed: int = 1):
+    """Target on [-1,1]^2: 3 Gaussian bumps (centres U[-0.8,0.8]^2, widths
+    U[0.2,0.5], amplitudes N(0,1)) + tanh(8 (a.x - b)), a a random unit
+    vector, b ~ U(-0.3, 0.3).  Returns a vectorised numpy callable."""
+
+    rng = np.random.default_rng(seed)
+    centres = rng.uniform(-0.8, 0.8, (3, 2))
+    widths = rng.uniform(0.2, 0.5, 3)
+    amps = rng.normal(size=3)
+    a = rng.normal(size=2)
+    a /= np.linalg.norm(a)
+    b = rng.uniform(-0.3, 0.3)
+
+    def f(X):
+        X = np.atleast_2d(X)
+        r2 = ((X[:, None, :] - centres[None]) ** 2).sum(-1)
+        return (amps * np.exp(-r2 / (2 * widths ** 2))).sum(1) + np.tanh(8 * (X @ a - b))
+
+    return f

@@ -119,6 +119,122 @@ __device__ int chol_packed(T* A, int p, int* s_fail) {
   return 0;
 }
 
+// The same factorisation with 32-column blocks: the diagonal block is
+// factored by warp 0 in registers (lane i holds row i of the block), the
+// panel below it by one thread per row, and the trailing matrix is updated
+// in 8x8 register tiles with a 32-deep inner loop -- four times fewer block
+// steps (and block barriers) than chol_packed for the same arithmetic.
+template <typename T>
+__device__ int chol_packed32(T* A, int p, int* s_fail) {
+  constexpr int NB = 32, CT = 8;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nthreads = blockDim.x;
+  if (tid == 0) *s_fail = 0;
+  __syncthreads();
+  for (int j0 = 0; j0 < p; j0 += NB) {
+    const int jb = min(NB, p - j0);
+    if (warp == 0) {
+      T row[NB];
+#pragma unroll
+      for (int c = 0; c < NB; ++c) row[c] = (lane < jb && c <= lane) ? A[pk(j0 + lane, j0 + c)] : T(0);
+      int fail = 0;
+#pragma unroll
+      for (int c = 0; c < NB; ++c) {
+        if (c < jb && !fail) {
+          const T dc = __shfl_sync(0xffffffffu, row[c], c);
+          if (!(dc > T(0)) || !isfinite((double)dc)) {
+            fail = j0 + c + 1;
+          } else {
+            const T lcc = sqrt(dc);
+            if (lane == c) row[c] = lcc;
+            else if (lane > c && lane < jb) row[c] = row[c] / lcc;
+#pragma unroll
+            for (int k = c + 1; k < NB; ++k) {
+              const T lkc = __shfl_sync(0xffffffffu, row[c], k);
+              if (k < jb && lane >= k && lane < jb) row[k] -= row[c] * lkc;
+            }
+          }
+        }
+      }
+      if (!fail && lane < jb) {
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+          if (c <= lane) A[pk(j0 + lane, j0 + c)] = row[c];
+      }
+      if (lane == 0 && fail) *s_fail = fail;
+    }
+    __syncthreads();
+    if (*s_fail) return *s_fail;
+    const int j1 = j0 + jb;
+    // panel: rows i >= j1, L[i, j0:j1] = A[i, j0:j1] L_JJ^{-T}
+    for (int i = j1 + tid; i < p; i += nthreads) {
+      T a[NB];
+#pragma unroll
+      for (int c = 0; c < NB; ++c) a[c] = (c < jb) ? A[pk(i, j0 + c)] : T(0);
+#pragma unroll
+      for (int c = 0; c < NB; ++c) {
+        if (c < jb) {
+          T sacc = a[c];
+          const T* lr = A + pk(j0 + c, j0);
+#pragma unroll
+          for (int k = 0; k < NB; ++k)
+            if (k < c) sacc -= a[k] * lr[k];
+          a[c] = sacc / lr[c];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < NB; ++c)
+        if (c < jb) A[pk(i, j0 + c)] = a[c];
+    }
+    __syncthreads();
+    // trailing update of the lower triangle of A[j1:p, j1:p] in CTxCT tiles
+    const int m = p - j1;
+    if (m > 0) {
+      const int nbt = (m + CT - 1) / CT;
+      const int ntiles = nbt * (nbt + 1) / 2;
+      for (int t = tid; t < ntiles; t += nthreads) {
+        int I = (int)((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
+        while (I * (I + 1) / 2 > t) --I;
+        while ((I + 1) * (I + 2) / 2 <= t) ++I;
+        const int J = t - I * (I + 1) / 2;
+        const int rb = j1 + CT * I, cb = j1 + CT * J;
+        const T* ra[CT];
+        const T* rc[CT];
+#pragma unroll
+        for (int i = 0; i < CT; ++i) {
+          ra[i] = A + pk(min(rb + i, p - 1), j0);
+          rc[i] = A + pk(min(cb + i, p - 1), j0);
+        }
+        T acc[CT][CT];
+#pragma unroll
+        for (int i = 0; i < CT; ++i)
+#pragma unroll
+          for (int j = 0; j < CT; ++j) acc[i][j] = T(0);
+        for (int c = 0; c < jb; ++c) {
+          T ai[CT], bj[CT];
+#pragma unroll
+          for (int i = 0; i < CT; ++i) ai[i] = ra[i][c];
+#pragma unroll
+          for (int j = 0; j < CT; ++j) bj[j] = rc[j][c];
+#pragma unroll
+          for (int i = 0; i < CT; ++i)
+#pragma unroll
+            for (int j = 0; j < CT; ++j) acc[i][j] = fma(ai[i], bj[j], acc[i][j]);
+        }
+#pragma unroll
+        for (int i = 0; i < CT; ++i)
+#pragma unroll
+          for (int j = 0; j < CT; ++j) {
+            const int r = rb + i, c = cb + j;
+            if (r < p && c <= r) A[pk(r, c)] -= acc[i][j];
+          }
+      }
+    }
+    __syncthreads();
+  }
+  return 0;
+}
+
 // Solve L z = b in place (z initially b), one warp, L packed lower.
 template <typename T, typename V>
 __device__ void warp_forward(const T* L, V* z, int p) {

@@ -143,7 +143,10 @@ __device__ inline bool finish_fp64(const RidgeArgs& a, const RidgeLists& L, int 
     if (tid == 0) s_scalar[1] = an;
   }
   __syncthreads();
-  const int fail = chol_packed<double, CT>(G, p, s_fail);
+  // wide systems: 32-column blocks; narrow ones keep the small-register form
+  int fail;
+  if constexpr (CT == 8) fail = chol_packed32<double>(G, p, s_fail);
+  else fail = chol_packed<double, CT>(G, p, s_fail);
   if (fail) {
     if (a.solver == ART_SOLVER_AUTO) {
       if (tid == 0) {

@@ -13,14 +13,20 @@
 //     G' = Hi Hi^T + Hi Lo^T + Lo Hi^T with M = 128 feature rows per tile
 //     (tile 1: features 0..127 x 0..P16-1; tile 2 covers features >= 128),
 //     committed to an mbarrier per stage so operand buffers recycle.
-//  3. The FP32 Gram is drained from TMEM (tcgen05.ld 32x32b), its diagonal
-//     replaced by the exact FP64 diag + lambda, and factored by an FP32
-//     Cholesky.
+//  3. The FP32 Gram is drained from TMEM (tcgen05.ld 32x32b) into shared
+//     memory every kDrainChunks chunks, its diagonal replaced by the exact
+//     FP64 diag + lambda, and factored by an FP32 Cholesky; the factor is
+//     then inverted in place, so M^{-1} = L^{-T} L^{-1} is applied by two
+//     block-wide matrix-vector products.
 //  4. FP64 iterative refinement: r = h - (G + lambda I) beta with G beta
-//     recomputed from the rows in FP64 each pass, delta = M^{-1} r with the
-//     FP32 factor, until the step is below 1e-12 of beta and has stopped
-//     shrinking.  Systems that fail the FP32 factorisation, stall, or carry
-//     bad inputs are appended to the FP64 resolve list.
+//     recomputed from the rows in FP64 each pass (one warp per row, phi
+//     formed once per row for both products), delta = M^{-1} r, until the
+//     estimated remaining error (step * rho / (1 - rho), rho the step ratio)
+//     is below 1e-13 of beta.  Systems that fail the FP32 factorisation,
+//     stall, or carry bad inputs are appended to the FP64 resolve list.
+// One operand stage (hi, lo) and two row stages keep a CTA near 110 KB of
+// shared memory, so two CTAs share an SM and one's solve phase overlaps the
+// other's tensor-core loop.
 // Every wait on an mbarrier is bounded; TMEM is allocated once per CTA and
 // always released before the CTA exits.
 #include <algorithm>
@@ -44,7 +50,7 @@ constexpr int kMaxRefine = 14;
 // FP32 accumulator of the tensor core loses low bits on every step, so the
 // chain length bounds the Gram error (~steps * 2^-24 relative); drained
 // partial Grams are summed in shared memory with round-to-nearest adds.
-constexpr int kDrainChunks = 8;
+constexpr int kDrainChunks = 4;
 
 // ------------------------------------------------------------- PTX wrappers
 __device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t ncols) {
@@ -125,7 +131,7 @@ __host__ __device__ inline TcLayout tc_layout(int pmax, int dmax, int factor_byt
   L.q = o; o = a16(o + kKC * 8);
   L.sq = o; o = a16(o + kKC * 8);
   o = (o + 127) & ~(size_t)127;
-  L.op = o; o = a16(o + (size_t)4 * kOpBytes);     // 2 stages x (hi, lo)
+  L.op = o; o = a16(o + (size_t)2 * kOpBytes);     // one stage: hi, lo
   L.bars = o; o = a16(o + 4 * 8);
   L.tmem = o; o = a16(o + 16);
   L.gram = o; o = a16(o + (size_t)pmax * (pmax + 1) / 2 * factor_bytes);
@@ -197,6 +203,17 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
     const int N1 = P16, N2 = two ? P16 - 128 : 0;
     const int g0 = two ? (P16 - 128) / 8 : 0;
     const int64_t nchunks = (it.n + kKC - 1) / kKC;
+    // bulk copies of rows [c*kKC, c*kKC + rows) of x and w into row stage st
+    // (the refinement passes need no y)
+    auto issue_rows = [&](int64_t c, int st) {
+      const int64_t rr = c * kKC;
+      const int rows = (int)min((int64_t)kKC, it.n - rr);
+      Granules gx = granules(a.x + it.xoff + rr * it.d, (uint64_t)rows * it.d * 8);
+      Granules gw = a.w ? granules(a.w + it.r0 + rr, (uint64_t)rows * 8) : Granules{nullptr, 0, 0};
+      mbar_arrive_expect_tx(&load_bar[st], gx.bytes + gw.bytes);
+      bulk_g2s(smem + lay.x[st], gx.base, gx.bytes, &load_bar[st]);
+      if (a.w) bulk_g2s(smem + lay.w[st], gw.base, gw.bytes, &load_bar[st]);
+    };
     if (nchunks == 0) {  // nothing to accumulate: the FP64 form reports the status
       if (tid == 0) push_list(L, a.K, CLS_RESOLVE, k);
       continue;
@@ -229,13 +246,17 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
     for (int64_t c = 0; c < nchunks && !abort; ++c) {
       const int st = (int)(c & 1);
       const bool okl = mbar_wait(&load_bar[st], S.load_uses[st] & 1);
-      // the MMAs that last read this stage's operands (two chunks back) must be
-      // done; a drain since then has already consumed their commit
-      const bool mpend = S.mma_waits[st] < S.mma_commits[st];
-      const bool okm = mpend ? mbar_wait(&mma_bar[st], S.mma_waits[st] & 1) : true;
+      // one operand buffer: every MMA issued so far (chunks c-2 on barrier st,
+      // c-1 on barrier st^1) must be done before it is rewritten; a drain
+      // since then has already consumed those commits
+      const bool p0 = S.mma_waits[st] < S.mma_commits[st];
+      const bool p1 = S.mma_waits[st ^ 1] < S.mma_commits[st ^ 1];
+      bool okm = p0 ? mbar_wait(&mma_bar[st], S.mma_waits[st] & 1) : true;
+      okm = okm && (p1 ? mbar_wait(&mma_bar[st ^ 1], S.mma_waits[st ^ 1] & 1) : true);
       if (!__syncthreads_and(okl && okm)) { abort = true; break; }
       S.load_uses[st]++;
-      if (mpend) S.mma_waits[st]++;
+      if (p0) S.mma_waits[st]++;
+      if (p1) S.mma_waits[st ^ 1]++;
       const int rows = (int)min((int64_t)kKC, it.n - c * kKC);
       const double* xs = (const double*)(smem + lay.x[st] +
                                          (((uintptr_t)(a.x + it.xoff + c * kKC * d)) & 15));
@@ -257,7 +278,7 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
         sq_s[tid] = sqrt(qv);
       }
       __syncthreads();
-      unsigned char* hi = op + (size_t)st * 2 * kOpBytes;
+      unsigned char* hi = op;
       unsigned char* lo = hi + kOpBytes;
       const int nitems = P16 * (kKC / 8);
 #pragma unroll
@@ -438,113 +459,13 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
       const double an = warp_sym_norm1(Gf, p);
       if (lane == 0) s_scalar[1] = an;
     }
-    const int fail = chol_packed<TF, 8>(Gf, p, &s_fail);
+    const int fail = chol_packed32<TF>(Gf, p, &s_fail);
     if (fail) {
       if (tid == 0) push_list(L, a.K, CLS_RESOLVE, k);
       continue;
     }
-    // ---- FP64 iterative refinement
-    for (int f = tid; f < p; f += kTcThreads) { beta[f] = 0.0; r[f] = h[f]; }
-    __syncthreads();
-    const int dp = d + 1;  // padded row stride in the refinement buffer
-    int KR = (int)((size_t)(4 * kOpBytes) / ((size_t)dp * 8 + 16));
-    KR = min(KR, kTcThreads);
-    double* xr = (double*)op;           // KR rows, stride dp
-    double* se = xr + (size_t)KR * dp;  // KR scaled row errors
-    double nd_prev = 0.0;
-    int outcome = 0;  // 1 converged, 2 stalled/failed
-    uint32_t info = 0;
-    int passes = 0;
-    for (int iter = 0; iter < kMaxRefine && outcome == 0; ++iter) {
-      passes = iter;
-      if (iter > 0) {
-        // r = h - lambda beta - sum_k q_k (phi_k . beta) phi_k, in FP64 from the rows.
-        // Phase 1: one warp per row, lane l owns features l + 32 m (m < 5).
-        int fa_r[5], fb_r[5];
-        double b_r[5];
-#pragma unroll
-        for (int m = 0; m < 5; ++m) {
-          const int f = lane + 32 * m;
-          fa_r[m] = f < p ? fidx[2 * f] : -3;
-          fb_r[m] = f < p ? fidx[2 * f + 1] : -1;
-          b_r[m] = f < p ? beta[f] : 0.0;
-        }
-        // per-lane accumulators of sum_k q_k e_k phi_f for the lane's features
-        double acc_r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-        for (int64_t c0 = 0; c0 < it.n; c0 += KR) {
-          const int rows = (int)min((int64_t)KR, it.n - c0);
-          for (int e = tid; e < rows * d; e += kTcThreads) {
-            const int rr = e / d, cc = e - rr * d;
-            xr[rr * dp + cc] = a.x[it.xoff + (c0 + rr) * d + cc];
-          }
-          for (int rr = tid; rr < rows; rr += kTcThreads)
-            se[rr] = fmax(a.w ? a.w[it.r0 + c0 + rr] : 1.0, a.weight_floor);
-          __syncthreads();
-          for (int rr = warp; rr < rows; rr += kTcThreads / 32) {
-            const double* xk = xr + rr * dp;
-            double ph[5];
-            double e_ = 0.0;
-#pragma unroll
-            for (int m = 0; m < 5; ++m) {
-              ph[m] = fa_r[m] == -3 ? 0.0
-                                    : (fa_r[m] < 0 ? 1.0 : xk[fa_r[m]]) * (fb_r[m] < 0 ? 1.0 : xk[fb_r[m]]);
-              e_ = fma(ph[m], b_r[m], e_);
-            }
-            e_ = warp_sum(e_) * se[rr];
-#pragma unroll
-            for (int m = 0; m < 5; ++m) acc_r[m] = fma(e_, ph[m], acc_r[m]);
-          }
-          __syncthreads();
-        }
-        // reduce the 8 warps' partial sums in a fixed order
-        double* part = xr;  // reuse: [warp][160]
-#pragma unroll
-        for (int m = 0; m < 5; ++m) part[warp * kPmax + lane + 32 * m] = acc_r[m];
-        __syncthreads();
-        double accf = 0.0;
-        if (tid < p)
-          for (int ww = 0; ww < kTcThreads / 32; ++ww) accf += part[ww * kPmax + tid];
-        if (tid < p) r[tid] = h[tid] - lam * beta[tid] - accf;
-        __syncthreads();
-      }
-      if (warp == 0) {
-        for (int f = lane; f < p; f += 32) v1[f] = r[f];
-        __syncwarp();
-        warp_forward<TF, double>(Gf, v1, p);
-        warp_backward<TF, double>(Gf, v1, p);
-        double nd = 0.0, nb = 0.0;
-        for (int f = lane; f < p; f += 32) {
-          const double b = beta[f] + v1[f];
-          beta[f] = b;
-          nd = fmax(nd, fabs(v1[f]));
-          nb = fmax(nb, fabs(b));
-        }
-        nd = warp_max(nd);
-        nb = warp_max(nb);
-        if (lane == 0) {
-          int out = 0;
-          if (!(nd <= 1e300) || !(nb <= 1e300)) out = 2;           // non-finite
-          else if (nd <= 2.3e-16 * nb) out = 1;                     // at working precision
-          else if (iter >= 1 && nd > 0.75 * nd_prev) out = (nd <= 1e-12 * nb) ? 1 : 2;
-          else if (iter == kMaxRefine - 1) out = (nd <= 1e-12 * nb) ? 3 : 2;
-          s_flag = out;
-        }
-        nd_prev = nd;
-      }
-      __syncthreads();
-      outcome = s_flag;
-      if (outcome == 3) { outcome = 1; info |= ART_INFO_REFINE_CAP; }
-    }
-    info |= (uint32_t)min(passes, 255) << ART_INFO_REFINE_SHIFT;
-    if (outcome != 1) {
-      if (tid == 0) {
-        push_list(L, a.K, CLS_RESOLVE, k);
-        if (a.info) a.info[k] = info;  // the FP64 form ORs its own bits in
-      }
-      continue;
-    }
     double cond = __longlong_as_double(0x7ff8000000000000ll);
-    if (want_cond) {
+    if (want_cond) {  // 1-norm estimate from the factor (dpocon's method)
       if (warp == 0) {
         const double est = warp_inv_norm1_estimate<TF>(Gf, p, v1, v2);
         if (lane == 0) {
@@ -560,6 +481,184 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
         continue;
       }
       cond = rcond > 0.0 ? sqrt(1.0 / fmin(rcond, 1.0)) : __longlong_as_double(0x7ff0000000000000ll);
+    }
+    // ---- M^{-1} v = L^{-T} L^{-1} v by blocked triangular solves: each
+    // 32-row diagonal block is solved by warp 0 in registers, then every
+    // thread updates the rows beyond the block (one row per thread).
+    double* part = (double*)op;  // [8 row slots][kPmax]
+    auto apply_minv = [&](const double* v, double* out) {
+      for (int i = tid; i < p; i += kTcThreads) out[i] = v[i];
+      __syncthreads();
+      for (int j0 = 0; j0 < p; j0 += 32) {           // L y = v
+        const int bs = min(32, p - j0);
+        if (warp == 0) {
+          double zl = lane < bs ? out[j0 + lane] : 0.0;
+          for (int t2 = 0; t2 < bs; ++t2) {
+            if (lane == t2) zl = zl / (double)Gf[pk(j0 + t2, j0 + t2)];
+            const double yt = __shfl_sync(0xffffffffu, zl, t2);
+            if (lane > t2 && lane < bs) zl -= (double)Gf[pk(j0 + lane, j0 + t2)] * yt;
+          }
+          if (lane < bs) out[j0 + lane] = zl;
+        }
+        __syncthreads();
+        for (int i = j0 + bs + tid; i < p; i += kTcThreads) {
+          double sacc = 0.0;
+          for (int t2 = 0; t2 < bs; ++t2) sacc = fma((double)Gf[pk(i, j0 + t2)], out[j0 + t2], sacc);
+          out[i] -= sacc;
+        }
+        __syncthreads();
+      }
+      for (int j0 = ((p - 1) / 32) * 32; j0 >= 0; j0 -= 32) {   // L^T x = y
+        const int bs = min(32, p - j0);
+        if (warp == 0) {
+          double zl = lane < bs ? out[j0 + lane] : 0.0;
+          for (int t2 = bs - 1; t2 >= 0; --t2) {
+            if (lane == t2) zl = zl / (double)Gf[pk(j0 + t2, j0 + t2)];
+            const double xt = __shfl_sync(0xffffffffu, zl, t2);
+            if (lane < t2) zl -= (double)Gf[pk(j0 + t2, j0 + lane)] * xt;
+          }
+          if (lane < bs) out[j0 + lane] = zl;
+        }
+        __syncthreads();
+        for (int i = tid; i < j0; i += kTcThreads) {
+          double sacc = 0.0;
+          for (int t2 = 0; t2 < bs; ++t2) sacc = fma((double)Gf[pk(j0 + t2, i)], out[j0 + t2], sacc);
+          out[i] -= sacc;
+        }
+        __syncthreads();
+      }
+    };
+    // ---- FP64 iterative refinement.  Residual passes: one warp per row (8
+    // rows per step), lane l owns features l + 32 m (m < 5) with their beta
+    // in registers; phi is formed once per row and used for both
+    // e_k = q_k phi_k . beta (warp shuffle sum) and the accumulation of
+    // e_k phi_k; the 8 row slots are summed in a fixed order at the end.
+    const int slot = warp, fl = lane;
+    int rfa[5], rfb[5];
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+      const int f = fl + 32 * m;
+      rfa[m] = f < p ? fidx[2 * f] : -3;
+      rfb[m] = f < p ? fidx[2 * f + 1] : -1;
+    }
+    apply_minv(h, beta);   // beta_0 = M^{-1} h
+    double nd_prev = 0.0;
+    {
+      if (warp == 0) {
+        double m0 = 0.0;
+        for (int f = lane; f < p; f += 32) m0 = fmax(m0, fabs(beta[f]));
+        m0 = warp_max(m0);
+        if (lane == 0) s_scalar[3] = m0;
+      }
+      __syncthreads();
+      nd_prev = s_scalar[3];
+    }
+    int outcome = (nd_prev <= 1e300) ? 0 : 2;  // 1 converged, 2 stalled/failed
+    uint32_t info = 0;
+    int passes = 0;
+    for (int iter = 1; iter < kMaxRefine && outcome == 0; ++iter) {
+      passes = iter;
+      double bt[5], accb[5];
+#pragma unroll
+      for (int m = 0; m < 5; ++m) {
+        const int f = fl + 32 * m;
+        bt[m] = f < p ? beta[f] : 0.0;
+        accb[m] = 0.0;
+      }
+      // rows stream through the two row stages again (bulk copies of x and
+      // w, prefetched two chunks ahead); warp `slot` takes rows slot, slot+8,
+      // ... of each chunk, so every warp stays converged
+      const int64_t nch = (it.n + kKC - 1) / kKC;
+      if (tid == 0)
+        for (int64_t c = 0; c < min((int64_t)2, nch); ++c) issue_rows(c, (int)c);
+      for (int64_t c = 0; c < min((int64_t)2, nch); ++c) S.load_issued[c]++;
+      for (int64_t c = 0; c < nch && !abort; ++c) {
+        const int st = (int)(c & 1);
+        const bool okl = mbar_wait(&load_bar[st], S.load_uses[st] & 1);
+        if (!__syncthreads_and(okl)) { abort = true; break; }
+        S.load_uses[st]++;
+        const int rows = (int)min((int64_t)kKC, it.n - c * kKC);
+        const double* xs = (const double*)(smem + lay.x[st] +
+                                           (((uintptr_t)(a.x + it.xoff + c * kKC * d)) & 15));
+        const double* ws = a.w ? (const double*)(smem + lay.w[st] +
+                                                 (((uintptr_t)(a.w + it.r0 + c * kKC)) & 15))
+                               : nullptr;
+        for (int j = slot; j < rows; j += kTcThreads / 32) {
+          const double* xk = xs + j * d;
+          double ph[5];
+          double dot = 0.0;
+#pragma unroll
+          for (int m = 0; m < 5; ++m) {
+            const int ua = rfa[m], ub = rfb[m];
+            const double va = ua >= 0 ? xk[ua] : (ua == -1 ? 1.0 : 0.0);
+            const double vb = ub >= 0 ? xk[ub] : 1.0;
+            ph[m] = va * vb;
+            dot = fma(ph[m], bt[m], dot);
+          }
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
+          const double e = fmax(ws ? ws[j] : 1.0, a.weight_floor) * dot;
+#pragma unroll
+          for (int m = 0; m < 5; ++m) accb[m] = fma(e, ph[m], accb[m]);
+        }
+        __syncthreads();  // every warp is done with this stage
+        if (c + 2 < nch) {
+          if (tid == 0) issue_rows(c + 2, st);
+          S.load_issued[st]++;
+        }
+      }
+      if (abort) break;
+#pragma unroll
+      for (int m = 0; m < 5; ++m) {
+        const int f = fl + 32 * m;
+        if (f < p) part[slot * kPmax + f] = accb[m];
+      }
+      __syncthreads();
+      for (int f = tid; f < p; f += kTcThreads) {
+        double sacc = 0.0;
+        for (int sl = 0; sl < kTcThreads / 32; ++sl) sacc += part[sl * kPmax + f];
+        r[f] = h[f] - lam * beta[f] - sacc;
+      }
+      __syncthreads();
+      apply_minv(r, v1);   // correction
+      if (warp == 0) {
+        double nd = 0.0, nb = 0.0;
+        for (int f = lane; f < p; f += 32) {
+          const double b = beta[f] + v1[f];
+          beta[f] = b;
+          nd = fmax(nd, fabs(v1[f]));
+          nb = fmax(nb, fabs(b));
+        }
+        nd = warp_max(nd);
+        nb = warp_max(nb);
+        if (lane == 0) {
+          int out = 0;
+          const double rho = nd_prev > 0.0 ? nd / nd_prev : 0.0;
+          if (!(nd <= 1e300) || !(nb <= 1e300)) out = 2;                       // non-finite
+          else if (nd <= 2.3e-16 * nb) out = 1;                                 // at working precision
+          else if (rho < 0.75 && nd * rho / (1.0 - rho) <= 1e-13 * nb) out = 1; // remaining error tiny
+          else if (rho >= 0.75) out = (nd <= 1e-12 * nb) ? 1 : 2;              // stalled
+          else if (iter == kMaxRefine - 1) out = (nd <= 1e-12 * nb) ? 3 : 2;
+          s_flag = out;
+          s_scalar[3] = nd;
+        }
+      }
+      __syncthreads();
+      outcome = s_flag;
+      nd_prev = s_scalar[3];
+      if (outcome == 3) { outcome = 1; info |= ART_INFO_REFINE_CAP; }
+    }
+    if (abort) {  // a bounded wait gave up in a refinement pass
+      if (tid == 0) { atomicExch(L.err, 1); a.status[k] = -5; }
+      break;
+    }
+    info |= (uint32_t)min(passes, 255) << ART_INFO_REFINE_SHIFT;
+    if (outcome != 1) {
+      if (tid == 0) {
+        push_list(L, a.K, CLS_RESOLVE, k);
+        if (a.info) a.info[k] = info;  // the FP64 form ORs its own bits in
+      }
+      continue;
     }
     for (int f = tid; f < p; f += kTcThreads) a.beta[(int64_t)k * a.beta_stride + f] = beta[f];
     if (tid == 0) {

@@ -28,7 +28,7 @@ constexpr int kWarpThreads = 128;             // 4 independent warps per CTA
 constexpr int kWarpsPerCta = kWarpThreads / 32;
 constexpr int kWRows = 32;                    // rows per batch (one per lane)
 constexpr int kWPad = kWarpMaxAug;            // padded augmented width (multiple of 4)
-constexpr int kWLdr = kWPad + 2;              // row stride of P (even: 16-byte rows)
+constexpr int kWLdr = kWPad + 2;              // row stride of P (even: 16-byte rows; 26 = 10 mod 16 spreads rows over banks)
 
 __host__ __device__ inline size_t wa16(size_t v) { return (v + 15) & ~(size_t)15; }
 
@@ -260,19 +260,23 @@ __global__ void __launch_bounds__(kWarpThreads) ridge_warp_kernel(RidgeArgs a, R
       const double* ws = a.w ? (const double*)(base + lay.w[st] +
                                                (((uintptr_t)(a.w + it.r0 + c * kWRows)) & 15))
                              : nullptr;
-      // 1. lane r forms row r of P (zeros past the last row)
+      // 1. lane r forms row r of P (zeros past the last row).  Lane r starts
+      // its walk over the inputs and features at an offset of r, so the
+      // lanes' strided row accesses spread over the shared-memory banks.
       {
         const int r = lane;
         double* pr = P + r * kWLdr;
         if (r < rows) {
           const double* xr = xs + r * d;
-          for (int j = 0; j < d; ++j) bad |= isfinite(xr[j]) ? 0 : 1;
+          const int j0 = r % d;
+          for (int t = 0, j = j0; t < d; ++t, j = (j + 1 == d) ? 0 : j + 1) bad |= isfinite(xr[j]) ? 0 : 1;
           const double yv = ys[r];
           bad |= isfinite(yv) ? 0 : 1;
           const double wv = ws ? ws[r] : 1.0;
           if (!(wv >= 0.0) || !isfinite(wv)) bad |= 2;
           const double sq = sqrt(fmax(wv, a.weight_floor));
-          for (int f = 0; f < PW; ++f) {
+          const int f0 = r % PW;
+          for (int t = 0, f = f0; t < PW; ++t, f = (f + 1 == PW) ? 0 : f + 1) {
             const int ia = fidx[2 * f], ib = fidx[2 * f + 1];
             double v;
             if (ia == -3) v = 0.0;

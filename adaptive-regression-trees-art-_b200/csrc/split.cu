@@ -53,6 +53,7 @@ struct SplitArgs {
   const int8_t* fallback;
   const double* theta0;
   int64_t theta0_stride;
+  const uint64_t* node_keys;
   ArtSplitParams prm;
   int R, Rg, groups, dmax, pmax, H, TC;
   // per (node, restart) results, index k * R + r
@@ -911,9 +912,16 @@ __global__ void split_init_theta(SplitArgs a, double* theta0, int64_t stride) {
   __shared__ double s_lo, s_hi;
   if (threadIdx.x == 0) {
     double nrm2 = 0.0;
+    // counter: (node k, restart) or, with per-node keys, (restart, node key):
+    // the latter does not depend on the node's position in the batch
+    const int64_t rr = kr - k * a.R;
+    const uint64_t nk = a.node_keys ? a.node_keys[k] : 0ull;
     for (int i = 0; i < d; i += 2) {
-      Philox4 r = philox4x32_10((uint32_t)kr, (uint32_t)(kr >> 32), (uint32_t)i, 0x5eedu,
-                                (uint32_t)a.prm.seed, (uint32_t)(a.prm.seed >> 32));
+      Philox4 r = a.node_keys
+                      ? philox4x32_10((uint32_t)rr, (uint32_t)nk, (uint32_t)i, (uint32_t)(nk >> 32) ^ 0x5eed0000u,
+                                      (uint32_t)a.prm.seed, (uint32_t)(a.prm.seed >> 32))
+                      : philox4x32_10((uint32_t)kr, (uint32_t)(kr >> 32), (uint32_t)i, 0x5eedu,
+                                      (uint32_t)a.prm.seed, (uint32_t)(a.prm.seed >> 32));
       double z0, z1;
       normal_pair(r, z0, z1);
       w[i] = z0;
@@ -1063,6 +1071,7 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
   a.dims = pr->seg.dims; a.features = pr->seg.features;
   a.x = pr->x; a.y = pr->y; a.temperature = pr->temperature; a.ridge = pr->ridge;
   a.parent_loss = pr->parent_loss; a.fallback = pr->min_side_fallback;
+  a.node_keys = pr->node_keys;
   a.prm = *prm;
   a.R = R; a.Rg = Rg; a.groups = (R + Rg - 1) / Rg;
   a.dmax = pr->max_dim; a.pmax = pr->max_features; a.TC = TC;

@@ -103,10 +103,81 @@ __global__ void predict_kernel(int d, int64_t n_nodes, const int32_t* child, con
   if (pred) pred[i] = leaf_predict(xr, d, features[node], coef + (int64_t)node * cs);
 }
 
+// Per segment: sum of squared residuals of phi(x) . beta and sum of y^2.
+// One CTA per segment; each thread walks its rows in order, then a fixed
+// shared-memory tree sums the threads (deterministic for a given segment).
+constexpr int kResThreads = 256;
+__global__ void __launch_bounds__(kResThreads)
+    residual_kernel(ArtSegments seg, const double* x, const double* y, const double* beta,
+                    int64_t bs, double* sse, double* ssy) {
+  const int k = blockIdx.x;
+  const int64_t r0 = seg.row_offsets[k], n = seg.row_offsets[k + 1] - r0;
+  const int64_t xoff = seg.x_offsets[k];
+  const int d = seg.dims[k], kind = seg.features[k];
+  const int p = feature_count(d, kind);
+  __shared__ double b[ART_MAX_FEATURES];
+  __shared__ int16_t fa[ART_MAX_FEATURES], fb[ART_MAX_FEATURES];
+  __shared__ double red[2][kResThreads];
+  for (int f = threadIdx.x; f < p; f += kResThreads) {
+    int u, v;
+    feature_factors(d, kind, f, u, v);
+    fa[f] = (int16_t)u;
+    fb[f] = (int16_t)v;
+    b[f] = beta[(int64_t)k * bs + f];
+  }
+  __syncthreads();
+  double s_e = 0.0, s_y = 0.0;
+  for (int64_t r = threadIdx.x; r < n; r += kResThreads) {
+    const double* xr = x + xoff + r * d;
+    double pred = 0.0;
+    for (int f = 0; f < p; ++f) {
+      const int u = fa[f], v = fb[f];
+      pred = fma((u < 0 ? 1.0 : xr[u]) * (v < 0 ? 1.0 : xr[v]), b[f], pred);
+    }
+    const double yv = y[r0 + r], e = yv - pred;
+    s_e = fma(e, e, s_e);
+    s_y = fma(yv, yv, s_y);
+  }
+  red[0][threadIdx.x] = s_e;
+  red[1][threadIdx.x] = s_y;
+  __syncthreads();
+  for (int h = kResThreads / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) {
+      red[0][threadIdx.x] += red[0][threadIdx.x + h];
+      red[1][threadIdx.x] += red[1][threadIdx.x + h];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    sse[k] = red[0][0];
+    ssy[k] = red[1][0];
+  }
+}
+
 }  // namespace
 }  // namespace art
 
 using namespace art;
+
+extern "C" int art_segment_residuals(const ArtSegments* seg, const double* x, const double* y,
+                                     const double* beta, int64_t beta_stride, double* sse,
+                                     double* ssy, art_stream_t stream) {
+  cudaGetLastError();
+  if (!seg || seg->count < 0) { set_error("art_segment_residuals: bad segments"); return ART_E_INVALID; }
+  if (seg->count == 0) return ART_OK;
+  if (!seg->row_offsets || !seg->x_offsets || !seg->dims || !seg->features || !x || !y || !beta ||
+      !sse || !ssy) {
+    set_error("art_segment_residuals: null argument");
+    return ART_E_INVALID;
+  }
+  if (seg->count > 0x7fffffffll) { set_error("art_segment_residuals: too many segments"); return ART_E_UNSUPPORTED; }
+  prof_begin("segment_residuals", (cudaStream_t)stream);
+  residual_kernel<<<(unsigned)seg->count, kResThreads, 0, (cudaStream_t)stream>>>(*seg, x, y, beta, beta_stride,
+                                                                                  sse, ssy);
+  prof_end((cudaStream_t)stream);
+  count_launch();
+  return check_launch("art_segment_residuals");
+}
 
 extern "C" int art_partition_rows(const ArtSegments* seg, const double* x, const double* theta,
                                   int64_t theta_stride, const int8_t* split, int64_t* perm,

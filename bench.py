@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--no-legs", action="store_true", help="skip the split-search and hit-and-run legs")
     ap.add_argument("--split-nodes", type=int, default=4096)
     ap.add_argument("--har-chains", type=int, default=16384)
+    ap.add_argument("--tree-builds", type=int, default=3)
+    ap.add_argument("--serve-jobs", type=int, default=40)
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
 
@@ -400,6 +402,67 @@ def leg_har(args, stream):
             "by_dim": out}
 
 
+def leg_serving(args, stream):
+    """Surrogate-build service: a Poisson stream at 20 jobs/s, d uniform over
+    {2, 4, 8, 16, 32}, n0 log-uniform in [1e3, 1e6], depth <= 12, quadratic
+    leaves for d <= 8 else affine, 3 adaptive rounds of +10% samples; the
+    first ``--serve-jobs`` jobs of the stream, mixed and plain FP64 leaf fits."""
+
+    from art.serving import ServingEngine, poisson_jobs
+
+    out = {}
+    for precision in ("mixed", "fp64"):
+        jobs = poisson_jobs(args.serve_jobs, 20.0, seed=5)
+        eng = ServingEngine(precision=precision, stream=stream)
+        t0 = time.perf_counter()
+        res = eng.run(jobs)
+        wall = time.perf_counter() - t0
+        lat = np.array([r.latency for r in res])
+        out[precision] = {"jobs": len(res), "builds_per_s": len(res) / wall, "wall_s": wall,
+                          "p50_latency_s": float(np.percentile(lat, 50)),
+                          "p99_latency_s": float(np.percentile(lat, 99)),
+                          "ticks": eng.ticks, "peak_active": eng.peak_active,
+                          "rows_total": int(sum(r.n_rows for r in res))}
+    return {"metric": "surrogate builds/s and build latency", "stream": f"first {args.serve_jobs} jobs of "
+            "a 20 jobs/s Poisson stream (seed 5)", **out}
+
+
+def leg_tree(args, stream):
+    """Tree builds/s on the 2-d configuration: N = 4096 uniform points, depth
+    <= 6, min 32 points per side, soft oblique splits (T = 0.05, 100
+    iterations), affine leaves (lambda = 1e-6); level-batched BFS build
+    against the per-node DFS build, both through RegressionTreeBuilder."""
+
+    from art import (AffineRidgeModel, BoxDomain, HitAndRunSampler, RegressionTreeBuilder, SoftObliqueSplitter,
+                     TemperatureConfig)
+    from art.workloads import bumps_ridge_2d
+
+    f = bumps_ridge_2d(1)
+
+    def build(traversal, dispatch):
+        model = AffineRidgeModel(ridge=1e-6, solver="normal")
+        sp = SoftObliqueSplitter(model, 0.05, max_iters=100, min_side_points=32, min_side_fraction=0.0)
+        b = RegressionTreeBuilder(domain=BoxDomain.hypercube(2, -1.0, 1.0), oracle=f, model_template=model,
+                                  splitter=sp, error_threshold=0.01, max_depth=6, sample_count=4096,
+                                  temperature_config=TemperatureConfig(strategy="splitter"), random_state=1,
+                                  oracle_vectorized=True, traversal=traversal, level_dispatch=dispatch,
+                                  isotropic_sampling=False, sampler=HitAndRunSampler(burn_in=0, thinning=5))
+        return b.build()
+
+    out = {}
+    for name, trav, disp in (("bfs_level_batched", "bfs", True), ("dfs_per_node", "dfs", False)):
+        build(trav, disp)  # warm-up
+        t0 = time.perf_counter()
+        reps = args.tree_builds
+        for _ in range(reps):
+            res = build(trav, disp)
+        wall = time.perf_counter() - t0
+        out[name] = {"builds_per_s": reps / wall, "ms_per_build": 1000 * wall / reps,
+                     "nodes": len(list(res.tree.iter_nodes())), "oracle_queries": res.oracle_queries}
+    out["speedup"] = out["bfs_level_batched"]["builds_per_s"] / out["dfs_per_node"]["builds_per_s"]
+    return {"metric": "tree builds/s", **out}
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -543,7 +606,8 @@ def run_b200(args):
 
     legs = {}
     if rank == 0 and not args.no_legs:
-        for name, fn in (("split_level", leg_split), ("hit_and_run", leg_har)):
+        for name, fn in (("split_level", leg_split), ("hit_and_run", leg_har), ("tree_build", leg_tree),
+                         ("serving", leg_serving)):
             try:
                 legs[name] = fn(args, stream)
             except Exception as exc:  # a failing leg is reported, the headline stands

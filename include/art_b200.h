@@ -215,6 +215,10 @@ typedef struct ArtSplitProblem {
   int64_t theta_stride;       /* >= ART_MAX_DIM + 1 elements per (k, r)     */
   int32_t max_dim;            /* host-known max d over the batch            */
   int32_t max_features;       /* host-known max p                           */
+  const uint64_t* node_keys;  /* device [K] or NULL: device restart draws keyed
+                                 by (seed, node_keys[k], r) instead of
+                                 (seed, k, r), so a node's draws do not depend
+                                 on its position in the batch               */
 } ArtSplitProblem;
 
 /* stop reasons (splitters.py:424-488) */
@@ -320,6 +324,13 @@ ART_API int art_partition_rows(const ArtSegments* seg, const double* x, const do
  * flat array: child[node][0/1] (left/right, -1 for a leaf), theta[node] =
  * [w, z], leaf coefficients coef[node][coef_stride] with feature kind
  * features[node].  Writes leaf[n] (node index) and pred[n].                  */
+/* Per segment k: sse[k] = sum (y - phi(x) . beta_k)^2 and ssy[k] = sum y^2
+ * over its rows (FP64, fixed summation order) -- the leaf fit error of
+ * relative_l2_error (metrics.py) for every node of a level at once.       */
+ART_API int art_segment_residuals(const ArtSegments* seg, const double* x, const double* y,
+                                  const double* beta, int64_t beta_stride, double* sse,
+                                  double* ssy, art_stream_t stream);
+
 ART_API int art_tree_predict(int32_t dim, int64_t n_nodes, const int32_t* child,
                      const double* theta, int64_t theta_stride, const double* coef,
                      int64_t coef_stride, const int32_t* features, int64_t n_points,
