@@ -135,7 +135,7 @@ def peaks():
 
 
 def algorithmic(wl, idx=None):
-    """SURVEY 8(d) formulas: F = n p(p+1) + 2np + p^3/3 + 2p^2 ; B = n (d+2) 8 + 8p."""
+    """Algorithmic work per system: F = n p(p+1) + 2np + p^3/3 + 2p^2 flops; B = n (d+2) 8 + 8p bytes."""
 
     from art.models import kind_feature_count
 
