@@ -75,7 +75,7 @@ class ArtRidgeProblem(C.Structure):
         ("seg", ArtSegments), ("x", P), ("y", P), ("w", P), ("ridge", P),
         ("weight_floor", F64), ("solver", I32), ("precision", I32),
         ("auto_rcond_threshold", F64), ("max_features", I32), ("max_dim", I32),
-        ("options", C.c_uint32), ("reserved", I32),
+        ("options", C.c_uint32), ("tensor_min_features", I32),
     ]
 
 
@@ -94,7 +94,7 @@ class ArtSplitParams(C.Structure):
         ("alpha_min", F64), ("alpha_max", F64), ("alpha_grow", F64), ("alpha_recovery", F64),
         ("heavy_backtrack_threshold", I32), ("max_line_search_failures", I32),
         ("weight_floor", F64), ("hard_refit", I32), ("precision", I32),
-        ("anneal_ratio", F64), ("seed", U64),
+        ("anneal_ratio", F64), ("seed", U64), ("group_restarts", I32), ("trial_steps", I32),
     ]
 
 

@@ -216,6 +216,18 @@ class BatchedRidgeResult:
     info: object            # (K,) int32 (ART_INFO_* bits)
 
 
+def _tensor_threshold(requested, precision, dims_t, feats, ro, max_features) -> int:
+    """Explicit threshold, else the autotuner's cached choice, else 0 (library default)."""
+
+    if requested is not None:
+        return int(requested)
+    if precision != "mixed":
+        return 0
+    from . import autotune
+
+    return autotune.cached_ridge_threshold(dims_t, feats, ro, fp64_factor=False)
+
+
 def solve_weighted_ridge_batched(
     x,
     y,
@@ -234,6 +246,7 @@ def solve_weighted_ridge_batched(
     max_dim: int | None = None,
     condition: bool = False,
     fp64_factor: bool = False,
+    tensor_min_features: int | None = None,
     out: BatchedRidgeResult | None = None,
     stream=None,
 ) -> BatchedRidgeResult:
@@ -246,6 +259,10 @@ def solve_weighted_ridge_batched(
     torch; they are moved to the current CUDA device.  No host sync happens
     unless the caller reads the result.  ``fp64_factor`` makes the mixed form
     factor its tensor-core Gram in FP64 (``ART_RIDGE_OPT_FP64_FACTOR``).
+    ``tensor_min_features`` is the smallest feature count the mixed form
+    solves on the tensor cores (smaller systems take the FP64 kernels); None
+    takes the autotuned choice for this device and batch, else the library
+    default (33).
     """
 
     t = torch()
@@ -294,7 +311,8 @@ def solve_weighted_ridge_batched(
     prob = N.ArtRidgeProblem(
         seg, ptr(x), ptr(y), ptr(w), ptr(ridge_t), float(weight_floor), _SOLVER_CODES[solver],
         _PRECISION_CODES[precision], float(auto_rcond_threshold), int(max_features), int(max_dim),
-        N.RIDGE_OPT_FP64_FACTOR if fp64_factor else 0, 0,
+        N.RIDGE_OPT_FP64_FACTOR if fp64_factor else 0,
+        int(_tensor_threshold(tensor_min_features, precision, dims_t, feats, ro, max_features)),
     )
     res = N.ArtRidgeResult(
         ptr(out.beta), int(out.beta.shape[1]), ptr(out.ridge_effective), ptr(out.cond_estimate),

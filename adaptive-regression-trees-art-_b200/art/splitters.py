@@ -158,20 +158,22 @@ class LevelResult:
     trace_grad_norm: object | None = None
 
 
-def split_params(s: "SoftObliqueSplitter", hard_refit: bool, anneal_ratio: float = 1.0, seed: int = 0):
+def split_params(s: "SoftObliqueSplitter", hard_refit: bool, anneal_ratio: float = 1.0, seed: int = 0,
+                 group_restarts: int = 0, trial_steps: int = 0):
     return N.ArtSplitParams(
         int(s.max_iters), int(max(1, s.n_restarts)), float(s.grad_atol), float(s.grad_rtol),
         int(s.min_side_points), float(s.min_side_fraction), float(s.alpha0), float(s.rho),
         float(s.armijo_c), int(s.max_backtracks), int(bool(s.adaptive_alpha)), float(s.alpha_min),
         float(s.alpha_max), float(s.alpha_grow), float(s.alpha_recovery), int(s.heavy_backtrack_threshold),
         int(s.max_line_search_failures), float(s.weight_floor), int(bool(hard_refit)), N.PRECISION_FP64,
-        float(anneal_ratio), int(seed) & ((1 << 64) - 1))
+        float(anneal_ratio), int(seed) & ((1 << 64) - 1), int(group_restarts), int(trial_steps))
 
 
 def split_level(splitter: "SoftObliqueSplitter", x, y, row_offsets, dims, features, temperature, ridge,
                 *, x_offsets=None, parent_loss=None, min_side_fallback=None, theta0=None,
                 hard_refit: bool = True, anneal_ratio: float = 1.0, seed: int = 0, traces: bool = False,
                 max_dim: int | None = None, max_features: int | None = None, node_keys=None,
+                group_restarts: int | None = None, trial_steps: int | None = None,
                 stream=None) -> LevelResult:
     """Split K nodes in one launch sequence; arrays are numpy or torch (moved to the device).
 
@@ -179,6 +181,9 @@ def split_level(splitter: "SoftObliqueSplitter", x, y, row_offsets, dims, featur
     device draws keyed by ``seed`` and the node's position k (unit Gaussian w,
     z = median(X w)), or by ``node_keys[k]`` (uint64 per node) when given, so
     that a node's draws do not depend on the batch it is solved in.
+    ``group_restarts`` / ``trial_steps`` fix the kernel's launch shape
+    (restarts per CTA, Armijo steps per trial pass); None takes the
+    autotuned choice for (d, p, R) on this device, else the library's.
     """
 
     t = torch()
@@ -234,7 +239,13 @@ def split_level(splitter: "SoftObliqueSplitter", x, y, row_offsets, dims, featur
                        else node_keys, t.int64, dev)
     prob = N.ArtSplitProblem(seg, ptr(x), ptr(y), ptr(temp), ptr(rid), ptr(pl), ptr(fb), ptr(th0), stride,
                              int(max_dim), int(max_features), ptr(nk))
-    prm = split_params(splitter, hard_refit, anneal_ratio, seed)
+    if group_restarts is None or trial_steps is None:
+        from . import autotune
+
+        g_auto, h_auto = autotune.cached_split_shape(int(max_dim), int(max_features), R)
+        group_restarts = g_auto if group_restarts is None else group_restarts
+        trial_steps = h_auto if trial_steps is None else trial_steps
+    prm = split_params(splitter, hard_refit, anneal_ratio, seed, group_restarts, trial_steps)
     res = N.ArtSplitResult(ptr(out.theta), max_dim + 1, ptr(out.beta), max_features, ptr(out.loss),
                            ptr(out.child_loss), ptr(out.ridge_effective), ptr(out.n_right), ptr(out.n_iters),
                            ptr(out.stop_reason), ptr(out.failure), ptr(out.flags), ptr(out.fallback_iteration),

@@ -75,6 +75,41 @@ int check_launch(const char* what) {
   return ART_OK;
 }
 
+int resident_ctas(const void* kern, int threads, size_t dyn_smem) {
+  cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       (int)cudaSharedmemCarveoutMaxShared);
+  cudaGetLastError();
+  int api = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&api, kern, threads, dyn_smem) != cudaSuccess) {
+    cudaGetLastError();
+    api = 0;
+  }
+  int derived = 0;
+  cudaFuncAttributes fa;
+  int dev = 0;
+  if (cudaFuncGetAttributes(&fa, kern) == cudaSuccess && cudaGetDevice(&dev) == cudaSuccess) {
+    int regs_sm = 65536, smem_sm = 228 * 1024, reserved = 1024, threads_sm = 2048, blocks_sm = 32;
+    cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    cudaDeviceGetAttribute(&threads_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev);
+    cudaDeviceGetAttribute(&blocks_sm, cudaDevAttrMaxBlocksPerMultiprocessor, dev);
+    const int warps = (threads + 31) / 32;
+    const int regs_warp = ((fa.numRegs * 32 + 255) / 256) * 256;  // 256-register allocation unit
+    const int by_regs = regs_warp > 0 ? (regs_sm / regs_warp) / warps : blocks_sm;
+    const size_t per_block = fa.sharedSizeBytes + dyn_smem + (size_t)reserved;
+    const int by_smem = per_block > 0 ? (int)((size_t)smem_sm / per_block) : blocks_sm;
+    const int by_threads = threads_sm / (warps * 32);
+    derived = by_regs < by_smem ? by_regs : by_smem;
+    derived = derived < by_threads ? derived : by_threads;
+    derived = derived < blocks_sm ? derived : blocks_sm;
+  } else {
+    cudaGetLastError();
+  }
+  const int occ = api > derived ? api : derived;
+  return occ > 0 ? occ : 1;
+}
+
 }  // namespace art
 
 extern "C" const char* art_last_error(void) { return art::g_error; }

@@ -21,6 +21,12 @@ int check_launch(const char* what);
 void prof_begin(const char* name, cudaStream_t s);
 void prof_end(cudaStream_t s);
 int device_sm_count();
+// CTAs of `kern` (with `threads` threads and `dyn_smem` bytes of dynamic
+// shared memory) that one SM holds at once.  Prefers the full shared-memory
+// carveout for the kernel, then takes the larger of the runtime's occupancy
+// answer and the count implied by the kernel's registers, its shared memory
+// and the SM's thread and block limits.  At least 1.
+int resident_ctas(const void* kern, int threads, size_t dyn_smem);
 
 constexpr int kWarp = 32;
 

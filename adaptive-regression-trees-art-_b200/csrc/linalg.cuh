@@ -235,6 +235,97 @@ __device__ int chol_packed32(T* A, int p, int* s_fail) {
   return 0;
 }
 
+// In-place inverse of the packed lower-triangular factor L (p x p, positive
+// diagonal): on return A holds X = L^{-1}, also lower triangular.  All
+// threads of the block call it; `Y` is scratch for (p - 32) x 32 values.
+//  1. Every 32 x 32 diagonal block is inverted independently, one warp per
+//     block: lane c builds column c of X_jj by forward substitution in
+//     registers (row i of L_jj read by every lane: broadcast loads).
+//  2. Block columns right to left: with X[j1:, j1:] already inverted,
+//     X[j1:, j0:j1] = -(X[j1:, j1:] L[j1:, j0:j1]) X_jj, the panel product
+//     staged in Y.  Each step reads only finished blocks of X and the still
+//     original panel of L, so the update is in place.
+template <typename T>
+__device__ void tri_inv_packed32(T* A, int p, T* Y) {
+  constexpr int NB = 32;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nthreads = blockDim.x, nwarps = nthreads >> 5;
+  const int nb = (p + NB - 1) / NB;
+  for (int jb = warp; jb < nb; jb += nwarps) {
+    const int j0 = jb * NB, bs = min(NB, p - j0);
+    T x[NB];
+#pragma unroll
+    for (int i = 0; i < NB; ++i) {
+      T s = T(0);
+      if (i < bs) {
+        const T* row = A + pk(j0 + i, j0);
+#pragma unroll
+        for (int k = 0; k < NB; ++k)
+          if (k < i) s = fma(row[k], x[k], s);
+        const T inv_d = T(1) / row[i];
+        x[i] = (i == lane) ? inv_d : (i > lane ? -s * inv_d : T(0));
+      } else {
+        x[i] = T(0);
+      }
+    }
+    __syncwarp();
+    if (lane < bs) {
+#pragma unroll
+      for (int i = 0; i < NB; ++i)
+        if (i >= lane && i < bs) A[pk(j0 + i, j0 + lane)] = x[i];
+    }
+  }
+  __syncthreads();
+  for (int jb = nb - 2; jb >= 0; --jb) {
+    const int j0 = jb * NB, bs = NB, j1 = j0 + NB, m = p - j1;
+    // Y[i][c] = sum_{k <= i} X[j1+i][j1+k] L[j1+k][j0+c], 8-column strips
+    for (int t = tid; t < m * (NB / 8); t += nthreads) {
+      const int i = t >> 2, c0 = (t & 3) * 8;
+      const T* xr = A + pk(j1 + i, j1);
+      T acc[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) acc[u] = T(0);
+      for (int k = 0; k <= i; ++k) {
+        const T xv = xr[k];
+        const T* lr = A + pk(j1 + k, j0 + c0);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) acc[u] = fma(xv, lr[u], acc[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) Y[i * NB + c0 + u] = acc[u];
+    }
+    __syncthreads();
+    // X[j1+i][j0+c] = -sum_{c' >= c} Y[i][c'] X_jj[c'][c]
+    for (int t = tid; t < m * bs; t += nthreads) {
+      const int i = t / bs, c = t - i * bs;
+      T sacc = T(0);
+      for (int c2 = c; c2 < bs; ++c2) sacc = fma(Y[i * NB + c2], A[pk(j0 + c2, j0 + c)], sacc);
+      A[pk(j1 + i, j0 + c)] = -sacc;
+    }
+    __syncthreads();
+  }
+}
+
+// v_out = X^T (X v) for X = L^{-1} from tri_inv_packed32 (the preconditioner
+// M^{-1} = L^{-T} L^{-1}); block-wide, `t` is scratch of length p.
+template <typename T>
+__device__ void apply_inv_factor(const T* X, int p, const double* v, double* t, double* out) {
+  const int tid = threadIdx.x, nthreads = blockDim.x;
+  for (int i = tid; i < p; i += nthreads) {
+    const T* row = X + pk(i, 0);
+    double s = 0.0;
+    for (int k = 0; k <= i; ++k) s = fma((double)row[k], v[k], s);
+    t[i] = s;
+  }
+  __syncthreads();
+  for (int j = tid; j < p; j += nthreads) {
+    double s = 0.0;
+    for (int i = j; i < p; ++i) s = fma((double)X[pk(i, j)], t[i], s);
+    out[j] = s;
+  }
+  __syncthreads();
+}
+
 // Solve L z = b in place (z initially b), one warp, L packed lower.
 template <typename T, typename V>
 __device__ void warp_forward(const T* L, V* z, int p) {

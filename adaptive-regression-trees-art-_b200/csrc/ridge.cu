@@ -27,7 +27,7 @@ namespace art {
 
 // ====================================================================== plan
 __device__ __forceinline__ int plan_class(const RidgeArgs& a, int p) {
-  if (a.precision == ART_PRECISION_MIXED && p >= kTensorMinP) return CLS_TENSOR;
+  if (a.precision == ART_PRECISION_MIXED && p >= a.tensor_min_p) return CLS_TENSOR;
   if (a.gram_out) return -1;  // Gram-only calls cover tensor-class systems only
   if (p + 1 <= kWarpMaxAug) return CLS_WARP;
   return (p + 1 <= kSmallMaxAug) ? CLS_SMALL : CLS_LARGE;
@@ -491,12 +491,7 @@ static int launch_persistent(Kern kern, size_t smem, int64_t max_items, cudaStre
     set_error("%s: cannot reserve %zu bytes of shared memory", name, smem);
     return ART_E_UNSUPPORTED;
   }
-  int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kRidgeThreads, smem) != cudaSuccess) {
-    cudaGetLastError();
-    occ = 1;
-  }
-  if (occ < 1) occ = 1;
+  const int occ = resident_ctas((const void*)kern, kRidgeThreads, smem);
   int64_t grid = (int64_t)device_sm_count() * occ;
   if (grid > max_items) grid = max_items;
   if (grid < 1) grid = 1;
@@ -584,6 +579,8 @@ static int ridge_entry(const ArtRidgeProblem* pr, const ArtRidgeResult* res, flo
   a.ridge_eff = res->ridge_effective; a.cond = res->cond_estimate;
   a.status = res->status; a.info = res->info;
   a.options = pr->options;
+  a.tensor_min_p = pr->tensor_min_features > 0 ? std::max(pr->tensor_min_features, kTensorMinP) : kTensorMinP;
+  if (gram_out) a.tensor_min_p = kTensorMinP;
   a.gram_out = gram_out;
   a.gram_stride = gram_stride;
   if (gram_out) a.precision = ART_PRECISION_MIXED;

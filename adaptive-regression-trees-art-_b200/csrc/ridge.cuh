@@ -48,6 +48,7 @@ struct RidgeArgs {
   int32_t* status;
   uint32_t* info;
   uint32_t options;
+  int tensor_min_p;       // mixed form: smallest p on the tensor-core kernel
   float* gram_out;        // art_ridge_gram: packed tensor-core Grams
   int64_t gram_stride;
 };

@@ -46,6 +46,7 @@ constexpr int kLBO = 128;                  // bytes between K-adjacent core matr
 constexpr int kSBO = (kKC / kKE) * 128;    // bytes between 8-feature groups
 constexpr int kOpBytes = kGroups * kSBO;   // one operand array (hi or lo)
 constexpr int kMaxRefine = 14;
+constexpr int kRefRows = 4;                // rows per warp step in refinement passes
 // TMEM accumulation chains are restarted every kDrainChunks stages: the
 // FP32 accumulator of the tensor core loses low bits on every step, so the
 // chain length bounds the Gram error (~steps * 2^-24 relative); drained
@@ -203,17 +204,6 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
     const int N1 = P16, N2 = two ? P16 - 128 : 0;
     const int g0 = two ? (P16 - 128) / 8 : 0;
     const int64_t nchunks = (it.n + kKC - 1) / kKC;
-    // bulk copies of rows [c*kKC, c*kKC + rows) of x and w into row stage st
-    // (the refinement passes need no y)
-    auto issue_rows = [&](int64_t c, int st) {
-      const int64_t rr = c * kKC;
-      const int rows = (int)min((int64_t)kKC, it.n - rr);
-      Granules gx = granules(a.x + it.xoff + rr * it.d, (uint64_t)rows * it.d * 8);
-      Granules gw = a.w ? granules(a.w + it.r0 + rr, (uint64_t)rows * 8) : Granules{nullptr, 0, 0};
-      mbar_arrive_expect_tx(&load_bar[st], gx.bytes + gw.bytes);
-      bulk_g2s(smem + lay.x[st], gx.base, gx.bytes, &load_bar[st]);
-      if (a.w) bulk_g2s(smem + lay.w[st], gw.base, gw.bytes, &load_bar[st]);
-    };
     if (nchunks == 0) {  // nothing to accumulate: the FP64 form reports the status
       if (tid == 0) push_list(L, a.K, CLS_RESOLVE, k);
       continue;
@@ -482,51 +472,27 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
       }
       cond = rcond > 0.0 ? sqrt(1.0 / fmin(rcond, 1.0)) : __longlong_as_double(0x7ff0000000000000ll);
     }
-    // ---- M^{-1} v = L^{-T} L^{-1} v by blocked triangular solves: each
-    // 32-row diagonal block is solved by warp 0 in registers, then every
-    // thread updates the rows beyond the block (one row per thread).
-    double* part = (double*)op;  // [8 row slots][kPmax]
-    auto apply_minv = [&](const double* v, double* out) {
-      for (int i = tid; i < p; i += kTcThreads) out[i] = v[i];
-      __syncthreads();
-      for (int j0 = 0; j0 < p; j0 += 32) {           // L y = v
-        const int bs = min(32, p - j0);
-        if (warp == 0) {
-          double zl = lane < bs ? out[j0 + lane] : 0.0;
-          for (int t2 = 0; t2 < bs; ++t2) {
-            if (lane == t2) zl = zl / (double)Gf[pk(j0 + t2, j0 + t2)];
-            const double yt = __shfl_sync(0xffffffffu, zl, t2);
-            if (lane > t2 && lane < bs) zl -= (double)Gf[pk(j0 + lane, j0 + t2)] * yt;
-          }
-          if (lane < bs) out[j0 + lane] = zl;
-        }
-        __syncthreads();
-        for (int i = j0 + bs + tid; i < p; i += kTcThreads) {
-          double sacc = 0.0;
-          for (int t2 = 0; t2 < bs; ++t2) sacc = fma((double)Gf[pk(i, j0 + t2)], out[j0 + t2], sacc);
-          out[i] -= sacc;
-        }
-        __syncthreads();
-      }
-      for (int j0 = ((p - 1) / 32) * 32; j0 >= 0; j0 -= 32) {   // L^T x = y
-        const int bs = min(32, p - j0);
-        if (warp == 0) {
-          double zl = lane < bs ? out[j0 + lane] : 0.0;
-          for (int t2 = bs - 1; t2 >= 0; --t2) {
-            if (lane == t2) zl = zl / (double)Gf[pk(j0 + t2, j0 + t2)];
-            const double xt = __shfl_sync(0xffffffffu, zl, t2);
-            if (lane < t2) zl -= (double)Gf[pk(j0 + t2, j0 + lane)] * xt;
-          }
-          if (lane < bs) out[j0 + lane] = zl;
-        }
-        __syncthreads();
-        for (int i = tid; i < j0; i += kTcThreads) {
-          double sacc = 0.0;
-          for (int t2 = 0; t2 < bs; ++t2) sacc = fma((double)Gf[pk(j0 + t2, i)], out[j0 + t2], sacc);
-          out[i] -= sacc;
-        }
-        __syncthreads();
-      }
+    // ---- M^{-1} = L^{-T} L^{-1}: invert the factor in place (the operand
+    // buffers are idle and hold the panel scratch), then every application
+    // is two block-wide triangular matrix-vector products.
+    tri_inv_packed32<TF>(Gf, p, (TF*)op);
+    double* tvec = vec + 6 * vs;
+    auto apply_minv = [&](const double* v, double* out) { apply_inv_factor<TF>(Gf, p, v, tvec, out); };
+    double* part = (double*)op;  // [8 row slots][kPmax], after the row passes
+    // refinement row stages also live in the operand buffers: two stages of
+    // RC rows of x (and w), RC a multiple of 8 (one row per warp per step)
+    int RC = (int)(((size_t)kOpBytes - 128) / ((size_t)a.dmax * 8 + 8)) & ~7;
+    RC = RC > 256 ? 256 : RC;
+    const size_t rx_bytes = a16((size_t)RC * a.dmax * 8 + 32);
+    const size_t rstage = rx_bytes + a16((size_t)RC * 8 + 32);
+    auto issue_rows = [&](int64_t c, int st) {
+      const int64_t rr = c * RC;
+      const int rows = (int)min((int64_t)RC, it.n - rr);
+      Granules gx = granules(a.x + it.xoff + rr * it.d, (uint64_t)rows * it.d * 8);
+      Granules gw = a.w ? granules(a.w + it.r0 + rr, (uint64_t)rows * 8) : Granules{nullptr, 0, 0};
+      mbar_arrive_expect_tx(&load_bar[st], gx.bytes + gw.bytes);
+      bulk_g2s(op + st * rstage, gx.base, gx.bytes, &load_bar[st]);
+      if (a.w) bulk_g2s(op + st * rstage + rx_bytes, gw.base, gw.bytes, &load_bar[st]);
     };
     // ---- FP64 iterative refinement.  Residual passes: one warp per row (8
     // rows per step), lane l owns features l + 32 m (m < 5) with their beta
@@ -534,6 +500,7 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
     // e_k = q_k phi_k . beta (warp shuffle sum) and the accumulation of
     // e_k phi_k; the 8 row slots are summed in a fixed order at the end.
     const int slot = warp, fl = lane;
+    const int mslots = (p + 31) >> 5;  // feature slots in use (<= 5)
     int rfa[5], rfb[5];
 #pragma unroll
     for (int m = 0; m < 5; ++m) {
@@ -568,7 +535,7 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
       // rows stream through the two row stages again (bulk copies of x and
       // w, prefetched two chunks ahead); warp `slot` takes rows slot, slot+8,
       // ... of each chunk, so every warp stays converged
-      const int64_t nch = (it.n + kKC - 1) / kKC;
+      const int64_t nch = (it.n + RC - 1) / RC;
       if (tid == 0)
         for (int64_t c = 0; c < min((int64_t)2, nch); ++c) issue_rows(c, (int)c);
       for (int64_t c = 0; c < min((int64_t)2, nch); ++c) S.load_issued[c]++;
@@ -577,29 +544,48 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
         const bool okl = mbar_wait(&load_bar[st], S.load_uses[st] & 1);
         if (!__syncthreads_and(okl)) { abort = true; break; }
         S.load_uses[st]++;
-        const int rows = (int)min((int64_t)kKC, it.n - c * kKC);
-        const double* xs = (const double*)(smem + lay.x[st] +
-                                           (((uintptr_t)(a.x + it.xoff + c * kKC * d)) & 15));
-        const double* ws = a.w ? (const double*)(smem + lay.w[st] +
-                                                 (((uintptr_t)(a.w + it.r0 + c * kKC)) & 15))
+        const int rows = (int)min((int64_t)RC, it.n - c * RC);
+        const double* xs = (const double*)(op + st * rstage +
+                                           (((uintptr_t)(a.x + it.xoff + c * RC * d)) & 15));
+        const double* ws = a.w ? (const double*)(op + st * rstage + rx_bytes +
+                                                 (((uintptr_t)(a.w + it.r0 + c * RC)) & 15))
                                : nullptr;
-        for (int j = slot; j < rows; j += kTcThreads / 32) {
-          const double* xk = xs + j * d;
-          double ph[5];
-          double dot = 0.0;
+        // four rows per warp step (slot, slot+8, slot+16, slot+24 of a group)
+        // so their shuffle reductions overlap; rows are still accumulated in
+        // the order slot, slot+8, ... of the single-row loop
+        for (int j0 = slot; j0 < rows; j0 += kRefRows * (kTcThreads / 32)) {
+          double dot[kRefRows], ph[kRefRows][5];
 #pragma unroll
-          for (int m = 0; m < 5; ++m) {
-            const int ua = rfa[m], ub = rfb[m];
-            const double va = ua >= 0 ? xk[ua] : (ua == -1 ? 1.0 : 0.0);
-            const double vb = ub >= 0 ? xk[ub] : 1.0;
-            ph[m] = va * vb;
-            dot = fma(ph[m], bt[m], dot);
+          for (int u = 0; u < kRefRows; ++u) {
+            const int j = j0 + (kTcThreads / 32) * u;
+            const double* xk = xs + (j < rows ? j : j0) * d;
+            dot[u] = 0.0;
+#pragma unroll
+            for (int m = 0; m < 5; ++m) {
+              ph[u][m] = 0.0;
+              if (m < mslots) {
+                const int ua = rfa[m], ub = rfb[m];
+                const double va = ua >= 0 ? xk[ua] : (ua == -1 ? 1.0 : 0.0);
+                const double vb = ub >= 0 ? xk[ub] : 1.0;
+                ph[u][m] = va * vb;
+                dot[u] = fma(ph[u][m], bt[m], dot[u]);
+              }
+            }
           }
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
-          const double e = fmax(ws ? ws[j] : 1.0, a.weight_floor) * dot;
+          for (int o = 16; o > 0; o >>= 1)
 #pragma unroll
-          for (int m = 0; m < 5; ++m) accb[m] = fma(e, ph[m], accb[m]);
+            for (int u = 0; u < kRefRows; ++u) dot[u] += __shfl_xor_sync(0xffffffffu, dot[u], o);
+#pragma unroll
+          for (int u = 0; u < kRefRows; ++u) {
+            const int j = j0 + (kTcThreads / 32) * u;
+            if (j < rows) {
+              const double e = fmax(ws ? ws[j] : 1.0, a.weight_floor) * dot[u];
+#pragma unroll
+              for (int m = 0; m < 5; ++m)
+                if (m < mslots) accb[m] = fma(e, ph[u][m], accb[m]);
+            }
+          }
         }
         __syncthreads();  // every warp is done with this stage
         if (c + 2 < nch) {
@@ -705,14 +691,11 @@ int launch_tc(const RidgeArgs& a, const RidgeLists& L, cudaStream_t s, const cha
       set_error("%s: cannot reserve %zu bytes of shared memory", name, smem);
       return ART_E_UNSUPPORTED;
     }
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kTcThreads, smem) != cudaSuccess) {
-      cudaGetLastError();
-      occ = 0;
-    }
+    occ = resident_ctas((const void*)kern, kTcThreads, smem);
     if (occ <= max_ctas || smem + 8 * 1024 > 200 * 1024) break;
     smem += 8 * 1024;
   }
-  if (occ > max_ctas || occ < 1) {
+  if (occ > max_ctas) {
     set_error("%s: cannot place CTAs within TMEM capacity (occ %d, cols %u)", name, occ, cols);
     return ART_E_UNSUPPORTED;
   }

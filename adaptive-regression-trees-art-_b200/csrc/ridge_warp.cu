@@ -361,13 +361,7 @@ int launch_ridge_warp(const RidgeArgs& a, const RidgeLists& L, cudaStream_t s) {
     set_error("ridge_warp: cannot reserve %zu bytes of shared memory", smem);
     return ART_E_UNSUPPORTED;
   }
-  int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ridge_warp_kernel, kWarpThreads, smem) !=
-      cudaSuccess) {
-    cudaGetLastError();
-    occ = 1;
-  }
-  if (occ < 1) occ = 1;
+  const int occ = resident_ctas((const void*)ridge_warp_kernel, kWarpThreads, smem);
   int64_t grid = (int64_t)device_sm_count() * occ;
   const int64_t need = (a.K + kWarpsPerCta - 1) / kWarpsPerCta;
   if (grid > need) grid = need;

@@ -25,6 +25,7 @@
 // A select kernel then keeps, per node, the best restart as split() does.
 #include <algorithm>
 
+#include "bulk.cuh"
 #include "common.cuh"
 #include "linalg.cuh"
 
@@ -38,6 +39,8 @@ constexpr int kMaxP = 64;        // child model features
 constexpr int kMaxRg = 16;       // restarts per work item
 constexpr int kRedSlots = 5;     // (restart, component) accumulators per thread
 constexpr int kBuckets = 64;
+constexpr int kMaxStages = 8;    // row-stage ring depth (chunks in flight)
+constexpr int kErrSlot = 2 + 2 * kBuckets;  // counts[kErrSlot]: a bounded wait gave up
 
 struct SplitArgs {
   int64_t K;
@@ -55,7 +58,7 @@ struct SplitArgs {
   int64_t theta0_stride;
   const uint64_t* node_keys;
   ArtSplitParams prm;
-  int R, Rg, groups, dmax, pmax, H, TC;
+  int R, Rg, groups, dmax, pmax, H, TC, S;
   // per (node, restart) results, index k * R + r
   double* r_theta;   // [.. ][dmax + 1]
   double* r_loss;
@@ -78,18 +81,22 @@ struct SplitArgs {
   int32_t* items;    // [K * groups]
 };
 
-// Shared-memory layout for a given (dmax, pmax, Rg, H).
+// Shared-memory layout for a given (dmax, pmax, Rg, H, S): `ring` holds S
+// stages of kCH rows of x and y (bulk copies in flight), `bars` their
+// mbarriers.
 struct SLayout {
-  size_t x, y, phi, q, G, cache, theta, dirn, grad, lastf, bl, br, trial, red, chol, eidx, rs,
+  size_t ring, rx, rstage, bars, phi, q, G, cache, theta, dirn, grad, lastf, bl, br, trial, red, chol, eidx, rs,
       total;
 };
 __host__ __device__ inline size_t al(size_t v) { return (v + 15) & ~(size_t)15; }
-__host__ __device__ inline SLayout split_layout(int dmax, int pmax, int Rg, int H) {
+__host__ __device__ inline SLayout split_layout(int dmax, int pmax, int Rg, int H, int S) {
   SLayout L;
   const int pa = pmax + 1, E = pa * (pa + 1) / 2, dt = dmax + 1;
   size_t o = 0;
-  L.x = o; o = al(o + (size_t)kCH * dmax * 8);
-  L.y = o; o = al(o + (size_t)kCH * 8);
+  L.rx = al((size_t)kCH * dmax * 8 + 32);
+  L.rstage = L.rx + al((size_t)kCH * 8 + 32);
+  L.ring = o; o = al(o + (size_t)S * L.rstage);
+  L.bars = o; o = al(o + (size_t)kMaxStages * 8);
   L.phi = o; o = al(o + (size_t)kCH * pa * 8);
   L.q = o; o = al(o + (size_t)kCH * 2 * Rg * 8);
   L.G = o; o = al(o + (size_t)E * 2 * Rg * 8);
@@ -174,13 +181,18 @@ struct SplitCta {
   unsigned char* sm;
   SLayout L;
   Item it;
-  double *xs, *ys, *phi, *Q, *G, *cache, *th, *dn, *gr, *lf, *bl, *br, *trial, *red, *chol, *rs;
+  uint64_t* rbar;
+  uint32_t rpar = 0, rbusy = 0;  // per-stage wait parity / copy in flight (uniform)
+  bool rabort = false;
+  const double *xs, *ys;
+  double *phi, *Q, *G, *cache, *th, *dn, *gr, *lf, *bl, *br, *trial, *red, *chol, *rs;
   int16_t* eidx;
   int tid, lane, warp;
 
   __device__ SplitCta(const SplitArgs& a_, unsigned char* sm_) : a(a_), sm(sm_) {
-    L = split_layout(a.dmax, a.pmax, a.Rg, a.H);
-    xs = (double*)(sm + L.x); ys = (double*)(sm + L.y); phi = (double*)(sm + L.phi);
+    L = split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S);
+    rbar = (uint64_t*)(sm + L.bars);
+    xs = (const double*)(sm + L.ring); ys = xs; phi = (double*)(sm + L.phi);
     Q = (double*)(sm + L.q); G = (double*)(sm + L.G); cache = (double*)(sm + L.cache);
     th = (double*)(sm + L.theta); dn = (double*)(sm + L.dirn); gr = (double*)(sm + L.grad);
     lf = (double*)(sm + L.lastf); bl = (double*)(sm + L.bl); br = (double*)(sm + L.br);
@@ -191,13 +203,61 @@ struct SplitCta {
   __device__ double& S(int r, int slot) { return rs[r * 32 + slot]; }
   __device__ int dt() const { return it.d + 1; }
 
-  // Stage rows [c0, c0 + rows) of x and y, then the augmented features.
+  // Row-stage ring: chunk ci of the current node goes to stage ci % S by
+  // 1-D bulk copies of its x and y rows; every pass over the rows primes S
+  // chunks and refills a stage as soon as the pass is done with it, so
+  // copies run S chunks ahead of the arithmetic.  Control flow is uniform:
+  // every thread tracks the same parity/in-flight bits; thread 0 issues.
+  __device__ void ring_issue(int64_t ci) {
+    const int st = (int)(ci % a.S);
+    if (tid == 0) {
+      const int64_t c0 = ci * kCH;
+      const int rows = (int)min((int64_t)kCH, it.n - c0);
+      Granules gx = granules(a.x + it.xoff + c0 * it.d, (uint64_t)rows * it.d * 8);
+      Granules gy = granules(a.y + it.r0 + c0, (uint64_t)rows * 8);
+      unsigned char* base = sm + L.ring + (size_t)st * L.rstage;
+      mbar_arrive_expect_tx(&rbar[st], gx.bytes + gy.bytes);
+      bulk_g2s(base, gx.base, gx.bytes, &rbar[st]);
+      bulk_g2s(base + L.rx, gy.base, gy.bytes, &rbar[st]);
+    }
+    rbusy |= 1u << st;
+  }
+  __device__ void begin_pass() {
+    if (rabort) return;
+    for (int st = 0; st < a.S && (int64_t)st * kCH < it.n; ++st) ring_issue(st);
+  }
+  // bounded waits for copies still in flight (only after a wait gave up)
+  __device__ void ring_drain() {
+    for (int st = 0; st < a.S; ++st)
+      if (rbusy & (1u << st)) {
+        mbar_wait(&rbar[st], (rpar >> st) & 1u);
+        rpar ^= 1u << st;
+        rbusy &= ~(1u << st);
+      }
+  }
+
+  // Rows [c0, c0 + rows) of x and y from the ring, then the augmented
+  // features.  The caller's loop ends every chunk with __syncthreads().
   __device__ int load_chunk(int64_t c0) {
     const int rows = (int)min((int64_t)kCH, it.n - c0);
     const int d = it.d;
-    for (int e = tid; e < rows * d; e += kSplitThreads) xs[e] = a.x[it.xoff + c0 * d + e];
-    for (int r = tid; r < rows; r += kSplitThreads) ys[r] = a.y[it.r0 + c0 + r];
-    __syncthreads();
+    const int64_t ci = c0 / kCH;
+    const int st = (int)(ci % a.S);
+    if (!rabort) {
+      if (ci >= 1 && (ci - 1 + a.S) * kCH < it.n) ring_issue(ci - 1 + a.S);
+      const bool ok = mbar_wait(&rbar[st], (rpar >> st) & 1u);
+      if (ok) {
+        rpar ^= 1u << st;
+        rbusy &= ~(1u << st);
+      }
+      if (!__syncthreads_and(ok)) {
+        rabort = true;
+        if (tid == 0) atomicExch(&a.counts[kErrSlot], 1);
+      }
+    }
+    const unsigned char* base = sm + L.ring + (size_t)st * L.rstage;
+    xs = (const double*)(base + (((uintptr_t)(a.x + it.xoff + c0 * d)) & 15));
+    ys = (const double*)(base + L.rx + (((uintptr_t)(a.y + it.r0 + c0)) & 15));
     const int pa = it.pa;
     for (int e = tid; e < rows * pa; e += kSplitThreads) {
       const int r = e / pa, f = e - r * pa;
@@ -248,6 +308,7 @@ struct SplitCta {
     for (int u = 0; u < TE; ++u)
 #pragma unroll
       for (int v = 0; v < TC; ++v) acc[u][v] = 0.0;
+    begin_pass();
     for (int64_t c0 = 0; c0 < it.n; c0 += kCH) {
       const int rows = load_chunk(c0);
       for (int pr = tid; pr < rows * a.Rg; pr += kSplitThreads) {
@@ -363,6 +424,7 @@ struct SplitCta {
     double* coef = cache;                      // [row][r]: a_k
     double* wl = cache + kCH * a.Rg;           // [row][r]: weighted loss term
     double* nr = cache + 2 * kCH * a.Rg;       // [row][r]: pi >= 0.5
+    begin_pass();
     for (int64_t c0 = 0; c0 < it.n; c0 += kCH) {
       const int rows = load_chunk(c0);
       for (int pr = tid; pr < rows * a.Rg; pr += kSplitThreads) {
@@ -456,6 +518,7 @@ struct SplitCta {
       pz = dn[r * dt() + d];
       T = S(r, RS_T);
     }
+    begin_pass();
     for (int64_t c0 = 0; c0 < it.n; c0 += kCH) {
       const int rows = load_chunk(c0);
       for (int pr = tid; pr < rows * a.Rg; pr += kSplitThreads) {
@@ -783,6 +846,7 @@ __device__ void SplitCta<TC>::run(int item_id) {
     // hard losses: mean squared residual on each side, reduced per (restart,
     // side) in row order
     double sl = 0.0;
+    begin_pass();
     for (int64_t c0 = 0; c0 < it.n; c0 += kCH) {
       const int rows = load_chunk(c0);
       for (int pr = tid; pr < rows * a.Rg; pr += kSplitThreads) {
@@ -849,6 +913,11 @@ __global__ void __launch_bounds__(kSplitThreads, 1) split_kernel(SplitArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_item;
   SplitCta<TC> cta(a, smem);
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < a.S; ++i) mbar_init(&cta.rbar[i], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
   const int count = a.counts[0];
   for (;;) {
     if (threadIdx.x == 0) s_item = atomicAdd(&a.counts[1], 1);
@@ -858,6 +927,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) split_kernel(SplitArgs a) {
     if (q >= count) break;
     cta.run(a.items[q]);
   }
+  cta.ring_drain();
 }
 
 // Per node: best non-fallback restart by hard loss, else best fallback,
@@ -892,7 +962,9 @@ __global__ void split_select(SplitArgs a, ArtSplitResult out) {
   if (out.n_right) out.n_right[k] = a.r_nright[kr];
   if (out.n_iters) out.n_iters[k] = a.r_iters[kr];
   if (out.stop_reason) out.stop_reason[k] = a.r_stop[kr];
-  if (out.failure) out.failure[k] = (best >= 0 || best_fb >= 0) ? 0 : a.r_fail[kr];
+  // a bounded row-copy wait gave up somewhere in the level: no result is trusted
+  const bool lost = a.counts[kErrSlot] != 0;
+  if (out.failure) out.failure[k] = lost ? ART_SPLIT_INVALID : ((best >= 0 || best_fb >= 0) ? 0 : a.r_fail[kr]);
   if (out.flags) out.flags[k] = a.r_flags[kr] | (pick << 8);
   if (out.fallback_iteration) out.fallback_iteration[k] = a.r_fbiter[kr];
   if (out.final_alpha) out.final_alpha[k] = a.r_alpha[kr];
@@ -981,7 +1053,7 @@ SplitWs split_ws(int64_t K, int R, int dmax, int pmax) {
   SplitWs w;
   size_t o = 0;
   auto take = [&](size_t bytes) { size_t at = o; o = (o + bytes + 255) & ~(size_t)255; return at; };
-  w.counts = take(4 * (2 + 2 * kBuckets));
+  w.counts = take(4 * (kErrSlot + 1));
   w.items = take(4 * (size_t)K * R);
   w.theta0 = take(8 * (size_t)K * R * (ART_MAX_DIM + 1));
   w.r_theta = take(8 * (size_t)K * R * (dmax + 1));
@@ -995,11 +1067,12 @@ SplitWs split_ws(int64_t K, int R, int dmax, int pmax) {
   return w;
 }
 
-int choose_rg(int R, int pa, int& TC) {
-  // largest group (<= 16 restarts) whose Gram tiles fit 256 threads and the
-  // accumulators a modest shared-memory budget
+int choose_rg(int R, int pa, int cap, int& TC) {
+  // largest group (<= 16 restarts, <= cap when cap > 0) whose Gram tiles fit
+  // 256 threads and the accumulators a modest shared-memory budget
   const int E = pa * (pa + 1) / 2;
-  for (int rg = std::min(R, kMaxRg); rg >= 1; --rg) {
+  const int top = std::min(std::min(R, kMaxRg), cap > 0 ? cap : kMaxRg);
+  for (int rg = top; rg >= 1; --rg) {
     const int c2 = 2 * rg;
     const int tc = c2 >= 8 ? 8 : (c2 >= 4 ? 4 : 2);
     const int te = 32 / tc;
@@ -1042,7 +1115,8 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
       prm->max_line_search_failures < 1 || !(prm->rho > 0.0 && prm->rho < 1.0) ||
       !(prm->armijo_c > 0.0 && prm->armijo_c < 1.0) || !(prm->alpha0 > 0.0) ||
       !(prm->alpha_min > 0.0) || prm->alpha_max < prm->alpha_min || prm->min_side_points < 1 ||
-      !(prm->min_side_fraction >= 0.0 && prm->min_side_fraction < 0.5) || !(prm->anneal_ratio > 0.0)) {
+      !(prm->min_side_fraction >= 0.0 && prm->min_side_fraction < 0.5) || !(prm->anneal_ratio > 0.0) ||
+      prm->group_restarts < 0 || prm->trial_steps < 0) {
     set_error("art_split_level: invalid splitter parameters");
     return ART_E_INVALID;
   }
@@ -1056,7 +1130,7 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
   }
   const int R = prm->n_restarts;
   int TC = 2;
-  const int Rg = choose_rg(R, pr->max_features + 1, TC);
+  const int Rg = choose_rg(R, pr->max_features + 1, prm->group_restarts, TC);
   if (Rg < 1) { set_error("art_split_level: model too large for the split kernel"); return ART_E_UNSUPPORTED; }
   const SplitWs wl = split_ws(K, R, pr->max_dim, pr->max_features);
   if (!workspace || ws_bytes < wl.total) {
@@ -1076,6 +1150,7 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
   a.R = R; a.Rg = Rg; a.groups = (R + Rg - 1) / Rg;
   a.dmax = pr->max_dim; a.pmax = pr->max_features; a.TC = TC;
   a.H = std::min(32, std::max(1, kSplitThreads / Rg));
+  if (prm->trial_steps > 0) a.H = std::min(prm->trial_steps, std::max(1, kSplitThreads / Rg));
   a.H = std::min(a.H, prm->max_backtracks + 1);
   a.r_theta = (double*)(ws + wl.r_theta); a.r_loss = (double*)(ws + wl.r_loss);
   a.r_beta = (double*)(ws + wl.r_beta); a.r_child = (double*)(ws + wl.r_child);
@@ -1098,7 +1173,7 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
     prof_end(s);
     count_launch();
   }
-  if (cudaMemsetAsync(a.counts, 0, 4 * (2 + 2 * kBuckets), s) != cudaSuccess) return check_launch("memset");
+  if (cudaMemsetAsync(a.counts, 0, 4 * (kErrSlot + 1), s) != cudaSuccess) return check_launch("memset");
   const unsigned pg = (unsigned)((K * a.groups + 255) / 256);
   prof_begin("split_plan", s);
   split_plan_hist<<<pg, 256, 0, s>>>(a);
@@ -1106,7 +1181,10 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
   split_plan_scatter<<<pg, 256, 0, s>>>(a);
   prof_end(s);
   count_launch(); count_launch(); count_launch();
-  const size_t smem = split_layout(a.dmax, a.pmax, a.Rg, a.H).total;
+  // deepest row ring (2..kMaxStages chunks in flight) that fits shared memory
+  a.S = kMaxStages;
+  while (a.S > 2 && split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S).total > 227 * 1024) --a.S;
+  const size_t smem = split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S).total;
   if (smem > 227 * 1024) { set_error("art_split_level: shared memory %zu too large", smem); return ART_E_UNSUPPORTED; }
   auto launch = [&](auto kern) -> int {
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
@@ -1114,11 +1192,7 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
       set_error("art_split_level: cannot reserve %zu bytes of shared memory", smem);
       return ART_E_UNSUPPORTED;
     }
-    int occ = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kSplitThreads, smem) != cudaSuccess) {
-      cudaGetLastError();
-      occ = 1;
-    }
+    const int occ = resident_ctas((const void*)kern, kSplitThreads, smem);
     const int64_t grid = std::min<int64_t>((int64_t)device_sm_count() * std::max(occ, 1), K * a.groups);
     prof_begin("split_level", s);
     kern<<<(unsigned)std::max<int64_t>(grid, 1), kSplitThreads, smem, s>>>(a);

@@ -430,14 +430,18 @@ def leg_serving(args, stream):
 def leg_tree(args, stream):
     """Tree builds/s on the 2-d configuration: N = 4096 uniform points, depth
     <= 6, min 32 points per side, soft oblique splits (T = 0.05, 100
-    iterations), affine leaves (lambda = 1e-6); level-batched BFS build
-    against the per-node DFS build, both through RegressionTreeBuilder."""
+    iterations), affine leaves (lambda = 1e-6), children topped up by
+    hit-and-run with device Philox draws; the level-batched BFS build
+    against the per-node DFS build, both through RegressionTreeBuilder, with
+    the held-out RMSE of each tree on 20,000 uniform points."""
 
     from art import (AffineRidgeModel, BoxDomain, HitAndRunSampler, RegressionTreeBuilder, SoftObliqueSplitter,
                      TemperatureConfig)
     from art.workloads import bumps_ridge_2d
 
     f = bumps_ridge_2d(1)
+    X_test = np.random.default_rng(99).uniform(-1.0, 1.0, (20000, 2))
+    y_test = f(X_test)
 
     def build(traversal, dispatch):
         model = AffineRidgeModel(ridge=1e-6, solver="normal")
@@ -446,7 +450,8 @@ def leg_tree(args, stream):
                                   splitter=sp, error_threshold=0.01, max_depth=6, sample_count=4096,
                                   temperature_config=TemperatureConfig(strategy="splitter"), random_state=1,
                                   oracle_vectorized=True, traversal=traversal, level_dispatch=dispatch,
-                                  isotropic_sampling=False, sampler=HitAndRunSampler(burn_in=0, thinning=5))
+                                  isotropic_sampling=False,
+                                  sampler=HitAndRunSampler(burn_in=0, thinning=5, rng_mode="device"))
         return b.build()
 
     out = {}
@@ -457,10 +462,14 @@ def leg_tree(args, stream):
         for _ in range(reps):
             res = build(trav, disp)
         wall = time.perf_counter() - t0
+        rmse = float(np.sqrt(np.mean((res.tree.predict(X_test) - y_test) ** 2)))
         out[name] = {"builds_per_s": reps / wall, "ms_per_build": 1000 * wall / reps,
-                     "nodes": len(list(res.tree.iter_nodes())), "oracle_queries": res.oracle_queries}
+                     "nodes": len(list(res.tree.iter_nodes())), "oracle_queries": res.oracle_queries,
+                     "heldout_rmse": rmse}
     out["speedup"] = out["bfs_level_batched"]["builds_per_s"] / out["dfs_per_node"]["builds_per_s"]
-    return {"metric": "tree builds/s", **out}
+    a, b = out["bfs_level_batched"]["heldout_rmse"], out["dfs_per_node"]["heldout_rmse"]
+    out["heldout_rmse_rel_diff"] = abs(a - b) / max(abs(b), 1e-300)
+    return {"metric": "tree builds/s", "sampler": "hit-and-run, device Philox draws", **out}
 
 
 def run_b200(args):
@@ -471,15 +480,16 @@ def run_b200(args):
     from art import workloads
     from art.models import solve_weighted_ridge_batched
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from art.sharding import max_over_ranks, rank_info, rank_seed
+
+    ri = rank_info()
+    world, rank, local = ri.world, ri.rank, ri.local
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     N.load_library()
-    wl = workloads.ridge_systems(args.systems, seed=2 + rank, device="cuda")
+    wl = workloads.ridge_systems(args.systems, seed=rank_seed(2, rank), device="cuda")
     ro = torch.from_numpy(wl.row_offsets).to(dev)
     xo = torch.from_numpy(wl.x_offsets).to(dev)
     dims = torch.from_numpy(wl.dims).to(dev)
@@ -516,10 +526,7 @@ def run_b200(args):
         ms = e0.elapsed_time(e1)
         launches = N.launch_count() - launches0
         prof = N.profile_report()
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ms)
         return ms / args.steps, launches // args.steps, prof, out
 
     # plain FP64 form, batched and per node (one call per system, the
@@ -594,10 +601,7 @@ def run_b200(args):
         e1.record(stream)
         barrier()
         e2e_ms = max(e0.elapsed_time(e1), 1000.0 * (time.perf_counter() - t0)) / args.steps
-        if world > 1:
-            t = torch.tensor([e2e_ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t.item())
+        e2e_ms = max_over_ranks(e2e_ms)
         h2d = sum(int(t.numel() * t.element_size()) for t in (hx, hy, hw, *meta))
         d2h = int(hbeta.numel() * 8 + hstat.numel() * 4)
         e2e = {"value": world * args.systems / (e2e_ms / 1000.0), "unit": UNIT,

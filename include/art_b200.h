@@ -126,7 +126,9 @@ typedef struct ArtRidgeProblem {
   int32_t max_features;   /* host-known upper bound of p over the batch     */
   int32_t max_dim;        /* host-known upper bound of d (0: use max_features) */
   uint32_t options;       /* ART_RIDGE_OPT_* bits                           */
-  int32_t reserved;
+  int32_t tensor_min_features; /* mixed form: systems with p >= this go to the
+                                  tensor-core kernel, smaller ones to the FP64
+                                  kernels (0: 33; > 160: none)               */
 } ArtRidgeProblem;
 
 /* Mixed form: factor the tensor-core Gram in FP64 instead of FP32 (fewer
@@ -201,6 +203,10 @@ typedef struct ArtSplitParams {
   int32_t precision;            /* ART_PRECISION_FP64 or _MIXED (FP32 core) */
   double anneal_ratio;          /* T_k = T * anneal_ratio^(k/(max_iters-1)); 1 = off */
   uint64_t seed;                /* Philox key for device initialisation     */
+  int32_t group_restarts;       /* restarts sharing one CTA's row passes
+                                   (0: the largest that fits, <= 16)         */
+  int32_t trial_steps;          /* Armijo step sizes evaluated per trial pass
+                                   (0: min(32, 256 / group, backtracks + 1)) */
 } ArtSplitParams;
 
 typedef struct ArtSplitProblem {

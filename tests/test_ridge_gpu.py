@@ -313,3 +313,44 @@ def test_mixed_edge_cases_fall_back_to_fp64_statuses():
                                        precision="mixed", max_features=45, max_dim=d)
     st = out.status.cpu().numpy()
     assert st[0] == 1 and st[1] == -2 and st[2] == -1
+
+
+def test_tensor_threshold_routes_feature_classes():
+    """The mixed form's tensor-core threshold only moves systems between kernels:
+    every routing meets the oracle tolerance, and systems below the threshold
+    carry no refinement passes (FP64 kernels)."""
+
+    from art import _native as N
+    from art.models import solve_weighted_ridge_batched
+
+    wl = make_batch(K=64, seed=11, n_max=900)
+    p = np.array([O.feature_count(int(d), int(k)) for d, k in zip(wl.dims, wl.kinds)])
+    for threshold in (33, 46, 161):
+        out = solve_weighted_ridge_batched(wl.x, wl.y, wl.w, wl.row_offsets, wl.dims, wl.kinds, wl.ridge,
+                                           x_offsets=wl.x_offsets, precision="mixed",
+                                           max_features=wl.max_features, max_dim=wl.max_dim,
+                                           tensor_min_features=threshold)
+        _oracle_check(wl, out)
+        passes = (out.info.cpu().numpy() >> N.INFO_REFINE_SHIFT) & 255
+        assert np.all(passes[p < threshold] == 0), threshold
+
+
+def test_autotuned_threshold_is_stored_and_used():
+    from art import autotune
+    from art.models import solve_weighted_ridge_batched
+
+    autotune.clear()
+    try:
+        wl = make_batch(K=64, seed=12, n_max=1500)
+        entry = autotune.tune_ridge_threshold(wl.x, wl.y, wl.w, wl.row_offsets, wl.dims, wl.kinds, wl.ridge,
+                                              x_offsets=wl.x_offsets, max_dim=wl.max_dim, per_class=16,
+                                              repeats=1)
+        assert entry["tensor_min_features"] in (45, 153, autotune.NO_TENSOR)
+        assert set(entry["classes"]) == {"45", "153"}
+        assert autotune.cached_ridge_threshold() == entry["tensor_min_features"]
+        out = solve_weighted_ridge_batched(wl.x, wl.y, wl.w, wl.row_offsets, wl.dims, wl.kinds, wl.ridge,
+                                           x_offsets=wl.x_offsets, precision="mixed",
+                                           max_features=wl.max_features, max_dim=wl.max_dim)
+        _oracle_check(wl, out)
+    finally:
+        autotune.clear()

@@ -162,3 +162,47 @@ def test_public_split_api_matches_oracle():
     np.testing.assert_allclose(np.r_[out.w, out.z], np.r_[ref["w"], ref["z"]], rtol=1e-9, atol=1e-11)
     np.testing.assert_allclose(out.predict(X), np.where((X @ ref["w"] - ref["z"]) >= 0, phi @ ref["br"], phi @ ref["bl"]),
                                rtol=1e-8, atol=1e-10)
+
+
+@pytest.mark.parametrize("shape", [(1, 1), (2, 4), (3, 32), (8, 2)])
+def test_launch_shape_does_not_change_results(shape):
+    """Restarts per CTA and trial steps per pass only regroup work: every
+    output is bit-identical to the library's default shape."""
+
+    from art.splitters import split_level
+
+    ns, Xs, ys, th0, kd = random_level(5)
+    K = len(ns)
+    s = splitter_for(O.AFFINE, 0.15, 1e-6, th0.shape[1], 12, {"min_side_points": 5})
+    ro = np.concatenate([[0], np.cumsum(ns)])
+    args = (s, np.concatenate([X.reshape(-1) for X in Xs]), np.concatenate(ys), ro, [4] * K, kd, 0.15, 1e-6)
+    base = split_level(*args, theta0=th0, anneal_ratio=0.3, traces=True, group_restarts=0, trial_steps=0)
+    got = split_level(*args, theta0=th0, anneal_ratio=0.3, traces=True, group_restarts=shape[0],
+                      trial_steps=shape[1])
+    for name in ("theta", "beta", "loss", "n_right", "n_iters", "stop_reason", "failure", "final_alpha",
+                 "trace_loss", "trace_step"):
+        a, b = getattr(base, name).cpu().numpy(), getattr(got, name).cpu().numpy()
+        np.testing.assert_array_equal(a, b, err_msg=name)
+
+
+def test_long_nodes_stream_through_the_row_ring():
+    """Nodes much longer than the row ring (many chunks per pass) match the oracle."""
+
+    from art.splitters import level_result_to_split, split_level
+
+    rng = np.random.default_rng(12)
+    ns = [3001, 1, 33, 2048]
+    Xs = [rng.uniform(-1, 1, (n, 3)) for n in ns]
+    ys = [np.sin(3 * X[:, 0]) + X[:, 1] * X[:, 2] for X in Xs]
+    T, lam, iters = 0.2, 1e-6, 8
+    s = splitter_for(O.AFFINE, T, lam, 1, iters, {"min_side_points": 1})
+    th0 = np.array([[[0.6, 0.8, 0.0, 0.05]] for _ in ns])
+    ro = np.concatenate([[0], np.cumsum(ns)])
+    res = split_level(s, np.concatenate([X.reshape(-1) for X in Xs]), np.concatenate(ys), ro, [3] * 4,
+                      [O.AFFINE] * 4, T, lam, parent_loss=[1.0] * 4, theta0=th0)
+    p = S.Params(max_iters=iters, n_restarts=1, min_side_points=1)
+    for k in (0, 3):
+        opt = S.optimize(Xs[k], ys[k], th0[k][0], T, O.AFFINE, lam, p)
+        out = level_result_to_split(s, res, k, ns[k], 1.0, True)
+        np.testing.assert_allclose(np.r_[out.w, out.z], opt["theta"], rtol=1e-9, atol=1e-11)
+        assert out.n_iters == opt["n_iters"]
