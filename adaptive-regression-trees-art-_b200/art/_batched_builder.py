@@ -32,6 +32,9 @@ def build_bfs(builder: "RegressionTreeBuilder", work: "_NodeWork",
 
     while queue:
         ready = []
+        # children about to be prepared get their samples in one launch, with
+        # the builder's draws taken in the same order as one at a time
+        builder._top_up_cohort([queue[i] for i in range(min(len(queue), builder.node_batch_size))])
         while queue and len(ready) < builder.node_batch_size:
             job = queue.popleft()
             leaf = builder._prepare_node(job)

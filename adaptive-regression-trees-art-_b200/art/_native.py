@@ -200,8 +200,19 @@ def launch_count() -> int:
     return int(load_library().art_launch_count())
 
 
+_profiling = False
+
+
 def profile_enable(on: bool = True) -> None:
+    global _profiling
     load_library().art_profile_enable(1 if on else 0)
+    _profiling = bool(on)
+
+
+def profiling() -> bool:
+    """Whether the library's per-launch profiler was last switched on."""
+
+    return _profiling
 
 
 def profile_reset() -> None:

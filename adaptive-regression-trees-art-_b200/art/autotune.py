@@ -211,7 +211,7 @@ def split_candidates(R: int, max_backtracks: int) -> list[tuple[int, int]]:
     out = []
     for g in groups:
         hmax = min(32, max(1, 256 // g), max_backtracks + 1)
-        for h in sorted({hmax, max(1, hmax // 2), min(hmax, 4)}, reverse=True):
+        for h in sorted({min(hmax, v) for v in (2, 4, 8, 16)}, reverse=True):
             out.append((g, h))
     return out
 

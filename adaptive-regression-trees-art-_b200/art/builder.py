@@ -9,7 +9,9 @@ Every numeric step runs on the GPU kernels: node fits (``art_ridge_batched``),
 split searches (``art_split_level``) and hit-and-run top-ups
 (``art_hit_and_run``).  With ``traversal="bfs"`` and the default
 ``level_dispatch=True`` a whole ready cohort is split in one launch sequence
-(the reference's BatchedSplitDispatcher role, _cuda_batched_builder.py:18-101).
+(the reference's BatchedSplitDispatcher role, _cuda_batched_builder.py:18-101),
+replayed from a captured CUDA graph per level shape class when
+``cuda_graphs=True`` (the default; see ``art.graphs``).
 
 Random streams are consumed in the reference's order (seeds from
 ``_next_seed``, host draws for sampler directions and splitter
@@ -90,6 +92,9 @@ class _NodeWork:
     metadata: dict[str, object] = field(default_factory=dict)
     convergence: dict[str, object] = field(default_factory=dict)
     prepared: PreparedDesign | None = None
+    topped: bool = False                      # samples already topped up (cohort launch)
+    topup_error: Exception | None = None      # the top-up's failure, raised at prepare
+    topup_pending: tuple | None = None        # cohort top-up awaiting its oracle values
 
 
 @dataclass
@@ -151,6 +156,8 @@ class RegressionTreeBuilder:
     batch_reorder: bool = True
     check_split_gain: bool = False
     level_dispatch: bool = True
+    cuda_graphs: bool = True
+    cohort_top_up: bool = True
     verbose: bool = False
 
     oracle_queries: int = field(default=0, init=False)
@@ -282,7 +289,11 @@ class RegressionTreeBuilder:
         if work.parent is not None:
             inherited = work.samples
             try:
-                work.samples = self._top_up_child(work.region, inherited.X, inherited.y)
+                if work.topped:
+                    if work.topup_error is not None:
+                        raise work.topup_error
+                else:
+                    work.samples = self._top_up_child(work.region, inherited.X, inherited.y)
             except (RuntimeError, ValueError) as exc:
                 prepared = self._prepare_design(inherited.X)
                 model, pred = self._fit_node_model(inherited.X, inherited.y, prepared)
@@ -373,6 +384,81 @@ class RegressionTreeBuilder:
             X, y = samples.X[mask], samples.y[mask]
             yield _NodeWork(child.region, _NodeSamples(X, y, n_inherited=len(X), n_new=0), child.depth,
                             child.node_id, parent=node, side=side)
+
+    def _top_up_cohort(self, jobs) -> None:
+        """Top up a cohort's children with one hit-and-run launch.
+
+        Only for the plain sampler with device draws: every child's builder
+        draws (subsample, start point, sampler seed) are taken in cohort order
+        exactly as the one-child-at-a-time top-up takes them, and each child's
+        chain uses its own seed, so the samples are the ones the sequential
+        top-ups produce.  Children whose chain reports a failure are redone by
+        the sequential path (which reproduces the failure at the same step).
+        """
+
+        from .sampling import HitAndRunSampler
+
+        sp = self.sampler
+        if (not self.cohort_top_up or type(sp) is not HitAndRunSampler or getattr(sp, "rng_mode", "reference") != "device"
+                or self.isotropic_sampling or sp.direction_eigenvectors is not None
+                or sp.direction_eigenvalues is not None):
+            return
+        todo = [j for j in jobs if j.parent is not None and not j.topped]
+        if len(todo) < 2:
+            return
+        reqs = []
+        with self._timing_context("sampling"):
+            for job in todo:
+                job.topped = True
+                X = np.asarray(job.samples.X, dtype=float)
+                y = np.asarray(job.samples.y, dtype=float).reshape(-1)
+                if X.shape[0] == 0:
+                    job.topup_error = RuntimeError("Cannot seed child sampling without an inherited point.")
+                    continue
+                if X.shape[0] > self._target_samples:
+                    keep = self._rng.choice(X.shape[0], size=self._target_samples, replace=False)
+                    X, y = X[keep], y[keep]
+                n_inh = X.shape[0]
+                n_new = self._target_samples - n_inh
+                if n_new == 0:
+                    job.samples = _NodeSamples(X, y, n_inh, 0, sampling_metadata={
+                        "sampling_method": "inherited_only", "sampling_thinning": None,
+                        "sampling_pilot_length": 0, "sampling_covariance_condition_number": None,
+                        "sampling_warnings": ()})
+                    continue
+                x0 = X[int(self._rng.integers(0, n_inh))]
+                reqs.append((job, X, y, n_inh, n_new, x0, self._next_seed()))
+            if not reqs:
+                return
+            out = sp.sample_many([r[0].region for r in reqs], [r[4] for r in reqs], [r[6] for r in reqs],
+                                 [r[5] for r in reqs])
+            meta = {"sampling_method": type(sp).__name__, "sampling_thinning": sp.thinning,
+                    "sampling_pilot_length": 0, "sampling_covariance_condition_number": None,
+                    "sampling_warnings": ()}
+            for (job, X, y, n_inh, n_new, x0, seed), X_new in zip(reqs, out):
+                if isinstance(X_new, Exception):
+                    job.topup_error = X_new
+                    continue
+                if X_new.shape != (n_new, self.dimension):
+                    job.topup_error = RuntimeError(f"Sampler returned shape {X_new.shape}; expected "
+                                                   f"{(n_new, self.dimension)}.")
+                    continue
+                if not np.all(job.region.contains(X_new)):
+                    job.topup_error = RuntimeError("Sampler returned points outside the region.")
+                    continue
+                job.topup_pending = (X, y, n_inh, n_new, X_new, dict(meta))
+        for job, *_ in reqs:
+            pend = getattr(job, "topup_pending", None)
+            if pend is None or job.topup_error is not None:
+                continue
+            X, y, n_inh, n_new, X_new, m = pend
+            job.topup_pending = None
+            try:
+                y_new = self._query_oracle(X_new)
+            except (RuntimeError, ValueError) as exc:
+                job.topup_error = exc
+                continue
+            job.samples = _NodeSamples(np.vstack([X, X_new]), np.concatenate([y, y_new]), n_inh, n_new, m)
 
     def _top_up_child(self, region, inherited_X, inherited_y) -> _NodeSamples:
         """builder.py:502-551"""
@@ -755,10 +841,20 @@ class LevelSplitDispatcher:
                     temps.append(s0.temperature if states[j].temperature is None else states[j].temperature)
                     fb.append(1 if states[j].fallback else 0)
                     parents.append(job.parent_mse)
-                res = split_level(s0, np.concatenate(Xs), np.concatenate(ys), ro, [d] * len(pending),
-                                  [kind] * len(pending), temps, s0.model_template.ridge, parent_loss=parents,
-                                  min_side_fallback=fb, theta0=np.array(th0), hard_refit=b.hard_refits,
-                                  traces=b.store_diagnostics)
+                if b.cuda_graphs:
+                    from .graphs import shared_split_graphs
+                    from .models import kind_feature_count
+
+                    res = shared_split_graphs().split_level(
+                        s0, np.concatenate(Xs), np.concatenate(ys), ro, [d] * len(pending), [kind] * len(pending),
+                        temps, s0.model_template.ridge, parent_loss=parents, min_side_fallback=fb,
+                        theta0=np.array(th0), hard_refit=b.hard_refits, traces=b.store_diagnostics,
+                        max_dim=d, max_features=kind_feature_count(d, kind))
+                else:
+                    res = split_level(s0, np.concatenate(Xs), np.concatenate(ys), ro, [d] * len(pending),
+                                      [kind] * len(pending), temps, s0.model_template.ridge, parent_loss=parents,
+                                      min_side_fallback=fb, theta0=np.array(th0), hard_refit=b.hard_refits,
+                                      traces=b.store_diagnostics)
             again = []
             for q, j in enumerate(pending):
                 job = jobs[j][1]

@@ -334,6 +334,62 @@ class HitAndRunSampler:
         _raise_status(status.cpu().numpy())
         return samples[:, 0, :].cpu().numpy()
 
+    def sample_many(self, regions, ns, random_states, x0s) -> list:
+        """``sample`` for several regions of one dimension in one launch.
+
+        Device draws only (``rng_mode="device"``, no direction spectrum).
+        Item k is what ``sample(regions[k], ns[k], random_states[k], x0s[k])``
+        returns, or the exception it raises: each chain is keyed by the seed
+        its own random state yields, and a chain's first n samples do not
+        depend on how many more it runs.  A chain that reports a failure is
+        rerun alone, which reproduces the single call exactly.
+        """
+
+        if self.rng_mode != "device" or self.direction_eigenvectors is not None \
+                or self.direction_eigenvalues is not None:
+            raise ValueError("sample_many needs rng_mode='device' and isotropic directions")
+        if self.burn_in < 0:
+            raise ValueError("burn_in must be nonnegative.")
+        if self.thinning < 1:
+            raise ValueError("thinning must be at least 1.")
+        out: list = [None] * len(regions)
+        live = []
+        for k, (reg, n, rs, x0) in enumerate(zip(regions, ns, random_states, x0s)):
+            n = int(n)
+            if n < 0:
+                out[k] = ValueError("n must be nonnegative.")
+                continue
+            rng = as_rng(rs)
+            x = np.asarray(x0, dtype=float).reshape(-1)
+            if x.shape[0] != reg.dimension:
+                out[k] = ValueError(f"x0 must have shape ({reg.dimension},), got {x.shape}.")
+                continue
+            if not bool(reg.contains(x, tol=self.feasibility_tol)[0]):
+                out[k] = ValueError("x0 is not feasible for the region.")
+                continue
+            if n == 0:
+                out[k] = np.empty((0, reg.dimension))
+                continue
+            live.append((k, reg, n, x, int(rng.integers(0, 2**63 - 1))))
+        if not live:
+            return out
+        polys = device_polytopes([it[1] for it in live])
+        samples, _, status = hit_and_run_device(
+            polys, np.arange(len(live)), np.stack([it[3] for it in live]), burn_in=self.burn_in,
+            thinning=self.thinning, n_rounds=max(it[2] for it in live), mode="scalar",
+            seeds=[it[4] for it in live])
+        st = status.cpu().numpy()
+        host = samples.cpu().numpy()
+        for c, (k, reg, n, x, _) in enumerate(live):
+            if st[c] != 0:
+                try:
+                    out[k] = self.sample(reg, n, random_state=random_states[k], x0=x0s[k])
+                except (RuntimeError, ValueError) as exc:
+                    out[k] = exc
+            else:
+                out[k] = host[:n, c, :].copy()
+        return out
+
     def _direction_spectrum(self, dimension: int):
         vecs, vals = self.direction_eigenvectors, self.direction_eigenvalues
         if vecs is None and vals is None:

@@ -160,12 +160,19 @@ class LevelResult:
 
 def split_params(s: "SoftObliqueSplitter", hard_refit: bool, anneal_ratio: float = 1.0, seed: int = 0,
                  group_restarts: int = 0, trial_steps: int = 0):
+    """ArtSplitParams of a splitter.  ``precision="mixed"`` evaluates the
+    sigmoid gates in single precision (objective within 1e-5 relative of the
+    FP64 form); sums, solves and the side decisions stay FP64."""
+
+    if getattr(s, "precision", "fp64") not in ("fp64", "mixed"):
+        raise ValueError("precision must be 'fp64' or 'mixed'.")
     return N.ArtSplitParams(
         int(s.max_iters), int(max(1, s.n_restarts)), float(s.grad_atol), float(s.grad_rtol),
         int(s.min_side_points), float(s.min_side_fraction), float(s.alpha0), float(s.rho),
         float(s.armijo_c), int(s.max_backtracks), int(bool(s.adaptive_alpha)), float(s.alpha_min),
         float(s.alpha_max), float(s.alpha_grow), float(s.alpha_recovery), int(s.heavy_backtrack_threshold),
-        int(s.max_line_search_failures), float(s.weight_floor), int(bool(hard_refit)), N.PRECISION_FP64,
+        int(s.max_line_search_failures), float(s.weight_floor), int(bool(hard_refit)),
+        N.PRECISION_MIXED if getattr(s, "precision", "fp64") == "mixed" else N.PRECISION_FP64,
         float(anneal_ratio), int(seed) & ((1 << 64) - 1), int(group_restarts), int(trial_steps))
 
 
@@ -174,7 +181,7 @@ def split_level(splitter: "SoftObliqueSplitter", x, y, row_offsets, dims, featur
                 hard_refit: bool = True, anneal_ratio: float = 1.0, seed: int = 0, traces: bool = False,
                 max_dim: int | None = None, max_features: int | None = None, node_keys=None,
                 group_restarts: int | None = None, trial_steps: int | None = None,
-                stream=None) -> LevelResult:
+                out: LevelResult | None = None, workspace=None, stream=None) -> LevelResult:
     """Split K nodes in one launch sequence; arrays are numpy or torch (moved to the device).
 
     theta0, when given, is (K, R, d_max + 1); otherwise restarts start from
@@ -184,6 +191,9 @@ def split_level(splitter: "SoftObliqueSplitter", x, y, row_offsets, dims, featur
     ``group_restarts`` / ``trial_steps`` fix the kernel's launch shape
     (restarts per CTA, Armijo steps per trial pass); None takes the
     autotuned choice for (d, p, R) on this device, else the library's.
+    ``out`` (a LevelResult of K rows) and ``workspace`` (a uint8 device
+    tensor of at least ``art_split_workspace_size`` bytes) make the call
+    allocate nothing, as a captured graph needs.
     """
 
     t = torch()
@@ -203,7 +213,9 @@ def split_level(splitter: "SoftObliqueSplitter", x, y, row_offsets, dims, featur
     rid = to_device(np.broadcast_to(np.asarray(ridge, float), (K,)).copy() if not isinstance(ridge, t.Tensor) else ridge, t.float64, dev)
     pl = None if parent_loss is None else to_device(np.asarray(parent_loss, float).reshape(K) if not isinstance(parent_loss, t.Tensor) else parent_loss, t.float64, dev)
     fb = None
-    if min_side_fallback is not None:
+    if isinstance(min_side_fallback, t.Tensor):
+        fb = to_device(min_side_fallback, t.int8, dev)
+    elif min_side_fallback is not None:
         fb = to_device(np.broadcast_to(np.asarray(min_side_fallback, dtype=np.int8), (K,)).copy(), t.int8, dev)
     elif splitter.min_side_fallback:
         fb = t.ones(K, dtype=t.int8, device=dev)
@@ -217,6 +229,39 @@ def split_level(splitter: "SoftObliqueSplitter", x, y, row_offsets, dims, featur
         th0 = to_device(theta0, t.float64, dev).reshape(K * R, -1).contiguous()
         stride = int(th0.shape[1])
     M = int(splitter.max_iters)
+    if out is None:
+        out = _level_result(K, R, M, int(max_dim), int(max_features), traces, dev)
+    nk = None
+    if node_keys is not None:
+        nk = to_device(np.asarray(node_keys, dtype=np.uint64).view(np.int64) if not isinstance(node_keys, t.Tensor)
+                       else node_keys, t.int64, dev)
+    seg = N.ArtSegments(K, ptr(ro), ptr(xo), ptr(dims_t), ptr(feats))
+    prob = N.ArtSplitProblem(seg, ptr(x), ptr(y), ptr(temp), ptr(rid), ptr(pl), ptr(fb), ptr(th0), stride,
+                             int(max_dim), int(max_features), ptr(nk))
+    if group_restarts is None or trial_steps is None:
+        from . import autotune
+
+        g_auto, h_auto = autotune.cached_split_shape(int(max_dim), int(max_features), R)
+        group_restarts = g_auto if group_restarts is None else group_restarts
+        trial_steps = h_auto if trial_steps is None else trial_steps
+    prm = split_params(splitter, hard_refit, anneal_ratio, seed, group_restarts, trial_steps)
+    res = N.ArtSplitResult(ptr(out.theta), int(out.theta.shape[1]), ptr(out.beta), int(out.beta.shape[2]),
+                           ptr(out.loss), ptr(out.child_loss), ptr(out.ridge_effective), ptr(out.n_right),
+                           ptr(out.n_iters), ptr(out.stop_reason), ptr(out.failure), ptr(out.flags),
+                           ptr(out.fallback_iteration), ptr(out.final_alpha), ptr(out.trace_loss),
+                           ptr(out.trace_step), ptr(out.trace_backtracks), ptr(out.trace_grad_norm))
+    nbytes = lib.art_split_workspace_size(K, R, int(max_dim), int(max_features))
+    ws = WORKSPACES.get(nbytes, stream) if workspace is None else workspace
+    if ws.numel() < nbytes:
+        raise ValueError(f"split workspace of {ws.numel()} bytes < {nbytes} required")
+    N.check(lib.art_split_level(C.byref(prob), C.byref(prm), C.byref(res), ptr(ws), ws.numel(),
+                                stream_handle(stream)), "art_split_level")
+    out._keepalive = (x, y, ro, xo, dims_t, feats, temp, rid, pl, fb, th0, nk)
+    return out
+
+
+def _level_result(K, R, M, max_dim, max_features, traces, dev) -> LevelResult:
+    t = torch()
     out = LevelResult(
         theta=t.full((K, max_dim + 1), float("nan"), dtype=t.float64, device=dev),
         beta=t.full((K, 2, max_features), float("nan"), dtype=t.float64, device=dev),
@@ -232,30 +277,6 @@ def split_level(splitter: "SoftObliqueSplitter", x, y, row_offsets, dims, featur
         out.trace_grad_norm = t.full((K, R, M + 1), float("nan"), dtype=t.float64, device=dev)
         out.trace_step = t.full((K, R, max(M, 1)), float("nan"), dtype=t.float64, device=dev)
         out.trace_backtracks = t.full((K, R, max(M, 1)), -1, dtype=t.int32, device=dev)
-    seg = N.ArtSegments(K, ptr(ro), ptr(xo), ptr(dims_t), ptr(feats))
-    nk = None
-    if node_keys is not None:
-        nk = to_device(np.asarray(node_keys, dtype=np.uint64).view(np.int64) if not isinstance(node_keys, t.Tensor)
-                       else node_keys, t.int64, dev)
-    prob = N.ArtSplitProblem(seg, ptr(x), ptr(y), ptr(temp), ptr(rid), ptr(pl), ptr(fb), ptr(th0), stride,
-                             int(max_dim), int(max_features), ptr(nk))
-    if group_restarts is None or trial_steps is None:
-        from . import autotune
-
-        g_auto, h_auto = autotune.cached_split_shape(int(max_dim), int(max_features), R)
-        group_restarts = g_auto if group_restarts is None else group_restarts
-        trial_steps = h_auto if trial_steps is None else trial_steps
-    prm = split_params(splitter, hard_refit, anneal_ratio, seed, group_restarts, trial_steps)
-    res = N.ArtSplitResult(ptr(out.theta), max_dim + 1, ptr(out.beta), max_features, ptr(out.loss),
-                           ptr(out.child_loss), ptr(out.ridge_effective), ptr(out.n_right), ptr(out.n_iters),
-                           ptr(out.stop_reason), ptr(out.failure), ptr(out.flags), ptr(out.fallback_iteration),
-                           ptr(out.final_alpha), ptr(out.trace_loss), ptr(out.trace_step),
-                           ptr(out.trace_backtracks), ptr(out.trace_grad_norm))
-    nbytes = lib.art_split_workspace_size(K, R, int(max_dim), int(max_features))
-    ws = WORKSPACES.get(nbytes, stream)
-    N.check(lib.art_split_level(C.byref(prob), C.byref(prm), C.byref(res), ptr(ws), ws.numel(),
-                                stream_handle(stream)), "art_split_level")
-    out._keepalive = (x, y, ro, xo, dims_t, feats, temp, rid, pl, fb, th0, nk)
     return out
 
 
@@ -292,6 +313,7 @@ class SoftObliqueSplitter:
     backtrack_batch_size: int = 8
     qr_parallel: bool = True
     Xw_refresh: int = 32
+    precision: Literal["fp64", "mixed"] = "fp64"
 
     def _validate_inputs(self, X: np.ndarray, y: np.ndarray) -> None:
         """splitters.py:732-750"""

@@ -165,6 +165,21 @@ __device__ inline void normal_pair(const Philox4& r, double& z0, double& z1) {
   z1 = rad * s;
 }
 
+// The same transform in single precision for directions drawn on the device:
+// a direction only needs i.i.d. Gaussian coordinates (the chord arithmetic
+// that uses it stays FP64), and CUDA's logf/sqrtf/sincospif cost a fraction
+// of the double-precision functions.  24-bit uniforms: u1 in (0, 1), so the
+// radius is finite (at most ~5.9).
+__device__ inline void normal_pair_f32(const Philox4& r, double& z0, double& z1) {
+  const float u1 = ((float)(r.v[0] >> 8) + 0.5f) * (1.0f / 16777216.0f);
+  const float u2 = (float)(r.v[2] >> 8) * (1.0f / 16777216.0f);
+  const float rad = sqrtf(-2.0f * logf(u1));
+  float sn, cs;
+  sincospif(2.0f * u2, &sn, &cs);
+  z0 = (double)(rad * cs);
+  z1 = (double)(rad * sn);
+}
+
 // ---------------------------------------------------------------- misc
 __device__ __forceinline__ bool finite(double v) { return isfinite(v); }
 

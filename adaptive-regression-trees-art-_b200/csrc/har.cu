@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(kHarThreads) har_kernel(HarArgs a) {
       const uint64_t ctr = a.counter_base + (uint64_t)step;
       Philox4 r = philox4x32_10((uint32_t)ctr, (uint32_t)(ctr >> 32), (uint32_t)lane, 0u, key0,
                                 key1);
-      normal_pair(r, u0, u1);
+      normal_pair_f32(r, u0, u1);
       if (!h0) u0 = 0.0;
       if (!h1) u1 = 0.0;
     }

@@ -46,7 +46,6 @@ constexpr int kLBO = 128;                  // bytes between K-adjacent core matr
 constexpr int kSBO = (kKC / kKE) * 128;    // bytes between 8-feature groups
 constexpr int kOpBytes = kGroups * kSBO;   // one operand array (hi or lo)
 constexpr int kMaxRefine = 14;
-constexpr int kRefRows = 4;                // rows per warp step in refinement passes
 // TMEM accumulation chains are restarted every kDrainChunks stages: the
 // FP32 accumulator of the tensor core loses low bits on every step, so the
 // chain length bounds the Gram error (~steps * 2^-24 relative); drained
@@ -500,7 +499,6 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
     // e_k = q_k phi_k . beta (warp shuffle sum) and the accumulation of
     // e_k phi_k; the 8 row slots are summed in a fixed order at the end.
     const int slot = warp, fl = lane;
-    const int mslots = (p + 31) >> 5;  // feature slots in use (<= 5)
     int rfa[5], rfb[5];
 #pragma unroll
     for (int m = 0; m < 5; ++m) {
@@ -550,42 +548,23 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
         const double* ws = a.w ? (const double*)(op + st * rstage + rx_bytes +
                                                  (((uintptr_t)(a.w + it.r0 + c * RC)) & 15))
                                : nullptr;
-        // four rows per warp step (slot, slot+8, slot+16, slot+24 of a group)
-        // so their shuffle reductions overlap; rows are still accumulated in
-        // the order slot, slot+8, ... of the single-row loop
-        for (int j0 = slot; j0 < rows; j0 += kRefRows * (kTcThreads / 32)) {
-          double dot[kRefRows], ph[kRefRows][5];
+        for (int j = slot; j < rows; j += kTcThreads / 32) {
+          const double* xk = xs + j * d;
+          double ph[5];
+          double dot = 0.0;
 #pragma unroll
-          for (int u = 0; u < kRefRows; ++u) {
-            const int j = j0 + (kTcThreads / 32) * u;
-            const double* xk = xs + (j < rows ? j : j0) * d;
-            dot[u] = 0.0;
-#pragma unroll
-            for (int m = 0; m < 5; ++m) {
-              ph[u][m] = 0.0;
-              if (m < mslots) {
-                const int ua = rfa[m], ub = rfb[m];
-                const double va = ua >= 0 ? xk[ua] : (ua == -1 ? 1.0 : 0.0);
-                const double vb = ub >= 0 ? xk[ub] : 1.0;
-                ph[u][m] = va * vb;
-                dot[u] = fma(ph[u][m], bt[m], dot[u]);
-              }
-            }
+          for (int m = 0; m < 5; ++m) {
+            const int ua = rfa[m], ub = rfb[m];
+            const double va = ua >= 0 ? xk[ua] : (ua == -1 ? 1.0 : 0.0);
+            const double vb = ub >= 0 ? xk[ub] : 1.0;
+            ph[m] = va * vb;
+            dot = fma(ph[m], bt[m], dot);
           }
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1)
+          for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
+          const double e = fmax(ws ? ws[j] : 1.0, a.weight_floor) * dot;
 #pragma unroll
-            for (int u = 0; u < kRefRows; ++u) dot[u] += __shfl_xor_sync(0xffffffffu, dot[u], o);
-#pragma unroll
-          for (int u = 0; u < kRefRows; ++u) {
-            const int j = j0 + (kTcThreads / 32) * u;
-            if (j < rows) {
-              const double e = fmax(ws ? ws[j] : 1.0, a.weight_floor) * dot[u];
-#pragma unroll
-              for (int m = 0; m < 5; ++m)
-                if (m < mslots) accb[m] = fma(e, ph[u][m], accb[m]);
-            }
-          }
+          for (int m = 0; m < 5; ++m) accb[m] = fma(e, ph[m], accb[m]);
         }
         __syncthreads();  // every warp is done with this stage
         if (c + 2 < nch) {

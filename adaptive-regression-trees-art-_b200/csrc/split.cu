@@ -34,7 +34,7 @@ namespace {
 
 constexpr int kSplitThreads = 256;
 constexpr int kWarps = kSplitThreads / 32;
-constexpr int kCH = 32;          // rows per chunk
+constexpr int kMaxCH = 256;      // rows per chunk: a multiple of 32 up to this
 constexpr int kMaxP = 64;        // child model features
 constexpr int kMaxRg = 16;       // restarts per work item
 constexpr int kRedSlots = 5;     // (restart, component) accumulators per thread
@@ -58,7 +58,8 @@ struct SplitArgs {
   int64_t theta0_stride;
   const uint64_t* node_keys;
   ArtSplitParams prm;
-  int R, Rg, groups, dmax, pmax, H, TC, S;
+  int R, Rg, groups, dmax, pmax, H, TC, S, CH;
+  int mixed;  // ART_PRECISION_MIXED: gates in single precision
   // per (node, restart) results, index k * R + r
   double* r_theta;   // [.. ][dmax + 1]
   double* r_loss;
@@ -81,26 +82,26 @@ struct SplitArgs {
   int32_t* items;    // [K * groups]
 };
 
-// Shared-memory layout for a given (dmax, pmax, Rg, H, S): `ring` holds S
-// stages of kCH rows of x and y (bulk copies in flight), `bars` their
+// Shared-memory layout for a given (dmax, pmax, Rg, H, S, CH): `ring` holds S
+// stages of CH rows of x and y (bulk copies in flight), `bars` their
 // mbarriers.
 struct SLayout {
   size_t ring, rx, rstage, bars, phi, q, G, cache, theta, dirn, grad, lastf, bl, br, trial, red, chol, eidx, rs,
       total;
 };
 __host__ __device__ inline size_t al(size_t v) { return (v + 15) & ~(size_t)15; }
-__host__ __device__ inline SLayout split_layout(int dmax, int pmax, int Rg, int H, int S) {
+__host__ __device__ inline SLayout split_layout(int dmax, int pmax, int Rg, int H, int S, int CH) {
   SLayout L;
   const int pa = pmax + 1, E = pa * (pa + 1) / 2, dt = dmax + 1;
   size_t o = 0;
-  L.rx = al((size_t)kCH * dmax * 8 + 32);
-  L.rstage = L.rx + al((size_t)kCH * 8 + 32);
+  L.rx = al((size_t)CH * dmax * 8 + 32);
+  L.rstage = L.rx + al((size_t)CH * 8 + 32);
   L.ring = o; o = al(o + (size_t)S * L.rstage);
   L.bars = o; o = al(o + (size_t)kMaxStages * 8);
-  L.phi = o; o = al(o + (size_t)kCH * pa * 8);
-  L.q = o; o = al(o + (size_t)kCH * 2 * Rg * 8);
+  L.phi = o; o = al(o + (size_t)CH * pa * 8);
+  L.q = o; o = al(o + (size_t)CH * 2 * Rg * 8);
   L.G = o; o = al(o + (size_t)E * 2 * Rg * 8);
-  L.cache = o; o = al(o + (size_t)kCH * Rg * 4 * 8);
+  L.cache = o; o = al(o + (size_t)CH * Rg * 4 * 8);
   L.theta = o; o = al(o + (size_t)Rg * dt * 8);
   L.dirn = o; o = al(o + (size_t)Rg * dt * 8);
   L.grad = o; o = al(o + (size_t)Rg * dt * 8);
@@ -124,6 +125,22 @@ enum RS {
   RS_HLOSSR, RS_PARENT, RS_COUNT_
 };
 
+// Row groups for a pass: the largest power of two <= 32 such that `items`
+// work items times the groups fit the CTA.  Group g of an item takes rows
+// g, g + RG, ... of every chunk; the RG threads of an item are consecutive
+// lanes of one warp (RG divides 32), so their partials are combined by a
+// fixed butterfly of shuffles.
+__device__ __forceinline__ int row_groups(int items) {
+  int rg = 1;
+  while (rg < 32 && items * rg * 2 <= kSplitThreads) rg <<= 1;
+  return rg;
+}
+// Sum over the RG consecutive lanes of a row group (every lane calls).
+__device__ __forceinline__ double group_sum(double v, int RG) {
+  for (int o = 1; o < RG; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
 struct Item {
   int64_t r0, n, xoff;
   int d, kind, p, pa, E;
@@ -134,6 +151,14 @@ struct Item {
 __device__ __forceinline__ double sigm(double s) {
   s = fmin(fmax(s, -50.0), 50.0);  // objectives.py:49-51
   return 1.0 / (1.0 + exp(-s));
+}
+
+// Mixed form: the gate in single precision with CUDA's fast exponential
+// (relative error ~1e-7, inside the form's 1e-5 objective tolerance); the
+// score, residuals, solves and every sum stay FP64.
+__device__ __forceinline__ double sigm32(double s) {
+  const float sf = fminf(fmaxf((float)s, -50.0f), 50.0f);
+  return (double)__frcp_rn(1.0f + __expf(-sf));
 }
 
 // Entry e of the packed lower triangle -> (i, j), i >= j.
@@ -190,7 +215,7 @@ struct SplitCta {
   int tid, lane, warp;
 
   __device__ SplitCta(const SplitArgs& a_, unsigned char* sm_) : a(a_), sm(sm_) {
-    L = split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S);
+    L = split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S, a.CH);
     rbar = (uint64_t*)(sm + L.bars);
     xs = (const double*)(sm + L.ring); ys = xs; phi = (double*)(sm + L.phi);
     Q = (double*)(sm + L.q); G = (double*)(sm + L.G); cache = (double*)(sm + L.cache);
@@ -201,6 +226,7 @@ struct SplitCta {
     tid = threadIdx.x; lane = tid & 31; warp = tid >> 5;
   }
   __device__ double& S(int r, int slot) { return rs[r * 32 + slot]; }
+  __device__ double gate(double s) const { return a.mixed ? sigm32(s) : sigm(s); }
   __device__ int dt() const { return it.d + 1; }
 
   // Row-stage ring: chunk ci of the current node goes to stage ci % S by
@@ -211,8 +237,8 @@ struct SplitCta {
   __device__ void ring_issue(int64_t ci) {
     const int st = (int)(ci % a.S);
     if (tid == 0) {
-      const int64_t c0 = ci * kCH;
-      const int rows = (int)min((int64_t)kCH, it.n - c0);
+      const int64_t c0 = ci * a.CH;
+      const int rows = (int)min((int64_t)a.CH, it.n - c0);
       Granules gx = granules(a.x + it.xoff + c0 * it.d, (uint64_t)rows * it.d * 8);
       Granules gy = granules(a.y + it.r0 + c0, (uint64_t)rows * 8);
       unsigned char* base = sm + L.ring + (size_t)st * L.rstage;
@@ -224,7 +250,7 @@ struct SplitCta {
   }
   __device__ void begin_pass() {
     if (rabort) return;
-    for (int st = 0; st < a.S && (int64_t)st * kCH < it.n; ++st) ring_issue(st);
+    for (int st = 0; st < a.S && (int64_t)st * a.CH < it.n; ++st) ring_issue(st);
   }
   // bounded waits for copies still in flight (only after a wait gave up)
   __device__ void ring_drain() {
@@ -239,12 +265,12 @@ struct SplitCta {
   // Rows [c0, c0 + rows) of x and y from the ring, then the augmented
   // features.  The caller's loop ends every chunk with __syncthreads().
   __device__ int load_chunk(int64_t c0) {
-    const int rows = (int)min((int64_t)kCH, it.n - c0);
+    const int rows = (int)min((int64_t)a.CH, it.n - c0);
     const int d = it.d;
-    const int64_t ci = c0 / kCH;
+    const int64_t ci = c0 / a.CH;
     const int st = (int)(ci % a.S);
     if (!rabort) {
-      if (ci >= 1 && (ci - 1 + a.S) * kCH < it.n) ring_issue(ci - 1 + a.S);
+      if (ci >= 1 && (ci - 1 + a.S) * a.CH < it.n) ring_issue(ci - 1 + a.S);
       const bool ok = mbar_wait(&rbar[st], (rpar >> st) & 1u);
       if (ok) {
         rpar ^= 1u << st;
@@ -291,11 +317,18 @@ struct SplitCta {
 
   // ---- Gram pass: G[e][c] = sum_k Q[k][c] P[k][e]; hard = gates from the
   // exact side of each row (weights 1/0, no floor), else soft gates.
+  // Threads beyond the tiles share their rows: RG row groups, group g taking
+  // rows g, g + RG, ... of every chunk; the group partials are added in
+  // group order at the end (RG = 1, one thread per tile, when the tiles
+  // already fill the CTA).
   __device__ void gram_pass(bool hard) {
     const int E = it.E, C2 = 2 * a.Rg;
     const int nct = (C2 + TC - 1) / TC, net = (E + TE - 1) / TE;
-    const bool mine = tid < nct * net;
-    const int ct = tid % nct, et = tid / nct;
+    const int ntiles = nct * net;
+    const int RG = row_groups(ntiles);
+    const int tile = tid / RG, grp = tid % RG;
+    const bool mine = tile < ntiles;
+    const int ct = tile % nct, et = tile / nct;
     int ei[TE], ej[TE];
 #pragma unroll
     for (int u = 0; u < TE; ++u) {
@@ -309,7 +342,7 @@ struct SplitCta {
 #pragma unroll
       for (int v = 0; v < TC; ++v) acc[u][v] = 0.0;
     begin_pass();
-    for (int64_t c0 = 0; c0 < it.n; c0 += kCH) {
+    for (int64_t c0 = 0; c0 < it.n; c0 += a.CH) {
       const int rows = load_chunk(c0);
       for (int pr = tid; pr < rows * a.Rg; pr += kSplitThreads) {
         const int row = pr / a.Rg, r = pr - row * a.Rg;
@@ -323,7 +356,7 @@ struct SplitCta {
             // integer-valued sums below 2^53 are exact in any order
             if (right) atomicAdd(&S(r, RS_NRIGHT), 1.0);
           } else {
-            const double pi = sigm((score(r, row) - th[r * dt() + it.d]) / S(r, RS_T));
+            const double pi = gate((score(r, row) - th[r * dt() + it.d]) / S(r, RS_T));
             qL = fmax(1.0 - pi, a.prm.weight_floor);
             qR = fmax(pi, a.prm.weight_floor);
           }
@@ -333,7 +366,7 @@ struct SplitCta {
       }
       __syncthreads();
       if (mine) {
-        for (int row = 0; row < rows; ++row) {
+        for (int row = grp; row < rows; row += RG) {
           const double* pr = phi + row * it.pa;
           const double* qr = Q + row * C2 + ct * TC;
           double pv[TE], qv[TC];
@@ -349,7 +382,11 @@ struct SplitCta {
       }
       __syncthreads();
     }
-    if (mine) {
+#pragma unroll
+    for (int u = 0; u < TE; ++u)
+#pragma unroll
+      for (int v = 0; v < TC; ++v) acc[u][v] = group_sum(acc[u][v], RG);
+    if (mine && grp == 0) {
 #pragma unroll
       for (int u = 0; u < TE; ++u)
 #pragma unroll
@@ -418,20 +455,25 @@ struct SplitCta {
   __device__ void resid_pass() {
     const int d = it.d, comps = d + 3;  // grad_w (d), sum a, loss, n_right
     const int pairs = a.Rg * comps;
+    // few (restart, component) pairs: RGr row groups share each pair (as in
+    // gram_pass), combined in group order at the end; otherwise one thread
+    // per pair over kRedSlots slots
+    const int RGr = pairs <= kSplitThreads ? row_groups(pairs) : 1;
+    const int gq = tid / RGr, ggrp = tid % RGr;
     double accs[kRedSlots];
 #pragma unroll
     for (int s = 0; s < kRedSlots; ++s) accs[s] = 0.0;
     double* coef = cache;                      // [row][r]: a_k
-    double* wl = cache + kCH * a.Rg;           // [row][r]: weighted loss term
-    double* nr = cache + 2 * kCH * a.Rg;       // [row][r]: pi >= 0.5
+    double* wl = cache + a.CH * a.Rg;          // [row][r]: weighted loss term
+    double* nr = cache + 2 * a.CH * a.Rg;      // [row][r]: pi >= 0.5
     begin_pass();
-    for (int64_t c0 = 0; c0 < it.n; c0 += kCH) {
+    for (int64_t c0 = 0; c0 < it.n; c0 += a.CH) {
       const int rows = load_chunk(c0);
       for (int pr = tid; pr < rows * a.Rg; pr += kSplitThreads) {
         const int row = pr / a.Rg, r = pr - row * a.Rg;
         double cf = 0.0, lw = 0.0, ge = 0.0;
         if (r < it.rn && S(r, RS_ACTIVE) != 0.0) {
-          const double pi = sigm((score(r, row) - th[r * dt() + d]) / S(r, RS_T));
+          const double pi = gate((score(r, row) - th[r * dt() + d]) / S(r, RS_T));
           const double yv = ys[row];
           const double eL = yv - fitted(bl + r * a.pmax, row);
           const double eR = yv - fitted(br + r * a.pmax, row);
@@ -445,6 +487,20 @@ struct SplitCta {
         nr[row * a.Rg + r] = ge;
       }
       __syncthreads();
+      if (RGr > 1) {
+        if (gq < pairs) {
+          const int r = gq / comps, cp = gq - r * comps;
+          double acc = accs[0];
+          for (int row = ggrp; row < rows; row += RGr) {
+            const double cv = coef[row * a.Rg + r];
+            if (cp < d) acc = fma(cv, xs[row * d + cp], acc);
+            else if (cp == d) acc += cv;
+            else if (cp == d + 1) acc += wl[row * a.Rg + r];
+            else acc += nr[row * a.Rg + r];
+          }
+          accs[0] = acc;
+        }
+      } else {
 #pragma unroll
       for (int s = 0; s < kRedSlots; ++s) {
         const int q = tid + s * kSplitThreads;
@@ -461,14 +517,21 @@ struct SplitCta {
           accs[s] = acc;
         }
       }
+      }
       __syncthreads();
     }
+    if (RGr > 1) {
+      const double tot = group_sum(accs[0], RGr);
+      if (gq < pairs && ggrp == 0) red[gq] = tot;
+      __syncthreads();
+    } else {
 #pragma unroll
-    for (int s = 0; s < kRedSlots; ++s) {
-      const int q = tid + s * kSplitThreads;
-      if (q < pairs) red[q] = accs[s];
+      for (int s = 0; s < kRedSlots; ++s) {
+        const int q = tid + s * kSplitThreads;
+        if (q < pairs) red[q] = accs[s];
+      }
+      __syncthreads();
     }
-    __syncthreads();
     // finalize per restart (one thread each)
     if (tid < it.rn && S(tid, RS_ACTIVE) != 0.0) {
       const int r = tid;
@@ -506,8 +569,12 @@ struct SplitCta {
     double* tal = trial;                       // [r][H] alpha
     double* tnr = trial + a.Rg * H;            // [r][H] ||w + alpha p_w||
     double* tf = trial + 2 * a.Rg * H;         // [r][H] accumulated loss
-    const bool mine = tid < a.Rg * H;
-    const int r = tid / H, j = tid - (tid / H) * H;
+    // row groups as in gram_pass: RG threads share each (restart, step) item
+    const int items = a.Rg * H;
+    const int RG = row_groups(items);
+    const int item = tid / RG, grp = tid % RG;
+    const bool mine = item < items;
+    const int r = item / H, j = item - (item / H) * H;
     double f = 0.0;
     const bool on = mine && r < it.rn && S(r, RS_SEARCH) != 0.0;
     double alpha = 0.0, nrm = 1.0, z = 0.0, pz = 0.0, T = 1.0;
@@ -519,7 +586,7 @@ struct SplitCta {
       T = S(r, RS_T);
     }
     begin_pass();
-    for (int64_t c0 = 0; c0 < it.n; c0 += kCH) {
+    for (int64_t c0 = 0; c0 < it.n; c0 += a.CH) {
       const int rows = load_chunk(c0);
       for (int pr = tid; pr < rows * a.Rg; pr += kSplitThreads) {
         const int row = pr / a.Rg, rr = pr - row * a.Rg;
@@ -538,16 +605,17 @@ struct SplitCta {
       }
       __syncthreads();
       if (on) {
-        for (int row = 0; row < rows; ++row) {
+        for (int row = grp; row < rows; row += RG) {
           const double* cp = cache + (row * a.Rg + r) * 4;
           const double s = ((cp[0] + alpha * cp[1]) / nrm - (z + alpha * pz)) / T;
-          const double pi = sigm(s);
+          const double pi = gate(s);
           f += (1.0 - pi) * cp[2] + pi * cp[3];
         }
       }
       __syncthreads();
     }
-    if (on) tf[r * H + j] = f / (double)it.n;
+    f = group_sum(f, RG);
+    if (on && grp == 0) tf[r * H + j] = f / (double)it.n;
     __syncthreads();
   }
 
@@ -847,7 +915,7 @@ __device__ void SplitCta<TC>::run(int item_id) {
     // side) in row order
     double sl = 0.0;
     begin_pass();
-    for (int64_t c0 = 0; c0 < it.n; c0 += kCH) {
+    for (int64_t c0 = 0; c0 < it.n; c0 += a.CH) {
       const int rows = load_chunk(c0);
       for (int pr = tid; pr < rows * a.Rg; pr += kSplitThreads) {
         const int row = pr / a.Rg, r = pr - row * a.Rg;
@@ -1120,9 +1188,9 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
     set_error("art_split_level: invalid splitter parameters");
     return ART_E_INVALID;
   }
-  if (prm->precision != ART_PRECISION_FP64) {
-    set_error("art_split_level: only the FP64 form is built");
-    return ART_E_UNSUPPORTED;
+  if (prm->precision != ART_PRECISION_FP64 && prm->precision != ART_PRECISION_MIXED) {
+    set_error("art_split_level: precision must be ART_PRECISION_FP64 or ART_PRECISION_MIXED");
+    return ART_E_INVALID;
   }
   if (out->theta_stride < pr->max_dim + 1 || (out->beta && out->beta_stride < pr->max_features)) {
     set_error("art_split_level: output strides too small");
@@ -1149,7 +1217,11 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
   a.prm = *prm;
   a.R = R; a.Rg = Rg; a.groups = (R + Rg - 1) / Rg;
   a.dmax = pr->max_dim; a.pmax = pr->max_features; a.TC = TC;
-  a.H = std::min(32, std::max(1, kSplitThreads / Rg));
+  a.mixed = prm->precision == ART_PRECISION_MIXED ? 1 : 0;
+  // default: four speculative Armijo steps per trial pass (adaptive step
+  // sizes are usually accepted within the first two; longer backtracks take
+  // further passes), spare threads share the rows instead
+  a.H = std::min(4, std::max(1, kSplitThreads / Rg));
   if (prm->trial_steps > 0) a.H = std::min(prm->trial_steps, std::max(1, kSplitThreads / Rg));
   a.H = std::min(a.H, prm->max_backtracks + 1);
   a.r_theta = (double*)(ws + wl.r_theta); a.r_loss = (double*)(ws + wl.r_loss);
@@ -1181,10 +1253,13 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
   split_plan_scatter<<<pg, 256, 0, s>>>(a);
   prof_end(s);
   count_launch(); count_launch(); count_launch();
-  // deepest row ring (2..kMaxStages chunks in flight) that fits shared memory
+  // longest chunk (fewer block barriers per row) with a ring of at least 4
+  // stages that fits shared memory, then the deepest ring for that chunk
+  a.CH = kMaxCH;
+  while (a.CH > 32 && split_layout(a.dmax, a.pmax, a.Rg, a.H, 4, a.CH).total > 200 * 1024) a.CH >>= 1;
   a.S = kMaxStages;
-  while (a.S > 2 && split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S).total > 227 * 1024) --a.S;
-  const size_t smem = split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S).total;
+  while (a.S > 1 && split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S, a.CH).total > 227 * 1024) --a.S;
+  const size_t smem = split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S, a.CH).total;
   if (smem > 227 * 1024) { set_error("art_split_level: shared memory %zu too large", smem); return ART_E_UNSUPPORTED; }
   auto launch = [&](auto kern) -> int {
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {

@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--systems", type=int, default=65536)
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
-    ap.add_argument("--cpu-per-class", type=int, default=48,
+    ap.add_argument("--cpu-per-class", type=int, default=384,
                     help="systems per feature class in the timed CPU sample")
     ap.add_argument("--fp64-factor", action="store_true",
                     help="mixed form factors the tensor-core Gram in FP64")
@@ -57,11 +57,16 @@ def parse():
                     help="systems per feature class in the per-node FP64 sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-legs", action="store_true", help="skip the split-search and hit-and-run legs")
+    ap.add_argument("--legs", default="split_level,hit_and_run,tree_build,serving",
+                    help="comma-separated legs to run after the headline")
     ap.add_argument("--split-nodes", type=int, default=4096)
     ap.add_argument("--har-chains", type=int, default=16384)
     ap.add_argument("--tree-builds", type=int, default=3)
     ap.add_argument("--serve-jobs", type=int, default=40)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the library's default launch shapes")
+    ap.add_argument("--autotune-per-class", type=int, default=1024,
+                    help="systems per feature class in the autotuner's sample")
     return ap.parse_args()
 
 
@@ -339,9 +344,11 @@ def _event_ms(fn, steps, warmup, stream):
 def leg_split(args, stream):
     """Batched soft oblique split search: 4096 nodes, d = 16, n log-uniform in
     [256, 16384], 16 restarts x 60 projected-gradient steps, affine child fits
-    (lambda = 1e-6), temperature annealed 0.2 -> 0.02; FP64 form."""
+    (lambda = 1e-6), temperature annealed 0.2 -> 0.02; the plain FP64 form
+    and the mixed form (single-precision gates, FP64 sums and solves)."""
 
     from art import _native as N
+    from art import autotune
     from art import workloads
     from art.models import AffineRidgeModel
     from art.splitters import SoftObliqueSplitter, split_level
@@ -349,28 +356,45 @@ def leg_split(args, stream):
     wl = workloads.split_nodes(args.split_nodes, device="cuda")
     sp = SoftObliqueSplitter(AffineRidgeModel(ridge=1e-6), 0.2, max_iters=60, grad_atol=0.0, grad_rtol=0.0,
                              min_side_points=8, min_side_fraction=0.0, n_restarts=16)
-
-    def step():
-        return split_level(sp, wl.x, wl.y, wl.row_offsets, wl.dims, wl.kinds, wl.temperature, wl.ridge,
-                           theta0=wl.theta0, anneal_ratio=0.1, hard_refit=True, max_dim=wl.d,
-                           max_features=wl.d + 1, stream=stream)
-
-    N.profile_reset()
-    N.profile_enable(True)
-    ms, res = _event_ms(step, 1, 1, stream)
-    N.profile_enable(False)
-    prof = N.profile_report()
+    # launch shape tuned on a separate 296-node level of the same distribution
+    tw = workloads.split_nodes(296, seed=33, device="cuda")
+    tuned = autotune.tune_split_shape(sp, tw.x, tw.y, tw.row_offsets, tw.dims, tw.kinds, tw.temperature, tw.ridge,
+                                      max_dim=tw.d, max_features=tw.d + 1, theta0=tw.theta0, anneal_ratio=0.1,
+                                      repeats=1, stream=stream) if not args.no_autotune else None
     units = wl.count * 16 * 60
     n = np.diff(wl.row_offsets).astype(float)
     d, p, H = wl.d, wl.d + 1, 4
     flops = float((n * (2 * d + p * (p + 1) + 8 * p + 2 * d + 12 + 6 * H)).sum()) * 16 * 60
-    top = max(prof.items(), key=lambda kv: kv[1][1])
-    return {"metric": "split restart-steps/s", "value": units / (ms / 1000.0), "unit": "restart-steps/s",
-            "ms_per_step": ms, "nodes": wl.count, "rows": wl.n_rows, "restarts": 16, "iterations": 60,
-            "precision": "fp64", "mean_iters_chosen": float(res.n_iters.double().mean().item()),
-            "failures": int((res.failure != 0).sum().item()),
-            "achieved_fp64_tflops": flops / (ms / 1000.0) / 1e12, "kernel": top[0],
-            "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()}}
+    out = {"metric": "split restart-steps/s", "unit": "restart-steps/s", "nodes": wl.count, "rows": wl.n_rows,
+           "restarts": 16, "iterations": 60, "autotune": tuned}
+    thetas = {}
+    for prec in ("fp64", "mixed"):
+        sp.precision = prec
+
+        def step():
+            return split_level(sp, wl.x, wl.y, wl.row_offsets, wl.dims, wl.kinds, wl.temperature, wl.ridge,
+                               theta0=wl.theta0, anneal_ratio=0.1, hard_refit=True, max_dim=wl.d,
+                               max_features=wl.d + 1, stream=stream)
+
+        N.profile_reset()
+        N.profile_enable(True)
+        ms, res = _event_ms(step, 1, 1, stream)
+        N.profile_enable(False)
+        prof = N.profile_report()
+        top = max(prof.items(), key=lambda kv: kv[1][1])
+        thetas[prec] = (res.loss.cpu().numpy(), res.n_right.cpu().numpy())
+        out[prec] = {"value": units / (ms / 1000.0), "ms_per_step": ms,
+                     "mean_iters_chosen": float(res.n_iters.double().mean().item()),
+                     "failures": int((res.failure != 0).sum().item()),
+                     "achieved_fp64_tflops": flops / (ms / 1000.0) / 1e12, "kernel": top[0],
+                     "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()}}
+    la, lb = thetas["fp64"][0], thetas["mixed"][0]
+    ok = np.isfinite(la) & np.isfinite(lb)
+    out["value"] = out["fp64"]["value"]
+    out["mixed_speedup"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    out["mixed_vs_fp64_hard_loss_rel_diff_median"] = float(np.median(np.abs(lb[ok] - la[ok]) / np.abs(la[ok])))
+    out["mixed_same_partition_fraction"] = float(np.mean(thetas["fp64"][1] == thetas["mixed"][1]))
+    return out
 
 
 def leg_har(args, stream):
@@ -529,6 +553,16 @@ def run_b200(args):
         ms = max_over_ranks(ms)
         return ms / args.steps, launches // args.steps, prof, out
 
+    # launch-shape choice of the mixed form, measured on a sample of this
+    # batch before any timed region (the solves below read the tuned value)
+    from art import autotune
+
+    tuned = None
+    if args.precision == "mixed" and not args.no_autotune:
+        tuned = autotune.tune_ridge_threshold(wl.x, wl.y, wl.w, ro, dims, kinds, ridge, x_offsets=xo,
+                                              max_dim=wl.max_dim, fp64_factor=args.fp64_factor,
+                                              per_class=args.autotune_per_class, stream=stream)
+
     # plain FP64 form, batched and per node (one call per system, the
     # comparison point of the >=5x target), then the headline form
     plain_ms, _, plain_prof, plain_out = timed("fp64")
@@ -563,7 +597,7 @@ def run_b200(args):
     elif "fp64<8>" in name:
         cls_idx = np.flatnonzero(p_all + 1 > 48) if args.precision == "fp64" else np.flatnonzero(info & N.INFO_FP64_RESOLVE)
     else:
-        cls_idx = np.flatnonzero(p_all >= 33)
+        cls_idx = np.flatnonzero(p_all >= (tuned["tensor_min_features"] if tuned else 33))
     flops, nbytes = algorithmic(wl, cls_idx)
     achieved_gbs = nbytes / (per_launch_ms / 1000.0) / 1e9
     roofline = {"bound": "hbm", "kernel": name, "achieved": achieved_gbs, "peak": hbm,
@@ -610,8 +644,11 @@ def run_b200(args):
 
     legs = {}
     if rank == 0 and not args.no_legs:
+        chosen = set(args.legs.split(","))
         for name, fn in (("split_level", leg_split), ("hit_and_run", leg_har), ("tree_build", leg_tree),
                          ("serving", leg_serving)):
+            if name not in chosen:
+                continue
             try:
                 legs[name] = fn(args, stream)
             except Exception as exc:  # a failing leg is reported, the headline stands
@@ -652,6 +689,7 @@ def run_b200(args):
         "fp64_resolve_fraction": float(np.mean((info & N.INFO_FP64_RESOLVE) != 0)),
         "mean_refine_passes_tensor_class": float(np.mean(((info >> N.INFO_REFINE_SHIFT) & 255)[p_all >= 33])),
         "fp64_factor": bool(args.fp64_factor),
+        "autotune": tuned,
         "variants": variants,
         "plain_kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in plain_prof.items()},
         "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()},

@@ -200,13 +200,14 @@ typedef struct ArtSplitParams {
   int32_t max_line_search_failures;
   double weight_floor;          /* soft fits                               */
   int32_t hard_refit;           /* bool: fit hard children + hard loss      */
-  int32_t precision;            /* ART_PRECISION_FP64 or _MIXED (FP32 core) */
+  int32_t precision;            /* ART_PRECISION_FP64, or _MIXED: sigmoid gates
+                                   in single precision, sums/solves FP64     */
   double anneal_ratio;          /* T_k = T * anneal_ratio^(k/(max_iters-1)); 1 = off */
   uint64_t seed;                /* Philox key for device initialisation     */
   int32_t group_restarts;       /* restarts sharing one CTA's row passes
                                    (0: the largest that fits, <= 16)         */
   int32_t trial_steps;          /* Armijo step sizes evaluated per trial pass
-                                   (0: min(32, 256 / group, backtracks + 1)) */
+                                   (0: min(4, 256 / group, backtracks + 1))  */
 } ArtSplitParams;
 
 typedef struct ArtSplitProblem {
