@@ -102,7 +102,7 @@ class ArtSplitProblem(C.Structure):
     _fields_ = [
         ("seg", ArtSegments), ("x", P), ("y", P), ("temperature", P), ("ridge", P),
         ("parent_loss", P), ("min_side_fallback", P), ("theta0", P), ("theta_stride", I64),
-        ("max_dim", I32), ("max_features", I32), ("node_keys", P),
+        ("max_dim", I32), ("max_features", I32), ("node_keys", P), ("min_side_points", P),
     ]
 
 

@@ -287,17 +287,17 @@ class ServingEngine:
                 st.leaves.append(nd)
             else:
                 split_idx.append(k)
-        # min_side_points and max_iters are per-call parameters of the split
-        # search: one call per distinct pair, so a node's split never depends
-        # on the jobs it is batched with
-        groups: dict[tuple, list[int]] = {}
+        # max_iters is a per-call parameter of the split search (one call per
+        # distinct value); the minimum side count goes per node, so nodes of
+        # every dimension share a launch.  A node's split never depends on the
+        # jobs it is batched with.
+        groups: dict[int, list[int]] = {}
         for k in split_idx:
-            st = work[k][0]
-            groups.setdefault((st.min_side, st.job.max_iters), []).append(k)
-        for (min_side, iters), ks in sorted(groups.items()):
-            self._split([work[k] for k in ks], x, y, ro, xo, d, kinds, ks, min_side, iters)
+            groups.setdefault(work[k][0].job.max_iters, []).append(k)
+        for iters, ks in sorted(groups.items()):
+            self._split([work[k] for k in ks], x, y, ro, xo, d, kinds, ks, iters)
 
-    def _split(self, sub, x, y, ro, xo, d, kinds, idx, min_side, iters) -> None:
+    def _split(self, sub, x, y, ro, xo, d, kinds, idx, iters) -> None:
         t = torch()
         dev = x.device
         # the split nodes' rows, gathered from the fit batch
@@ -310,11 +310,13 @@ class ServingEngine:
         keys = np.array([_key(st.job.seed, "split", nd.path) for st, nd in sub], dtype=np.uint64)
         temps = np.array([st.job.temperature for st, _ in sub])
         ridge = np.array([st.job.ridge for st, _ in sub])
+        min_side = np.array([st.min_side for st, _ in sub], dtype=np.int32)
         sp = SoftObliqueSplitter(AffineRidgeModel(ridge=1e-6), 1.0, max_iters=iters, grad_atol=1e-8,
-                                 grad_rtol=1e-5, min_side_points=min_side, min_side_fraction=0.0, n_restarts=1)
+                                 grad_rtol=1e-5, min_side_points=int(min_side.min()), min_side_fraction=0.0,
+                                 n_restarts=1)
         res = split_level(sp, xs, ys, sro, dd, kinds[idx], temps, ridge, x_offsets=sxo, hard_refit=False,
                           node_keys=keys, max_dim=int(dd.max()), max_features=int(max(st.job.n_features for st, _ in sub)),
-                          stream=self.stream)
+                          min_side_points=min_side, group_restarts=0, trial_steps=0, stream=self.stream)
         failure = res.failure.cpu().numpy()
         theta = res.theta
         ok = failure == 0

@@ -181,7 +181,8 @@ def split_level(splitter: "SoftObliqueSplitter", x, y, row_offsets, dims, featur
                 hard_refit: bool = True, anneal_ratio: float = 1.0, seed: int = 0, traces: bool = False,
                 max_dim: int | None = None, max_features: int | None = None, node_keys=None,
                 group_restarts: int | None = None, trial_steps: int | None = None,
-                out: LevelResult | None = None, workspace=None, stream=None) -> LevelResult:
+                min_side_points=None, out: LevelResult | None = None, workspace=None,
+                stream=None) -> LevelResult:
     """Split K nodes in one launch sequence; arrays are numpy or torch (moved to the device).
 
     theta0, when given, is (K, R, d_max + 1); otherwise restarts start from
@@ -191,6 +192,8 @@ def split_level(splitter: "SoftObliqueSplitter", x, y, row_offsets, dims, featur
     ``group_restarts`` / ``trial_steps`` fix the kernel's launch shape
     (restarts per CTA, Armijo steps per trial pass); None takes the
     autotuned choice for (d, p, R) on this device, else the library's.
+    ``min_side_points`` (K ints) overrides the splitter's minimum side count
+    per node, so nodes with different limits share one launch.
     ``out`` (a LevelResult of K rows) and ``workspace`` (a uint8 device
     tensor of at least ``art_split_workspace_size`` bytes) make the call
     allocate nothing, as a captured graph needs.
@@ -236,8 +239,12 @@ def split_level(splitter: "SoftObliqueSplitter", x, y, row_offsets, dims, featur
         nk = to_device(np.asarray(node_keys, dtype=np.uint64).view(np.int64) if not isinstance(node_keys, t.Tensor)
                        else node_keys, t.int64, dev)
     seg = N.ArtSegments(K, ptr(ro), ptr(xo), ptr(dims_t), ptr(feats))
+    ms = None
+    if min_side_points is not None:
+        ms = to_device(np.asarray(min_side_points, dtype=np.int32).reshape(K) if not isinstance(min_side_points, t.Tensor)
+                       else min_side_points, t.int32, dev)
     prob = N.ArtSplitProblem(seg, ptr(x), ptr(y), ptr(temp), ptr(rid), ptr(pl), ptr(fb), ptr(th0), stride,
-                             int(max_dim), int(max_features), ptr(nk))
+                             int(max_dim), int(max_features), ptr(nk), ptr(ms))
     if group_restarts is None or trial_steps is None:
         from . import autotune
 
@@ -256,7 +263,7 @@ def split_level(splitter: "SoftObliqueSplitter", x, y, row_offsets, dims, featur
         raise ValueError(f"split workspace of {ws.numel()} bytes < {nbytes} required")
     N.check(lib.art_split_level(C.byref(prob), C.byref(prm), C.byref(res), ptr(ws), ws.numel(),
                                 stream_handle(stream)), "art_split_level")
-    out._keepalive = (x, y, ro, xo, dims_t, feats, temp, rid, pl, fb, th0, nk)
+    out._keepalive = (x, y, ro, xo, dims_t, feats, temp, rid, pl, fb, th0, nk, ms)
     return out
 
 

@@ -41,6 +41,16 @@ constexpr int kRedSlots = 5;     // (restart, component) accumulators per thread
 constexpr int kBuckets = 64;
 constexpr int kMaxStages = 8;    // row-stage ring depth (chunks in flight)
 constexpr int kErrSlot = 2 + 2 * kBuckets;  // counts[kErrSlot]: a bounded wait gave up
+// Gangs: with at most two restarts per node, a node of n rows is split by
+// min(kGangMax, ceil(n / kGangRows)) CTAs that take interleaved chunks and
+// add their pass sums in rank order through global scratch.  The gang size
+// depends on n alone, so a node's result never depends on its batch.
+constexpr int kGangRows = 65536;
+constexpr int kGangMax = 16;
+// A gang forms when its last member is popped, which can wait for other
+// work items to finish: that wait is bounded by a longer limit than the
+// in-pass barriers (members then run side by side).
+constexpr uint64_t kGangFormNs = 60ull * 1000000000ull;
 
 struct SplitArgs {
   int64_t K;
@@ -57,6 +67,7 @@ struct SplitArgs {
   const double* theta0;
   int64_t theta0_stride;
   const uint64_t* node_keys;
+  const int32_t* min_side;  // per-node minimum side count or NULL
   ArtSplitParams prm;
   int R, Rg, groups, dmax, pmax, H, TC, S, CH;
   int mixed;  // ART_PRECISION_MIXED: gates in single precision
@@ -78,15 +89,19 @@ struct SplitArgs {
   int32_t* tr_back;
   double* tr_gnorm;
   // work queue
-  int32_t* counts;   // [0] items, [1] cursor, [2..2+64) hist, [66..130) start
-  int32_t* items;    // [K * groups]
+  int32_t* counts;   // [0] entries, [1] cursor, [2..2+64) hist, [66..130) start
+  int4* items;       // queue entries (item, gang rank, gang size, 0)
+  int gang_on, nslots, gang_P;  // gangs enabled; scratch slots; doubles per rank partial
+  int4* gang_rec;    // [K * groups]: slot + 1, barrier arrivals, members done, abort
+  int32_t* slot_flags;  // [nslots]
+  double* gang_scratch; // [nslots][2][kGangMax][gang_P]
 };
 
 // Shared-memory layout for a given (dmax, pmax, Rg, H, S, CH): `ring` holds S
 // stages of CH rows of x and y (bulk copies in flight), `bars` their
 // mbarriers.
 struct SLayout {
-  size_t ring, rx, rstage, bars, phi, q, G, cache, theta, dirn, grad, lastf, bl, br, trial, red, chol, eidx, rs,
+  size_t ring, rx, rstage, bars, xp, phi, q, G, cache, theta, dirn, grad, lastf, bl, br, trial, red, chol, eidx, rs,
       total;
 };
 __host__ __device__ inline size_t al(size_t v) { return (v + 15) & ~(size_t)15; }
@@ -98,10 +113,13 @@ __host__ __device__ inline SLayout split_layout(int dmax, int pmax, int Rg, int 
   L.rstage = L.rx + al((size_t)CH * 8 + 32);
   L.ring = o; o = al(o + (size_t)S * L.rstage);
   L.bars = o; o = al(o + (size_t)kMaxStages * 8);
-  L.phi = o; o = al(o + (size_t)CH * pa * 8);
-  L.q = o; o = al(o + (size_t)CH * 2 * Rg * 8);
+  // row-indexed arrays use odd row strides (in doubles), so that lanes
+  // reading different rows of a chunk fall in different banks
+  L.xp = o; o = al(o + (size_t)CH * (dmax | 1) * 8);
+  L.phi = o; o = al(o + (size_t)CH * (pa | 1) * 8);
+  L.q = o; o = al(o + (size_t)CH * (2 * Rg + 1) * 8);
   L.G = o; o = al(o + (size_t)E * 2 * Rg * 8);
-  L.cache = o; o = al(o + (size_t)CH * Rg * 4 * 8);
+  L.cache = o; o = al(o + (size_t)CH * (4 * Rg + 4) * 8);
   L.theta = o; o = al(o + (size_t)Rg * dt * 8);
   L.dirn = o; o = al(o + (size_t)Rg * dt * 8);
   L.grad = o; o = al(o + (size_t)Rg * dt * 8);
@@ -122,7 +140,7 @@ enum RS {
   RS_LOSS = 0, RS_DD, RS_TOL, RS_GNORM, RS_T, RS_ALPHA, RS_ASTART, RS_STEP, RS_LSVAL,
   RS_LAML, RS_LAMR, RS_NRIGHT, RS_ACTIVE, RS_ITERS, RS_STOP, RS_FAIL, RS_FAILURES, RS_NBBASE,
   RS_SEARCH, RS_ACCEPT, RS_NB, RS_FEASIT, RS_HASFEAS, RS_CONV, RS_FB, RS_CHOLBAD, RS_HLOSSL,
-  RS_HLOSSR, RS_PARENT, RS_COUNT_
+  RS_HLOSSR, RS_PARENT, RS_INVT, RS_COUNT_
 };
 
 // Row groups for a pass: the largest power of two <= 32 such that `items`
@@ -170,13 +188,17 @@ __device__ __forceinline__ void entry_ij(int e, int& i, int& j) {
 }
 
 // =========================================================== plan (LPT order)
+__device__ __forceinline__ int gang_size(const SplitArgs& a, int64_t n) {
+  if (!a.gang_on) return 1;
+  return (int)min((int64_t)kGangMax, max((int64_t)1, (n + kGangRows - 1) / kGangRows));
+}
 __global__ void split_plan_hist(SplitArgs a) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= a.K * a.groups) return;
   const int64_t k = t / a.groups;
   const int64_t n = a.row_offsets[k + 1] - a.row_offsets[k];
   const int b = kBuckets - 1 - max(0, min(kBuckets - 1, ilogb((double)(n + 1))));
-  atomicAdd(&a.counts[2 + b], 1);
+  atomicAdd(&a.counts[2 + b], gang_size(a, n));
 }
 __global__ void split_plan_scan(SplitArgs a) {
   if (threadIdx.x != 0) return;
@@ -194,8 +216,11 @@ __global__ void split_plan_scatter(SplitArgs a) {
   const int64_t k = t / a.groups;
   const int64_t n = a.row_offsets[k + 1] - a.row_offsets[k];
   const int b = kBuckets - 1 - max(0, min(kBuckets - 1, ilogb((double)(n + 1))));
-  const int slot = atomicSub(&a.counts[2 + b], 1) - 1;
-  a.items[a.counts[2 + kBuckets + b] + slot] = (int32_t)t;
+  const int G = gang_size(a, n);
+  // a gang's members take consecutive entries, so they are popped together
+  const int slot = atomicSub(&a.counts[2 + b], G) - G;
+  const int base = a.counts[2 + kBuckets + b] + slot;
+  for (int r = 0; r < G; ++r) a.items[base + r] = make_int4((int)t, r, G, 0);
 }
 
 // ================================================================ kernel
@@ -209,8 +234,12 @@ struct SplitCta {
   uint64_t* rbar;
   uint32_t rpar = 0, rbusy = 0;  // per-stage wait parity / copy in flight (uniform)
   bool rabort = false;
+  // gang of this item: member rank, size, scratch slot, reductions so far
+  int grank = 0, gsize = 1, gslot = -1, gpass = 0;
+  int64_t gitem = 0;
   const double *xs, *ys;
-  double *phi, *Q, *G, *cache, *th, *dn, *gr, *lf, *bl, *br, *trial, *red, *chol, *rs;
+  double *xp, *phi, *Q, *G, *cache, *th, *dn, *gr, *lf, *bl, *br, *trial, *red, *chol, *rs;
+  int xps, phs, qs;  // padded row strides of xp, phi, Q (odd, in doubles)
   int16_t* eidx;
   int tid, lane, warp;
 
@@ -218,6 +247,8 @@ struct SplitCta {
     L = split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S, a.CH);
     rbar = (uint64_t*)(sm + L.bars);
     xs = (const double*)(sm + L.ring); ys = xs; phi = (double*)(sm + L.phi);
+    xp = (double*)(sm + L.xp);
+    qs = 2 * a.Rg + 1;
     Q = (double*)(sm + L.q); G = (double*)(sm + L.G); cache = (double*)(sm + L.cache);
     th = (double*)(sm + L.theta); dn = (double*)(sm + L.dirn); gr = (double*)(sm + L.grad);
     lf = (double*)(sm + L.lastf); bl = (double*)(sm + L.bl); br = (double*)(sm + L.br);
@@ -234,8 +265,7 @@ struct SplitCta {
   // chunks and refills a stage as soon as the pass is done with it, so
   // copies run S chunks ahead of the arithmetic.  Control flow is uniform:
   // every thread tracks the same parity/in-flight bits; thread 0 issues.
-  __device__ void ring_issue(int64_t ci) {
-    const int st = (int)(ci % a.S);
+  __device__ void ring_issue(int64_t ci, int st) {
     if (tid == 0) {
       const int64_t c0 = ci * a.CH;
       const int rows = (int)min((int64_t)a.CH, it.n - c0);
@@ -248,9 +278,15 @@ struct SplitCta {
     }
     rbusy |= 1u << st;
   }
+  // A gang member takes chunks grank, grank + gsize, ...; its j-th chunk
+  // goes to stage j % S.
   __device__ void begin_pass() {
     if (rabort) return;
-    for (int st = 0; st < a.S && (int64_t)st * a.CH < it.n; ++st) ring_issue(st);
+    for (int j = 0; j < a.S; ++j) {
+      const int64_t ci = grank + (int64_t)j * gsize;
+      if (ci * a.CH >= it.n) break;
+      ring_issue(ci, j);
+    }
   }
   // bounded waits for copies still in flight (only after a wait gave up)
   __device__ void ring_drain() {
@@ -262,15 +298,64 @@ struct SplitCta {
       }
   }
 
+  // Gang sum of arr[0..len): every member publishes its partial, waits for
+  // the others (bounded) and adds all partials in rank order, so every
+  // member holds the same total.  Partials alternate between two buffers;
+  // a member can only reuse one after passing the next barrier, which the
+  // others reach only after reading it.
+  __device__ void gang_reduce(double* arr, int len) {
+    if (gsize == 1) return;
+    __shared__ int s_gok;
+    int4* rec = a.gang_rec + gitem;
+    const int buf = gpass & 1;
+    ++gpass;
+    double* base = a.gang_scratch + (size_t)(gslot * 2 + buf) * kGangMax * a.gang_P;
+    for (int i = tid; i < len; i += kSplitThreads) __stcg(base + (size_t)grank * a.gang_P + i, arr[i]);
+    __threadfence();  // each writer's partial is visible device-wide before the arrival
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      atomicAdd(&rec->y, 1);
+      const int target = gpass * gsize;
+      const uint64_t t0 = globaltimer_ns();
+      int ok = 1;
+      for (uint32_t spin = 0;; ++spin) {
+        if (atomicAdd(&rec->y, 0) >= target) break;
+        if (atomicAdd(&rec->w, 0) != 0 || ((spin & 63u) == 63u && globaltimer_ns() - t0 > kWaitNs)) {
+          ok = 0;
+          break;
+        }
+      }
+      if (!ok) {
+        atomicExch(&rec->w, 1);
+        atomicExch(&a.counts[kErrSlot], 1);
+      }
+      __threadfence();
+      s_gok = ok;
+    }
+    __syncthreads();
+    if (!s_gok) rabort = true;
+    for (int i = tid; i < len; i += kSplitThreads) {
+      double v = 0.0;
+      for (int r = 0; r < gsize; ++r) v += __ldcg(base + (size_t)r * a.gang_P + i);
+      arr[i] = v;
+    }
+    __syncthreads();
+  }
+
   // Rows [c0, c0 + rows) of x and y from the ring, then the augmented
   // features.  The caller's loop ends every chunk with __syncthreads().
   __device__ int load_chunk(int64_t c0) {
     const int rows = (int)min((int64_t)a.CH, it.n - c0);
     const int d = it.d;
     const int64_t ci = c0 / a.CH;
-    const int st = (int)(ci % a.S);
+    const int64_t jj = (ci - grank) / gsize;
+    const int st = (int)(jj % a.S);
     if (!rabort) {
-      if (ci >= 1 && (ci - 1 + a.S) * a.CH < it.n) ring_issue(ci - 1 + a.S);
+      if (jj >= 1) {
+        const int64_t cn = grank + (jj - 1 + a.S) * gsize;
+        if (cn * a.CH < it.n) ring_issue(cn, (int)((jj - 1) % a.S));
+      }
       const bool ok = mbar_wait(&rbar[st], (rpar >> st) & 1u);
       if (ok) {
         rpar ^= 1u << st;
@@ -285,6 +370,10 @@ struct SplitCta {
     xs = (const double*)(base + (((uintptr_t)(a.x + it.xoff + c0 * d)) & 15));
     ys = (const double*)(base + L.rx + (((uintptr_t)(a.y + it.r0 + c0)) & 15));
     const int pa = it.pa;
+    for (int e = tid; e < rows * d; e += kSplitThreads) {
+      const int r = e / d, i = e - r * d;
+      xp[r * xps + i] = xs[e];
+    }
     for (int e = tid; e < rows * pa; e += kSplitThreads) {
       const int r = e / pa, f = e - r * pa;
       double v;
@@ -295,24 +384,34 @@ struct SplitCta {
         const double* xr = xs + r * d;
         v = (ia < 0 ? 1.0 : xr[ia]) * (ib < 0 ? 1.0 : xr[ib]);
       }
-      phi[r * pa + f] = v;
+      phi[r * phs + f] = v;
     }
     __syncthreads();
     return rows;
   }
 
   __device__ double score(int r, int row) {  // x . w_r
-    const double* xr = xs + row * it.d;
+    const double* xr = xp + row * xps;
     const double* w = th + r * dt();
-    double u = 0.0;
-    for (int i = 0; i < it.d; ++i) u = fma(xr[i], w[i], u);
-    return u;
+    double u0 = 0.0, u1 = 0.0;
+    int i = 0;
+    for (; i + 1 < it.d; i += 2) {
+      u0 = fma(xr[i], w[i], u0);
+      u1 = fma(xr[i + 1], w[i + 1], u1);
+    }
+    if (i < it.d) u0 = fma(xr[i], w[i], u0);
+    return u0 + u1;
   }
   __device__ double fitted(const double* beta, int row) {
-    const double* pr = phi + row * it.pa;
-    double s = 0.0;
-    for (int f = 0; f < it.p; ++f) s = fma(pr[f], beta[f], s);
-    return s;
+    const double* pr = phi + row * phs;
+    double s0 = 0.0, s1 = 0.0;
+    int f = 0;
+    for (; f + 1 < it.p; f += 2) {
+      s0 = fma(pr[f], beta[f], s0);
+      s1 = fma(pr[f + 1], beta[f + 1], s1);
+    }
+    if (f < it.p) s0 = fma(pr[f], beta[f], s0);
+    return s0 + s1;
   }
 
   // ---- Gram pass: G[e][c] = sum_k Q[k][c] P[k][e]; hard = gates from the
@@ -342,7 +441,7 @@ struct SplitCta {
 #pragma unroll
       for (int v = 0; v < TC; ++v) acc[u][v] = 0.0;
     begin_pass();
-    for (int64_t c0 = 0; c0 < it.n; c0 += a.CH) {
+    for (int64_t c0 = (int64_t)grank * a.CH; c0 < it.n; c0 += (int64_t)gsize * a.CH) {
       const int rows = load_chunk(c0);
       for (int pr = tid; pr < rows * a.Rg; pr += kSplitThreads) {
         const int row = pr / a.Rg, r = pr - row * a.Rg;
@@ -350,25 +449,25 @@ struct SplitCta {
         if (r < it.rn && S(r, RS_ACTIVE) != 0.0) {
           if (hard) {
             const double* w = th + r * dt();
-            const bool right = dot2_score(xs + row * it.d, w, it.d, w[it.d]) >= 0.0;
+            const bool right = dot2_score(xp + row * xps, w, it.d, w[it.d]) >= 0.0;
             qL = right ? 0.0 : 1.0;
             qR = right ? 1.0 : 0.0;
             // integer-valued sums below 2^53 are exact in any order
             if (right) atomicAdd(&S(r, RS_NRIGHT), 1.0);
           } else {
-            const double pi = gate((score(r, row) - th[r * dt() + it.d]) / S(r, RS_T));
+            const double pi = gate((score(r, row) - th[r * dt() + it.d]) * S(r, RS_INVT));
             qL = fmax(1.0 - pi, a.prm.weight_floor);
             qR = fmax(pi, a.prm.weight_floor);
           }
         }
-        Q[row * C2 + 2 * r] = qL;
-        Q[row * C2 + 2 * r + 1] = qR;
+        Q[row * qs + 2 * r] = qL;
+        Q[row * qs + 2 * r + 1] = qR;
       }
       __syncthreads();
       if (mine) {
         for (int row = grp; row < rows; row += RG) {
-          const double* pr = phi + row * it.pa;
-          const double* qr = Q + row * C2 + ct * TC;
+          const double* pr = phi + row * phs;
+          const double* qr = Q + row * qs + ct * TC;
           double pv[TE], qv[TC];
 #pragma unroll
           for (int u = 0; u < TE; ++u) pv[u] = pr[ei[u]] * pr[ej[u]];
@@ -396,6 +495,16 @@ struct SplitCta {
         }
     }
     __syncthreads();
+    if (gsize > 1) {
+      gang_reduce(G, E * C2);
+      if (hard) {  // right-side counts (integers: exact in any order)
+        if (tid < a.Rg) red[tid] = S(tid, RS_NRIGHT);
+        __syncthreads();
+        gang_reduce(red, a.Rg);
+        if (tid < a.Rg) S(tid, RS_NRIGHT) = red[tid];
+        __syncthreads();
+      }
+    }
   }
 
   // ---- trace-scaled ridge + Cholesky + solve for every (restart, side).
@@ -463,28 +572,30 @@ struct SplitCta {
     double accs[kRedSlots];
 #pragma unroll
     for (int s = 0; s < kRedSlots; ++s) accs[s] = 0.0;
+    const int cst = a.Rg + 1;                  // padded row stride
+    const double inv_n = 1.0 / (double)it.n;
     double* coef = cache;                      // [row][r]: a_k
-    double* wl = cache + a.CH * a.Rg;          // [row][r]: weighted loss term
-    double* nr = cache + 2 * a.CH * a.Rg;      // [row][r]: pi >= 0.5
+    double* wl = cache + a.CH * cst;           // [row][r]: weighted loss term
+    double* nr = cache + 2 * a.CH * cst;       // [row][r]: pi >= 0.5
     begin_pass();
-    for (int64_t c0 = 0; c0 < it.n; c0 += a.CH) {
+    for (int64_t c0 = (int64_t)grank * a.CH; c0 < it.n; c0 += (int64_t)gsize * a.CH) {
       const int rows = load_chunk(c0);
       for (int pr = tid; pr < rows * a.Rg; pr += kSplitThreads) {
         const int row = pr / a.Rg, r = pr - row * a.Rg;
         double cf = 0.0, lw = 0.0, ge = 0.0;
         if (r < it.rn && S(r, RS_ACTIVE) != 0.0) {
-          const double pi = gate((score(r, row) - th[r * dt() + d]) / S(r, RS_T));
+          const double pi = gate((score(r, row) - th[r * dt() + d]) * S(r, RS_INVT));
           const double yv = ys[row];
           const double eL = yv - fitted(bl + r * a.pmax, row);
           const double eR = yv - fitted(br + r * a.pmax, row);
           const double eL2 = eL * eL, eR2 = eR * eR;
           lw = (1.0 - pi) * eL2 + pi * eR2;
-          cf = (eR2 - eL2) * pi * (1.0 - pi) / (double)it.n;
+          cf = (eR2 - eL2) * pi * (1.0 - pi) * inv_n;
           ge = pi >= 0.5 ? 1.0 : 0.0;
         }
-        coef[row * a.Rg + r] = cf;
-        wl[row * a.Rg + r] = lw;
-        nr[row * a.Rg + r] = ge;
+        coef[row * cst + r] = cf;
+        wl[row * cst + r] = lw;
+        nr[row * cst + r] = ge;
       }
       __syncthreads();
       if (RGr > 1) {
@@ -492,11 +603,11 @@ struct SplitCta {
           const int r = gq / comps, cp = gq - r * comps;
           double acc = accs[0];
           for (int row = ggrp; row < rows; row += RGr) {
-            const double cv = coef[row * a.Rg + r];
-            if (cp < d) acc = fma(cv, xs[row * d + cp], acc);
+            const double cv = coef[row * cst + r];
+            if (cp < d) acc = fma(cv, xp[row * xps + cp], acc);
             else if (cp == d) acc += cv;
-            else if (cp == d + 1) acc += wl[row * a.Rg + r];
-            else acc += nr[row * a.Rg + r];
+            else if (cp == d + 1) acc += wl[row * cst + r];
+            else acc += nr[row * cst + r];
           }
           accs[0] = acc;
         }
@@ -508,11 +619,11 @@ struct SplitCta {
           const int r = q / comps, cp = q - r * comps;
           double acc = accs[s];
           for (int row = 0; row < rows; ++row) {
-            const double cv = coef[row * a.Rg + r];
-            if (cp < d) acc = fma(cv, xs[row * d + cp], acc);
+            const double cv = coef[row * cst + r];
+            if (cp < d) acc = fma(cv, xp[row * xps + cp], acc);
             else if (cp == d) acc += cv;
-            else if (cp == d + 1) acc += wl[row * a.Rg + r];
-            else acc += nr[row * a.Rg + r];
+            else if (cp == d + 1) acc += wl[row * cst + r];
+            else acc += nr[row * cst + r];
           }
           accs[s] = acc;
         }
@@ -532,6 +643,7 @@ struct SplitCta {
       }
       __syncthreads();
     }
+    gang_reduce(red, pairs);
     // finalize per restart (one thread each)
     if (tid < it.rn && S(tid, RS_ACTIVE) != 0.0) {
       const int r = tid;
@@ -577,26 +689,35 @@ struct SplitCta {
     const int r = item / H, j = item - (item / H) * H;
     double f = 0.0;
     const bool on = mine && r < it.rn && S(r, RS_SEARCH) != 0.0;
-    double alpha = 0.0, nrm = 1.0, z = 0.0, pz = 0.0, T = 1.0;
+    double alpha = 0.0, inv_nrm = 1.0, z = 0.0, pz = 0.0, inv_t = 1.0;
     if (on) {
       alpha = tal[r * H + j];
-      nrm = tnr[r * H + j];
+      inv_nrm = 1.0 / tnr[r * H + j];
       z = th[r * dt() + d];
       pz = dn[r * dt() + d];
-      T = S(r, RS_T);
+      inv_t = S(r, RS_INVT);
     }
     begin_pass();
-    for (int64_t c0 = 0; c0 < it.n; c0 += a.CH) {
+    for (int64_t c0 = (int64_t)grank * a.CH; c0 < it.n; c0 += (int64_t)gsize * a.CH) {
       const int rows = load_chunk(c0);
       for (int pr = tid; pr < rows * a.Rg; pr += kSplitThreads) {
         const int row = pr / a.Rg, rr = pr - row * a.Rg;
-        double* cp = cache + (row * a.Rg + rr) * 4;
+        double* cp = cache + row * (4 * a.Rg + 1) + rr * 4;
         if (rr < it.rn && S(rr, RS_SEARCH) != 0.0) {
-          const double* xr = xs + row * d;
+          const double* xr = xp + row * xps;
           const double* w = th + rr * dt();
           const double* pw = dn + rr * dt();
-          double u = 0.0, v = 0.0;
-          for (int i = 0; i < d; ++i) { u = fma(xr[i], w[i], u); v = fma(xr[i], pw[i], v); }
+          double u = 0.0, v = 0.0, u1 = 0.0, v1 = 0.0;
+          int i = 0;
+          for (; i + 1 < d; i += 2) {
+            u = fma(xr[i], w[i], u);
+            v = fma(xr[i], pw[i], v);
+            u1 = fma(xr[i + 1], w[i + 1], u1);
+            v1 = fma(xr[i + 1], pw[i + 1], v1);
+          }
+          if (i < d) { u = fma(xr[i], w[i], u); v = fma(xr[i], pw[i], v); }
+          u += u1;
+          v += v1;
           const double yv = ys[row];
           const double eL = yv - fitted(bl + rr * a.pmax, row);
           const double eR = yv - fitted(br + rr * a.pmax, row);
@@ -606,8 +727,8 @@ struct SplitCta {
       __syncthreads();
       if (on) {
         for (int row = grp; row < rows; row += RG) {
-          const double* cp = cache + (row * a.Rg + r) * 4;
-          const double s = ((cp[0] + alpha * cp[1]) / nrm - (z + alpha * pz)) / T;
+          const double* cp = cache + row * (4 * a.Rg + 1) + r * 4;
+          const double s = ((cp[0] + alpha * cp[1]) * inv_nrm - (z + alpha * pz)) * inv_t;
           const double pi = gate(s);
           f += (1.0 - pi) * cp[2] + pi * cp[3];
         }
@@ -615,23 +736,108 @@ struct SplitCta {
       __syncthreads();
     }
     f = group_sum(f, RG);
-    if (on && grp == 0) tf[r * H + j] = f / (double)it.n;
+    if (on && grp == 0) tf[r * H + j] = f;
+    __syncthreads();
+    gang_reduce(tf, a.Rg * H);
+    if (on && grp == 0) tf[r * H + j] = tf[r * H + j] / (double)it.n;
     __syncthreads();
   }
 
   __device__ void record_trace(int r, int iter) {
     const int64_t kr = (int64_t)it.k * a.R + it.rbase + r;
     const int M = a.prm.max_iters;
+    if (grank != 0) return;
     if (a.tr_loss) a.tr_loss[kr * (M + 1) + iter] = S(r, RS_LOSS);
     if (a.tr_gnorm) a.tr_gnorm[kr * (M + 1) + iter] = S(r, RS_GNORM);
   }
 
-  __device__ void run(int item_id);
+  __device__ void run(int item_id, int rank, int members);
+  __device__ bool gang_begin(int item_id, int rank, int members);
+  __device__ void gang_end();
 };
 
 template <int TC>
-__device__ void SplitCta<TC>::run(int item_id) {
+__device__ bool SplitCta<TC>::gang_begin(int item_id, int rank, int members) {
+  // rank 0 takes a free scratch slot and publishes it; the other members
+  // wait (bounded) for it.  At most one gang is being popped at a time and
+  // every other active gang holds >= 2 CTAs, so the slots (one per SM plus
+  // two) never run out.
+  __shared__ int s_slot;
+  grank = rank;
+  gsize = members;
+  gitem = item_id;
+  gpass = 0;
+  if (members == 1) return true;
+  int4* rec = a.gang_rec + item_id;
+  if (tid == 0) {
+    int slot = -1;
+    const uint64_t t0 = globaltimer_ns();
+    if (rank == 0) {
+      for (uint32_t spin = 0; slot < 0; ++spin) {
+        for (int q = 0; q < a.nslots && slot < 0; ++q)
+          if (atomicCAS(&a.slot_flags[q], 0, 1) == 0) slot = q;
+        if (slot < 0 && (spin & 63u) == 63u && globaltimer_ns() - t0 > kWaitNs) break;
+      }
+      if (slot >= 0) {
+        __threadfence();
+        atomicExch(&rec->x, slot + 1);
+      }
+    } else {
+      for (uint32_t spin = 0;; ++spin) {
+        const int v = atomicAdd(&rec->x, 0);
+        if (v > 0) { slot = v - 1; break; }
+        if ((spin & 63u) == 63u && globaltimer_ns() - t0 > kWaitNs) break;
+      }
+      __threadfence();
+    }
+    // formation: every member arrives once, then waits for all of them
+    if (slot >= 0) {
+      atomicAdd(&rec->y, 1);
+      const uint64_t t1 = globaltimer_ns();
+      for (uint32_t spin = 0;; ++spin) {
+        if (atomicAdd(&rec->y, 0) >= members) break;
+        if (atomicAdd(&rec->w, 0) != 0 ||
+            ((spin & 63u) == 63u && globaltimer_ns() - t1 > kGangFormNs)) {
+          slot = -1;
+          break;
+        }
+      }
+      __threadfence();
+    }
+    if (slot < 0) {
+      atomicExch(&rec->w, 1);
+      atomicExch(&a.counts[kErrSlot], 1);
+    }
+    s_slot = slot;
+  }
+  __syncthreads();
+  gslot = s_slot;
+  gpass = 1;  // the formation counted as the first barrier
+  __syncthreads();
+  return gslot >= 0;
+}
+
+template <int TC>
+__device__ void SplitCta<TC>::gang_end() {
+  if (gsize == 1) return;
+  __syncthreads();
+  if (tid == 0 && gslot >= 0) {
+    __threadfence();
+    int4* rec = a.gang_rec + gitem;
+    if (atomicAdd(&rec->z, 1) == gsize - 1) atomicExch(&a.slot_flags[gslot], 0);
+  }
+  gsize = 1;
+  grank = 0;
+  gslot = -1;
+}
+
+template <int TC>
+__device__ void SplitCta<TC>::run(int item_id, int rank, int members) {
   const ArtSplitParams& P = a.prm;
+  if (!gang_begin(item_id, rank, members)) {  // no slot: the level is reported lost
+    gang_end();
+    return;
+  }
   // ---------------------------------------------------------------- setup
   const int k = item_id / a.groups, g = item_id - (item_id / a.groups) * a.groups;
   it.k = k;
@@ -643,13 +849,16 @@ __device__ void SplitCta<TC>::run(int item_id) {
   it.kind = a.features[k];
   it.p = feature_count(it.d, it.kind);
   it.pa = it.p + 1;
+  xps = it.d | 1;
+  phs = it.pa | 1;
   it.E = it.pa * (it.pa + 1) / 2;
   it.T0 = a.temperature[k];
   it.ridge = a.ridge[k];
   it.rbase = g * a.Rg;
   it.rn = min(a.Rg, a.R - it.rbase);
   const int d = it.d, n = (int)it.n;
-  const int req = max(P.min_side_points, (int)ceil(P.min_side_fraction * (double)n));
+  const int req = max(a.min_side ? max(1, a.min_side[k]) : P.min_side_points,
+                      (int)ceil(P.min_side_fraction * (double)n));
   const bool fb_allowed = a.fallback ? a.fallback[k] != 0 : false;
   for (int e = tid; e < it.E; e += kSplitThreads) {
     int i, j;
@@ -676,6 +885,7 @@ __device__ void SplitCta<TC>::run(int item_id) {
     for (int i = 0; i < d; ++i) t[i] = t0[i] / nrm;
     t[d] = t0[d];
     S(r, RS_T) = it.T0;
+    S(r, RS_INVT) = 1.0 / it.T0;
     S(r, RS_ALPHA) = fmin(fmax(P.alpha0, P.alpha_min), P.alpha_max);
     S(r, RS_STOP) = ART_STOP_MAX_ITERS;
     S(r, RS_FEASIT) = -1.0;
@@ -847,11 +1057,14 @@ __device__ void SplitCta<TC>::run(int item_id) {
       for (int i = 0; i < d; ++i) t[i] = t[i] / nrm;
       t[d] = t[d] + al * pd[d];
       if (P.anneal_ratio != 1.0 && P.max_iters > 1)
+      {
         S(r, RS_T) = it.T0 * pow(P.anneal_ratio, (double)(iter + 1) / (double)(P.max_iters - 1));
+        S(r, RS_INVT) = 1.0 / S(r, RS_T);
+      }
       S(r, RS_ITERS) = iter + 1;
       const int64_t kr = (int64_t)k * a.R + it.rbase + r;
-      if (a.tr_step) a.tr_step[kr * P.max_iters + iter] = al;
-      if (a.tr_back) a.tr_back[kr * P.max_iters + iter] = (int)S(r, RS_NB);
+      if (a.tr_step && grank == 0) a.tr_step[kr * P.max_iters + iter] = al;
+      if (a.tr_back && grank == 0) a.tr_back[kr * P.max_iters + iter] = (int)S(r, RS_NB);
     } else if (tid < it.rn) {
       S(tid, RS_ACTIVE) = 0.0;  // stopped this iteration (reason already set)
     }
@@ -915,29 +1128,30 @@ __device__ void SplitCta<TC>::run(int item_id) {
     // side) in row order
     double sl = 0.0;
     begin_pass();
-    for (int64_t c0 = 0; c0 < it.n; c0 += a.CH) {
+    for (int64_t c0 = (int64_t)grank * a.CH; c0 < it.n; c0 += (int64_t)gsize * a.CH) {
       const int rows = load_chunk(c0);
       for (int pr = tid; pr < rows * a.Rg; pr += kSplitThreads) {
         const int row = pr / a.Rg, r = pr - row * a.Rg;
         double eL2 = 0.0, eR2 = 0.0;
         if (r < it.rn && S(r, RS_ACTIVE) != 0.0) {
           const double* w = th + r * dt();
-          const bool right = dot2_score(xs + row * d, w, d, w[d]) >= 0.0;
+          const bool right = dot2_score(xp + row * xps, w, d, w[d]) >= 0.0;
           const double e = ys[row] - fitted((right ? br : bl) + r * a.pmax, row);
           (right ? eR2 : eL2) = e * e;
         }
-        cache[(row * a.Rg + r) * 2] = eL2;
-        cache[(row * a.Rg + r) * 2 + 1] = eR2;
+        cache[row * (2 * a.Rg + 1) + r * 2] = eL2;
+        cache[row * (2 * a.Rg + 1) + r * 2 + 1] = eR2;
       }
       __syncthreads();
       if (tid < 2 * it.rn) {
         const int r = tid >> 1, side = tid & 1;
-        for (int row = 0; row < rows; ++row) sl += cache[(row * a.Rg + r) * 2 + side];
+        for (int row = 0; row < rows; ++row) sl += cache[row * (2 * a.Rg + 1) + r * 2 + side];
       }
       __syncthreads();
     }
     if (tid < 2 * it.rn) red[tid] = sl;
     __syncthreads();
+    gang_reduce(red, 2 * it.rn);
     if (tid < it.rn && S(tid, RS_ACTIVE) != 0.0) {
       const int r = tid;
       const int nr = (int)S(r, RS_NRIGHT), nl = n - nr;
@@ -949,7 +1163,7 @@ __device__ void SplitCta<TC>::run(int item_id) {
     __syncthreads();
   }
   // ----------------------------------------------------------- write results
-  if (tid < it.rn) {
+  if (tid < it.rn && grank == 0) {
     const int r = tid;
     const int64_t kr = (int64_t)k * a.R + it.rbase + r;
     const int dts = a.dmax + 1;
@@ -974,6 +1188,7 @@ __device__ void SplitCta<TC>::run(int item_id) {
     }
   }
   __syncthreads();
+  gang_end();
 }
 
 template <int TC>
@@ -993,7 +1208,8 @@ __global__ void __launch_bounds__(kSplitThreads, 1) split_kernel(SplitArgs a) {
     const int q = s_item;
     __syncthreads();
     if (q >= count) break;
-    cta.run(a.items[q]);
+    const int4 e = a.items[q];
+    cta.run(e.x, e.y, e.z);
   }
   cta.ring_drain();
 }
@@ -1115,14 +1331,27 @@ __global__ void split_init_theta(SplitArgs a, double* theta0, int64_t stride) {
 }
 
 struct SplitWs {
-  size_t counts, items, theta0, r_theta, r_loss, r_beta, r_child, r_ridge, r_i, r_alpha, total;
+  size_t counts, items, gang_rec, slot_flags, gang_scratch, theta0, r_theta, r_loss, r_beta, r_child,
+      r_ridge, r_i, r_alpha, total;
+  int nslots, gang_P;
+  bool gang_on;
 };
+// Gangs run only for levels with at most two restarts per node (one or two
+// work items per node), where a large node would otherwise hold one SM for
+// the whole level.
 SplitWs split_ws(int64_t K, int R, int dmax, int pmax) {
   SplitWs w;
   size_t o = 0;
   auto take = [&](size_t bytes) { size_t at = o; o = (o + bytes + 255) & ~(size_t)255; return at; };
+  w.gang_on = R <= 2;
+  const int pa = pmax + 1, E = pa * (pa + 1) / 2;
+  w.gang_P = w.gang_on ? std::max(std::max(E * 4, 2 * (dmax + 3)), 256) : 0;
+  w.nslots = w.gang_on ? device_sm_count() + 2 : 0;
   w.counts = take(4 * (kErrSlot + 1));
-  w.items = take(4 * (size_t)K * R);
+  w.items = take(16 * (size_t)K * R * (w.gang_on ? kGangMax : 1));
+  w.gang_rec = take(16 * (size_t)K * R);
+  w.slot_flags = take(4 * (size_t)std::max(w.nslots, 1));
+  w.gang_scratch = take(8 * (size_t)w.nslots * 2 * kGangMax * w.gang_P);
   w.theta0 = take(8 * (size_t)K * R * (ART_MAX_DIM + 1));
   w.r_theta = take(8 * (size_t)K * R * (dmax + 1));
   w.r_loss = take(8 * (size_t)K * R);
@@ -1214,6 +1443,7 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
   a.x = pr->x; a.y = pr->y; a.temperature = pr->temperature; a.ridge = pr->ridge;
   a.parent_loss = pr->parent_loss; a.fallback = pr->min_side_fallback;
   a.node_keys = pr->node_keys;
+  a.min_side = pr->min_side_points;
   a.prm = *prm;
   a.R = R; a.Rg = Rg; a.groups = (R + Rg - 1) / Rg;
   a.dmax = pr->max_dim; a.pmax = pr->max_features; a.TC = TC;
@@ -1233,7 +1463,13 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
   a.r_alpha = (double*)(ws + wl.r_alpha);
   a.tr_loss = out->trace_loss; a.tr_step = out->trace_step; a.tr_back = out->trace_backtracks;
   a.tr_gnorm = out->trace_grad_norm;
-  a.counts = (int32_t*)(ws + wl.counts); a.items = (int32_t*)(ws + wl.items);
+  a.counts = (int32_t*)(ws + wl.counts); a.items = (int4*)(ws + wl.items);
+  a.gang_on = wl.gang_on && a.Rg <= 2 ? 1 : 0;
+  a.nslots = wl.nslots;
+  a.gang_P = wl.gang_P;
+  a.gang_rec = (int4*)(ws + wl.gang_rec);
+  a.slot_flags = (int32_t*)(ws + wl.slot_flags);
+  a.gang_scratch = (double*)(ws + wl.gang_scratch);
   if (pr->theta0) {
     a.theta0 = pr->theta0;
     a.theta0_stride = pr->theta_stride;
@@ -1246,6 +1482,10 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
     count_launch();
   }
   if (cudaMemsetAsync(a.counts, 0, 4 * (kErrSlot + 1), s) != cudaSuccess) return check_launch("memset");
+  if (a.gang_on &&
+      (cudaMemsetAsync(a.gang_rec, 0, 16 * (size_t)K * a.groups, s) != cudaSuccess ||
+       cudaMemsetAsync(a.slot_flags, 0, 4 * (size_t)std::max(a.nslots, 1), s) != cudaSuccess))
+    return check_launch("memset");
   const unsigned pg = (unsigned)((K * a.groups + 255) / 256);
   prof_begin("split_plan", s);
   split_plan_hist<<<pg, 256, 0, s>>>(a);
@@ -1268,7 +1508,10 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
       return ART_E_UNSUPPORTED;
     }
     const int occ = resident_ctas((const void*)kern, kSplitThreads, smem);
-    const int64_t grid = std::min<int64_t>((int64_t)device_sm_count() * std::max(occ, 1), K * a.groups);
+    // with gangs every resident CTA may be needed (a gang's members must all
+    // be resident), so the grid is the full residency
+    const int64_t resident = (int64_t)device_sm_count() * std::max(occ, 1);
+    const int64_t grid = a.gang_on ? resident : std::min<int64_t>(resident, K * a.groups);
     prof_begin("split_level", s);
     kern<<<(unsigned)std::max<int64_t>(grid, 1), kSplitThreads, smem, s>>>(a);
     prof_end(s);

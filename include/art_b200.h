@@ -226,6 +226,9 @@ typedef struct ArtSplitProblem {
                                  by (seed, node_keys[k], r) instead of
                                  (seed, k, r), so a node's draws do not depend
                                  on its position in the batch               */
+  const int32_t* min_side_points; /* device [K] or NULL: per-node minimum side
+                                 count in place of params->min_side_points,
+                                 so nodes with different limits share a call */
 } ArtSplitProblem;
 
 /* stop reasons (splitters.py:424-488) */

@@ -260,3 +260,58 @@ def test_precision_is_validated():
     s.precision = "bf16"
     with pytest.raises(ValueError):
         split_params(s, True)
+
+
+def test_per_node_min_side_equals_separate_calls():
+    """Per-node minimum side counts in one launch give each node the result of
+    its own call with that limit."""
+
+    from art.splitters import split_level
+
+    ns, Xs, ys, th0, kd = random_level(7)
+    K = len(ns)
+    ro = np.concatenate([[0], np.cumsum(ns)])
+    x, y = np.concatenate([X.reshape(-1) for X in Xs]), np.concatenate(ys)
+    limits = np.array([5 + 7 * (k % 3) for k in range(K)], dtype=np.int32)
+    s = splitter_for(O.AFFINE, 0.15, 1e-6, th0.shape[1], 10, {"min_side_points": 1})
+    both = split_level(s, x, y, ro, [4] * K, kd, 0.15, 1e-6, theta0=th0, min_side_points=limits,
+                       group_restarts=0, trial_steps=0)
+    for lim in sorted(set(limits.tolist())):
+        s.min_side_points = int(lim)
+        alone = split_level(s, x, y, ro, [4] * K, kd, 0.15, 1e-6, theta0=th0, group_restarts=0, trial_steps=0)
+        for k in np.flatnonzero(limits == lim):
+            for name in ("theta", "n_right", "n_iters", "failure", "loss"):
+                np.testing.assert_array_equal(getattr(both, name).cpu().numpy()[k],
+                                              getattr(alone, name).cpu().numpy()[k], err_msg=f"{name} {k}")
+
+
+def test_gang_split_of_large_nodes_matches_oracle_and_is_batch_independent():
+    """Nodes above 65,536 rows (one restart) are split by gangs of CTAs that
+    add their pass sums in rank order: the result meets the per-node oracle
+    and is bit-identical whether the node is split alone or in a batch."""
+
+    from art.splitters import level_result_to_split, split_level
+
+    rng = np.random.default_rng(21)
+    ns = [150_000, 700, 70_000]          # gangs of 3, 1 and 2 CTAs
+    d = 3
+    Xs = [rng.uniform(-1, 1, (n, d)) for n in ns]
+    ys = [np.sin(2 * X[:, 0]) + 0.5 * np.tanh(4 * (X[:, 1] - X[:, 2])) for X in Xs]
+    th0 = np.array([[[0.6, 0.8, 0.0, 0.1]] for _ in ns])
+    T, lam, iters = 0.2, 1e-6, 6
+    s = splitter_for(O.AFFINE, T, lam, 1, iters, {"min_side_points": 1})
+    ro = np.concatenate([[0], np.cumsum(ns)])
+    x, y = np.concatenate([X.reshape(-1) for X in Xs]), np.concatenate(ys)
+    res = split_level(s, x, y, ro, [d] * 3, [O.AFFINE] * 3, T, lam, parent_loss=[1.0] * 3, theta0=th0)
+    p = S.Params(max_iters=iters, n_restarts=1, min_side_points=1)
+    for k in range(3):
+        opt = S.optimize(Xs[k], ys[k], th0[k][0], T, O.AFFINE, lam, p)
+        out = level_result_to_split(s, res, k, ns[k], 1.0, True)
+        np.testing.assert_allclose(np.r_[out.w, out.z], opt["theta"], rtol=1e-8, atol=1e-10)
+        assert out.n_iters == opt["n_iters"]
+    for k in (0, 2):
+        alone = split_level(s, Xs[k].reshape(-1), ys[k], [0, ns[k]], [d], [O.AFFINE], T, lam, parent_loss=[1.0],
+                            theta0=th0[k:k + 1])
+        for name in ("theta", "loss", "n_right", "n_iters", "beta"):
+            np.testing.assert_array_equal(getattr(alone, name).cpu().numpy()[0],
+                                          getattr(res, name).cpu().numpy()[k], err_msg=f"{name} {k}")
