@@ -119,7 +119,7 @@ class ArtSplitResult(C.Structure):
 class ArtPolytopes(C.Structure):
     _fields_ = [
         ("count", I64), ("dim", I32), ("lo", P), ("hi", P), ("row_offsets", P), ("A", P),
-        ("b", P), ("max_rows", I32), ("reserved", I32),
+        ("b", P), ("max_rows", I32), ("reserved", I32), ("direction_maps", P),
     ]
 
 

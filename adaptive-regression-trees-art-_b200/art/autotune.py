@@ -5,9 +5,11 @@ caller's own batch, with CUDA events on the launching stream:
 
 * ``ridge_tensor_min_features`` -- in the mixed ridge form, the smallest
   feature count p solved by the tensor-core kernel; smaller systems take the
-  FP64 kernels.  Each feature class p >= 33 of the sample is timed both ways
-  and the threshold is the smallest p from which the tensor-core kernel wins
-  for every larger class.
+  FP64 kernels.  Each feature class p >= 33 of the sample is timed on the
+  FP64 kernels and on the tensor-core kernel with its FP32 and its FP64
+  factorisation; the threshold is the smallest p from which the tensor-core
+  kernel wins for every larger class, and the factorisation is the one with
+  the lower total time over the tensor classes.
 * ``split_shape`` for a (d, p, R) split level -- the restarts that share one
   CTA's row passes (``group_restarts``) and the Armijo step sizes evaluated
   per trial pass (``trial_steps``); each candidate pair runs the sample
@@ -86,23 +88,31 @@ def table() -> dict:
     return dict(_TABLE)
 
 
-def _ridge_key(fp64_factor: bool) -> str:
-    return f"ridge|{device_key()}|f64factor={int(bool(fp64_factor))}"
+def _ridge_key() -> str:
+    return f"ridge|{device_key()}"
 
 
 def _split_key(d: int, p: int, R: int) -> str:
     return f"split|{device_key()}|d={int(d)}|p={int(p)}|R={int(R)}"
 
 
-def cached_ridge_threshold(dims=None, features=None, row_offsets=None, fp64_factor: bool = False) -> int:
-    """Tuned tensor-core threshold for this device, or 0 (library default)."""
+def cached_ridge_choice() -> tuple[int, bool | None]:
+    """Tuned (tensor-core threshold, FP64 factorisation) for this device, or (0, None)."""
 
     _load()
     try:
-        entry = _TABLE.get(_ridge_key(fp64_factor))
+        entry = _TABLE.get(_ridge_key())
     except RuntimeError:
-        return 0
-    return int(entry["tensor_min_features"]) if entry else 0
+        return 0, None
+    if not entry:
+        return 0, None
+    return int(entry["tensor_min_features"]), bool(entry.get("fp64_factor", False))
+
+
+def cached_ridge_threshold(dims=None, features=None, row_offsets=None, fp64_factor: bool = False) -> int:
+    """Tuned tensor-core threshold for this device, or 0 (library default)."""
+
+    return cached_ridge_choice()[0]
 
 
 def cached_split_shape(d: int, p: int, R: int) -> tuple[int, int]:
@@ -158,9 +168,10 @@ def _subset(x, y, w, row_offsets, x_offsets, dims, kinds, ridge, idx):
 
 
 def tune_ridge_threshold(x, y, w, row_offsets, dims, kinds, ridge, *, x_offsets=None, max_dim=None,
-                         fp64_factor: bool = False, per_class: int = 512, repeats: int = 3, seed: int = 0,
+                         fp64_factor: bool | None = None, per_class: int = 512, repeats: int = 3, seed: int = 0,
                          stream=None) -> dict:
-    """Time each tensor-eligible feature class both ways; store and return the choice."""
+    """Time each tensor-eligible feature class on every route; store and return the choice.
+    ``fp64_factor`` None tunes the factorisation too, a bool fixes it."""
 
     from .models import kind_feature_count, solve_weighted_ridge_batched
 
@@ -184,23 +195,34 @@ def tune_ridge_threshold(x, y, w, row_offsets, dims, kinds, ridge, *, x_offsets=
         sub = _subset(x, y, w, row_offsets, x_offsets, dims, kinds, ridge, idx)
         md = int(max_dim) if max_dim is not None else int(dh.max())
 
-        def run(threshold, sub=sub, p=p, md=md):
+        def run(threshold, factor, sub=sub, p=p, md=md):
             return solve_weighted_ridge_batched(
                 sub["x"], sub["y"], sub["w"], sub["row_offsets"], sub["dims"], sub["kinds"], sub["ridge"],
                 x_offsets=sub["x_offsets"], precision="mixed", max_features=p, max_dim=md,
-                fp64_factor=fp64_factor, tensor_min_features=threshold, stream=stream)
+                fp64_factor=factor, tensor_min_features=threshold, stream=stream)
 
-        timings[p] = {"tensor_ms": _event_time(lambda: run(p), repeats, stream),
-                      "fp64_ms": _event_time(lambda: run(NO_TENSOR), repeats, stream),
-                      "systems": int(idx.size)}
+        tm = {"fp64_ms": _event_time(lambda: run(NO_TENSOR, False), repeats, stream), "systems": int(idx.size)}
+        for factor in ((False, True) if fp64_factor is None else (bool(fp64_factor),)):
+            key = "tensor_f64factor_ms" if factor else "tensor_ms"
+            tm[key] = _event_time(lambda: run(p, factor), repeats, stream)
+        timings[p] = tm
+    # factorisation: lower total tensor-core time over the classes
+    if fp64_factor is None:
+        f32 = sum(v["tensor_ms"] for v in timings.values())
+        f64 = sum(v["tensor_f64factor_ms"] for v in timings.values())
+        factor = bool(f64 < f32)
+    else:
+        factor = bool(fp64_factor)
+    tkey = "tensor_f64factor_ms" if factor else "tensor_ms"
     choice = NO_TENSOR
     for p in sorted(timings, reverse=True):
-        if timings[p]["tensor_ms"] < timings[p]["fp64_ms"]:
+        if timings[p][tkey] < timings[p]["fp64_ms"]:
             choice = p
         else:
             break
-    entry = {"tensor_min_features": int(choice), "classes": {str(k): v for k, v in timings.items()}}
-    _store(_ridge_key(fp64_factor), entry)
+    entry = {"tensor_min_features": int(choice), "fp64_factor": factor,
+             "classes": {str(k): v for k, v in timings.items()}}
+    _store(_ridge_key(), entry)
     return entry
 
 

@@ -400,12 +400,16 @@ class RegressionTreeBuilder:
 
         sp = self.sampler
         if (not self.cohort_top_up or type(sp) is not HitAndRunSampler or getattr(sp, "rng_mode", "reference") != "device"
-                or self.isotropic_sampling or sp.direction_eigenvectors is not None
-                or sp.direction_eigenvalues is not None):
+                or sp.direction_eigenvectors is not None or sp.direction_eigenvalues is not None):
             return
         todo = [j for j in jobs if j.parent is not None and not j.topped]
         if len(todo) < 2:
             return
+        # a covariance-shaped top-up whose pilot chain fails draws one seed
+        # less one child at a time; then the cohort is undone and left to it
+        rng_state = copy.deepcopy(self._rng.bit_generator.state)
+        queries0 = self.oracle_queries
+        saved = [(j, j.samples) for j in todo]
         reqs = []
         with self._timing_context("sampling"):
             for job in todo:
@@ -427,15 +431,63 @@ class RegressionTreeBuilder:
                         "sampling_warnings": ()})
                     continue
                 x0 = X[int(self._rng.integers(0, n_inh))]
-                reqs.append((job, X, y, n_inh, n_new, x0, self._next_seed()))
+                if self.isotropic_sampling and bool(job.region.contains(x0, tol=sp.feasibility_tol)[0]):
+                    seeds = (self._next_seed(), self._next_seed())
+                else:  # an infeasible start fails in the pilot call, before the main seed
+                    seeds = (self._next_seed(), None)
+                reqs.append((job, X, y, n_inh, n_new, x0, seeds))
             if not reqs:
                 return
-            out = sp.sample_many([r[0].region for r in reqs], [r[4] for r in reqs], [r[6] for r in reqs],
-                                 [r[5] for r in reqs])
-            meta = {"sampling_method": type(sp).__name__, "sampling_thinning": sp.thinning,
-                    "sampling_pilot_length": 0, "sampling_covariance_condition_number": None,
-                    "sampling_warnings": ()}
-            for (job, X, y, n_inh, n_new, x0, seed), X_new in zip(reqs, out):
+            regions = [r[0].region for r in reqs]
+            metas = [{"sampling_method": type(sp).__name__, "sampling_thinning": sp.thinning,
+                      "sampling_pilot_length": 0, "sampling_covariance_condition_number": None,
+                      "sampling_warnings": ()} for _ in reqs]
+            if not self.isotropic_sampling:
+                out = sp.sample_many(regions, [r[4] for r in reqs], [r[6][0] for r in reqs], [r[5] for r in reqs])
+            else:
+                # covariance-shaped top-ups (builder.py:1141-1200): every child's
+                # pilot chain in one launch, its spectrum on the host, then every
+                # main chain in one launch with its own direction map
+                pilot_len = self.isotropic_pilot_multiplier * self.dimension
+                pilot_sampler = replace(sp, burn_in=0, thinning=1, direction_eigenvectors=None,
+                                        direction_eigenvalues=None)
+                pilots = pilot_sampler.sample_many(regions, [pilot_len] * len(reqs), [r[6][0] for r in reqs],
+                                                   [r[5] for r in reqs])
+                out = [None] * len(reqs)
+                main_idx, spectra, starts = [], [], []
+                for q, pilot in enumerate(pilots):
+                    if isinstance(pilot, Exception):
+                        if reqs[q][6][1] is not None:  # failed after the main seed was drawn: undo
+                            self._rng.bit_generator.state = rng_state
+                            self.oracle_queries = queries0
+                            for j, smp in saved:
+                                j.topped, j.topup_error, j.topup_pending, j.samples = False, None, None, smp
+                            return
+                        out[q] = pilot
+                        continue
+                    pilot = np.asarray(pilot, float)
+                    if pilot.shape != (pilot_len, self.dimension):
+                        out[q] = RuntimeError(f"Pilot sampler returned shape {pilot.shape}.")
+                        continue
+                    vecs, vals = sample_covariance_eigendecomposition(pilot)
+                    safe, floor = floor_covariance_eigenvalues(vals, sp.direction_eigenvalue_floor)
+                    saturated = bool(np.any(vals <= floor))
+                    metas[q] = {"sampling_method": "isotropic_hit_and_run", "sampling_thinning": sp.thinning,
+                                "sampling_pilot_length": pilot_len,
+                                "sampling_covariance_condition_number": float(np.max(safe) / np.min(safe)),
+                                "sampling_covariance_eigenvalue_floor": floor,
+                                "sampling_covariance_floor_saturated": saturated,
+                                "sampling_warnings": ("covariance_eigenvalue_floor_saturated",) if saturated else ()}
+                    main_idx.append(q)
+                    spectra.append((vecs, vals))
+                    starts.append(pilot[-1])
+                if main_idx:
+                    mains = sp.sample_many([regions[q] for q in main_idx], [reqs[q][4] for q in main_idx],
+                                           [reqs[q][6][1] for q in main_idx], starts, spectra=spectra)
+                    for q, X_new in zip(main_idx, mains):
+                        out[q] = X_new
+            for q, ((job, X, y, n_inh, n_new, x0, seeds), X_new) in enumerate(zip(reqs, out)):
+                meta = metas[q]
                 if isinstance(X_new, Exception):
                     job.topup_error = X_new
                     continue

@@ -216,6 +216,18 @@ class BatchedRidgeResult:
     info: object            # (K,) int32 (ART_INFO_* bits)
 
 
+def _factor_choice(requested, precision) -> bool:
+    """Explicit FP64-factorisation flag, else the autotuner's cached choice, else FP32."""
+
+    if requested is not None:
+        return bool(requested)
+    if precision != "mixed":
+        return False
+    from . import autotune
+
+    return bool(autotune.cached_ridge_choice()[1])
+
+
 def _tensor_threshold(requested, precision, dims_t, feats, ro, max_features) -> int:
     """Explicit threshold, else the autotuner's cached choice, else 0 (library default)."""
 
@@ -225,7 +237,7 @@ def _tensor_threshold(requested, precision, dims_t, feats, ro, max_features) -> 
         return 0
     from . import autotune
 
-    return autotune.cached_ridge_threshold(dims_t, feats, ro, fp64_factor=False)
+    return autotune.cached_ridge_choice()[0]
 
 
 def solve_weighted_ridge_batched(
@@ -245,7 +257,7 @@ def solve_weighted_ridge_batched(
     max_features: int | None = None,
     max_dim: int | None = None,
     condition: bool = False,
-    fp64_factor: bool = False,
+    fp64_factor: bool | None = None,
     tensor_min_features: int | None = None,
     out: BatchedRidgeResult | None = None,
     stream=None,
@@ -258,7 +270,8 @@ def solve_weighted_ridge_batched(
     ``weights=None`` means unit weights.  All array arguments may be numpy or
     torch; they are moved to the current CUDA device.  No host sync happens
     unless the caller reads the result.  ``fp64_factor`` makes the mixed form
-    factor its tensor-core Gram in FP64 (``ART_RIDGE_OPT_FP64_FACTOR``).
+    factor its tensor-core Gram in FP64 (``ART_RIDGE_OPT_FP64_FACTOR``); None
+    takes the autotuned choice for this device, else FP32.
     ``tensor_min_features`` is the smallest feature count the mixed form
     solves on the tensor cores (smaller systems take the FP64 kernels); None
     takes the autotuned choice for this device and batch, else the library
@@ -311,7 +324,7 @@ def solve_weighted_ridge_batched(
     prob = N.ArtRidgeProblem(
         seg, ptr(x), ptr(y), ptr(w), ptr(ridge_t), float(weight_floor), _SOLVER_CODES[solver],
         _PRECISION_CODES[precision], float(auto_rcond_threshold), int(max_features), int(max_dim),
-        N.RIDGE_OPT_FP64_FACTOR if fp64_factor else 0,
+        N.RIDGE_OPT_FP64_FACTOR if _factor_choice(fp64_factor, precision) else 0,
         int(_tensor_threshold(tensor_min_features, precision, dims_t, feats, ro, max_features)),
     )
     res = N.ArtRidgeResult(

@@ -167,6 +167,7 @@ class DevicePolytopes:
     A: object
     b: object
     max_rows: int
+    maps: object = None   # [count][d][d] direction maps (covariance-shaped sampling) or None
 
     @property
     def count(self) -> int:
@@ -201,8 +202,9 @@ def split_box_rows(A: np.ndarray, b: np.ndarray):
     return lo, hi, A[keep], b[keep]
 
 
-def device_polytopes(regions: Sequence[PolytopeRegion] | Sequence[tuple]) -> DevicePolytopes:
-    """Pack regions (or (A, b) pairs) for ``art_hit_and_run``."""
+def device_polytopes(regions: Sequence[PolytopeRegion] | Sequence[tuple], maps=None) -> DevicePolytopes:
+    """Pack regions (or (A, b) pairs) for ``art_hit_and_run``; ``maps`` gives
+    one d x d direction map per region (device draws become u = M z)."""
 
     t = torch()
     dev = require_cuda()
@@ -227,7 +229,8 @@ def device_polytopes(regions: Sequence[PolytopeRegion] | Sequence[tuple]) -> Dev
     return DevicePolytopes(
         d, to_device(np.stack(los), t.float64, dev), to_device(np.stack(his), t.float64, dev),
         to_device(np.asarray(offs, np.int64), t.int64, dev), to_device(Acat, t.float64, dev),
-        to_device(bcat, t.float64, dev), max_rows)
+        to_device(bcat, t.float64, dev), max_rows,
+        None if maps is None else to_device(np.ascontiguousarray(np.stack(maps), dtype=float), t.float64, dev))
 
 
 def hit_and_run_device(polys: DevicePolytopes, chain_polytope, x0, *, burn_in: int, thinning: int,
@@ -247,7 +250,7 @@ def hit_and_run_device(polys: DevicePolytopes, chain_polytope, x0, *, burn_in: i
     dr = None if directions is None else to_device(directions, t.float64, dev)
     un = None if uniforms is None else to_device(uniforms, t.float64, dev)
     P = N.ArtPolytopes(polys.count, polys.dim, ptr(polys.lo), ptr(polys.hi), ptr(polys.row_offsets),
-                       ptr(polys.A), ptr(polys.b), polys.max_rows, 0)
+                       ptr(polys.A), ptr(polys.b), polys.max_rows, 0, ptr(polys.maps))
     Ch = N.ArtChains(Cn, ptr(cp), ptr(x), ptr(sd), ptr(dr), ptr(un),
                      N.HAR_SCALAR if mode == "scalar" else N.HAR_BATCHED, int(burn_in), int(thinning),
                      int(n_rounds), int(counter_base), ptr(samples), ptr(status))
@@ -325,8 +328,8 @@ class HitAndRunSampler:
                 polys, [0], x[None, :], burn_in=self.burn_in, thinning=self.thinning, n_rounds=n,
                 mode="scalar", directions=dirs[None], uniforms=unif[None])
         else:
-            if vecs is not None:
-                raise NotImplementedError("covariance-shaped directions need rng_mode='reference'")
+            if vecs is not None:  # covariance-shaped directions: u = vecs diag(sqrt_vals) z on the device
+                polys = device_polytopes([region], maps=[vecs * sqrt_vals[None, :]])
             seed = int(rng.integers(0, 2**63 - 1))
             samples, _, status = hit_and_run_device(
                 polys, [0], x[None, :], burn_in=self.burn_in, thinning=self.thinning, n_rounds=n,
@@ -334,15 +337,16 @@ class HitAndRunSampler:
         _raise_status(status.cpu().numpy())
         return samples[:, 0, :].cpu().numpy()
 
-    def sample_many(self, regions, ns, random_states, x0s) -> list:
+    def sample_many(self, regions, ns, random_states, x0s, spectra=None) -> list:
         """``sample`` for several regions of one dimension in one launch.
 
-        Device draws only (``rng_mode="device"``, no direction spectrum).
-        Item k is what ``sample(regions[k], ns[k], random_states[k], x0s[k])``
-        returns, or the exception it raises: each chain is keyed by the seed
-        its own random state yields, and a chain's first n samples do not
-        depend on how many more it runs.  A chain that reports a failure is
-        rerun alone, which reproduces the single call exactly.
+        Device draws only (``rng_mode="device"``; the sampler itself has no
+        direction spectrum, item k may bring one in ``spectra[k]`` as an
+        (eigenvectors, eigenvalues) pair).  Item k is what the matching
+        single ``sample`` call returns, or the exception it raises: each chain
+        is keyed by the seed its own random state yields, and a chain's first
+        n samples do not depend on how many more it runs.  A chain that
+        reports a failure is rerun alone, which reproduces the single call.
         """
 
         if self.rng_mode != "device" or self.direction_eigenvectors is not None \
@@ -354,11 +358,23 @@ class HitAndRunSampler:
             raise ValueError("thinning must be at least 1.")
         out: list = [None] * len(regions)
         live = []
+        singles = {}
         for k, (reg, n, rs, x0) in enumerate(zip(regions, ns, random_states, x0s)):
             n = int(n)
             if n < 0:
                 out[k] = ValueError("n must be nonnegative.")
                 continue
+            single = self
+            mp = None
+            if spectra is not None and spectra[k] is not None:
+                single = replace(self, direction_eigenvectors=spectra[k][0], direction_eigenvalues=spectra[k][1])
+                try:
+                    vecs, sv = single._direction_spectrum(reg.dimension)
+                except ValueError as exc:
+                    out[k] = exc
+                    continue
+                mp = vecs * sv[None, :]
+            singles[k] = single
             rng = as_rng(rs)
             x = np.asarray(x0, dtype=float).reshape(-1)
             if x.shape[0] != reg.dimension:
@@ -370,20 +386,24 @@ class HitAndRunSampler:
             if n == 0:
                 out[k] = np.empty((0, reg.dimension))
                 continue
-            live.append((k, reg, n, x, int(rng.integers(0, 2**63 - 1))))
+            live.append((k, reg, n, x, int(rng.integers(0, 2**63 - 1)), mp))
         if not live:
             return out
-        polys = device_polytopes([it[1] for it in live])
+        maps = None
+        if any(it[5] is not None for it in live):
+            d = live[0][1].dimension
+            maps = [np.eye(d) if it[5] is None else it[5] for it in live]
+        polys = device_polytopes([it[1] for it in live], maps=maps)
         samples, _, status = hit_and_run_device(
             polys, np.arange(len(live)), np.stack([it[3] for it in live]), burn_in=self.burn_in,
             thinning=self.thinning, n_rounds=max(it[2] for it in live), mode="scalar",
             seeds=[it[4] for it in live])
         st = status.cpu().numpy()
         host = samples.cpu().numpy()
-        for c, (k, reg, n, x, _) in enumerate(live):
+        for c, (k, reg, n, x, _, _) in enumerate(live):
             if st[c] != 0:
                 try:
-                    out[k] = self.sample(reg, n, random_state=random_states[k], x0=x0s[k])
+                    out[k] = singles[k].sample(reg, n, random_state=random_states[k], x0=x0s[k])
                 except (RuntimeError, ValueError) as exc:
                     out[k] = exc
             else:
@@ -436,9 +456,9 @@ class BatchedHitAndRunSampler(HitAndRunSampler):
         polys = device_polytopes([region])
         if self.rng_mode == "reference":
             raise NotImplementedError("batched chains use device draws; inject draws via hit_and_run_device")
-        vecs, _ = self._direction_spectrum(d)
-        if vecs is not None:
-            raise NotImplementedError("covariance-shaped directions need the scalar sampler in reference mode")
+        vecs, sqrt_vals = self._direction_spectrum(d)
+        if vecs is not None:  # covariance-shaped directions: u = vecs diag(sqrt_vals) z on the device
+            polys = device_polytopes([region], maps=[vecs * sqrt_vals[None, :]])
         seeds = rng.integers(0, 2**63 - 1, size=n_chains, dtype=np.int64).astype(np.uint64)
         rounds = full_rounds + (1 if remainder else 0)
         samples, _, status = hit_and_run_device(

@@ -33,6 +33,10 @@ sys.path.insert(0, str(ROOT / "adaptive-regression-trees-art-_b200"))
 sys.path.insert(0, str(ROOT))
 
 METRIC = "ridge solves/s"
+# DRAM bytes (read + write) per row of the tensor-core class, from the ncu
+# capture of the tensor-core ridge kernel on the 8,192-system case at the
+# tuned threshold (153 features); None until captured.
+RIDGE_TC_DRAM_BYTES_PER_ROW = None
 UNIT = "solves/s"
 WORKLOAD = ("batched weighted ridge: 65,536 systems/GPU, n log-uniform [64, 8192], d in {8,16}, "
             "affine or quadratic features (p = 9/17/45/153), sigmoid-product weights, "
@@ -47,7 +51,7 @@ def parse():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--systems", type=int, default=65536)
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
-    ap.add_argument("--cpu-per-class", type=int, default=384,
+    ap.add_argument("--cpu-per-class", type=int, default=1024,
                     help="systems per feature class in the timed CPU sample")
     ap.add_argument("--fp64-factor", action="store_true",
                     help="mixed form factors the tensor-core Gram in FP64")
@@ -65,6 +69,8 @@ def parse():
     ap.add_argument("--serve-jobs", type=int, default=40)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default launch shapes")
+    ap.add_argument("--tensor-min-features", type=int, default=None,
+                    help="fix the mixed form's tensor-core threshold instead of tuning it")
     ap.add_argument("--autotune-per-class", type=int, default=1024,
                     help="systems per feature class in the autotuner's sample")
     return ap.parse_args()
@@ -525,7 +531,8 @@ def run_b200(args):
         return solve_weighted_ridge_batched(
             wl.x, wl.y, wl.w, ro, dims, kinds, ridge, x_offsets=xo, precision=precision,
             max_features=wl.max_features, max_dim=wl.max_dim, out=out,
-            fp64_factor=args.fp64_factor if fp64_factor is None else fp64_factor)
+            fp64_factor=(True if args.fp64_factor else None) if fp64_factor is None else fp64_factor,
+            tensor_min_features=args.tensor_min_features)
 
     def barrier():
         if world > 1:
@@ -558,9 +565,9 @@ def run_b200(args):
     from art import autotune
 
     tuned = None
-    if args.precision == "mixed" and not args.no_autotune:
+    if args.precision == "mixed" and not args.no_autotune and args.tensor_min_features is None:
         tuned = autotune.tune_ridge_threshold(wl.x, wl.y, wl.w, ro, dims, kinds, ridge, x_offsets=xo,
-                                              max_dim=wl.max_dim, fp64_factor=args.fp64_factor,
+                                              max_dim=wl.max_dim, fp64_factor=True if args.fp64_factor else None,
                                               per_class=args.autotune_per_class, stream=stream)
 
     # plain FP64 form, batched and per node (one call per system, the
@@ -597,14 +604,27 @@ def run_b200(args):
     elif "fp64<8>" in name:
         cls_idx = np.flatnonzero(p_all + 1 > 48) if args.precision == "fp64" else np.flatnonzero(info & N.INFO_FP64_RESOLVE)
     else:
-        cls_idx = np.flatnonzero(p_all >= (tuned["tensor_min_features"] if tuned else 33))
+        thr = args.tensor_min_features or (tuned["tensor_min_features"] if tuned else 33)
+        cls_idx = np.flatnonzero(p_all >= thr)
     flops, nbytes = algorithmic(wl, cls_idx)
     achieved_gbs = nbytes / (per_launch_ms / 1000.0) / 1e9
-    roofline = {"bound": "hbm", "kernel": name, "achieved": achieved_gbs, "peak": hbm,
-                "unit": "GB/s", "frac": achieved_gbs / hbm, "traffic": None,
-                "peak_source": peak_kind,
-                "achieved_tflops": flops / (per_launch_ms / 1000.0) / 1e12,
-                "launch_ms": per_launch_ms, "kernel_share": total_ms / sum(v[1] for v in prof.values())}
+    achieved_tf = flops / (per_launch_ms / 1000.0) / 1e12
+    share = total_ms / sum(v[1] for v in prof.values())
+    if name.startswith("ridge_tc"):
+        # quadratic systems: 27-166 algorithmic flop/B, tensor-core bound;
+        # traffic per launch from the ncu capture of the 8,192-system case
+        # (DRAM bytes per tensor-class row, times this launch's rows)
+        n_rows = float(np.diff(wl.row_offsets)[cls_idx].sum())
+        roofline = {"bound": "tensor", "kernel": name, "achieved": achieved_tf, "peak": bf16,
+                    "unit": "TFLOP/s", "frac": achieved_tf / bf16,
+                    "traffic": RIDGE_TC_DRAM_BYTES_PER_ROW * n_rows if RIDGE_TC_DRAM_BYTES_PER_ROW else None,
+                    "peak_source": f"{peak_kind} bf16 dense (the kernel issues TF32 hi/lo split products)",
+                    "algorithmic_bytes": nbytes, "achieved_gbs": achieved_gbs, "hbm_frac": achieved_gbs / hbm,
+                    "launch_ms": per_launch_ms, "kernel_share": share}
+    else:
+        roofline = {"bound": "hbm", "kernel": name, "achieved": achieved_gbs, "peak": hbm,
+                    "unit": "GB/s", "frac": achieved_gbs / hbm, "traffic": None, "peak_source": peak_kind,
+                    "achieved_tflops": achieved_tf, "launch_ms": per_launch_ms, "kernel_share": share}
 
     # end-to-end through the public API with host buffers
     e2e = None
@@ -688,7 +708,7 @@ def run_b200(args):
         "status_ok_fraction": ok,
         "fp64_resolve_fraction": float(np.mean((info & N.INFO_FP64_RESOLVE) != 0)),
         "mean_refine_passes_tensor_class": float(np.mean(((info >> N.INFO_REFINE_SHIFT) & 255)[p_all >= 33])),
-        "fp64_factor": bool(args.fp64_factor),
+        "fp64_factor": bool(args.fp64_factor) or bool(tuned and tuned.get("fp64_factor")),
         "autotune": tuned,
         "variants": variants,
         "plain_kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in plain_prof.items()},

@@ -297,6 +297,11 @@ typedef struct ArtPolytopes {
   const double* b;            /* device [rows]                               */
   int32_t max_rows;           /* host-known max oblique rows per polytope    */
   int32_t reserved;
+  const double* direction_maps; /* device [count][d][d] or NULL: device-drawn
+                                 directions of polytope j's chains are
+                                 u = M_j z (covariance-shaped sampling,
+                                 sampling.py:86-127); injected draws are used
+                                 as given                                    */
 } ArtPolytopes;
 
 typedef struct ArtChains {

@@ -73,9 +73,12 @@ def test_bfs_build_with_graphs_equals_build_without():
             np.testing.assert_array_equal(u.model.coef_, v.model.coef_)
 
 
-def test_cohort_top_up_equals_one_child_at_a_time():
-    """BFS children topped up in one hit-and-run launch per cohort get the
-    samples (and hence the tree) of the one-at-a-time top-up."""
+@pytest.mark.parametrize("isotropic", [False, True])
+def test_cohort_top_up_equals_one_child_at_a_time(isotropic):
+    """BFS children topped up in one hit-and-run launch per cohort (two with
+    covariance-shaped sampling: pilots, then main chains with per-child
+    direction maps) get the samples, and hence the tree, of the one-at-a-time
+    top-up."""
 
     from art import (AffineRidgeModel, BoxDomain, HitAndRunSampler, RegressionTreeBuilder, SoftObliqueSplitter,
                      SplitNode, TemperatureConfig)
@@ -91,7 +94,7 @@ def test_cohort_top_up_equals_one_child_at_a_time():
                                   splitter=sp, error_threshold=0.01, max_depth=4, sample_count=400,
                                   temperature_config=TemperatureConfig(strategy="splitter"), random_state=9,
                                   oracle_vectorized=True, traversal="bfs", cohort_top_up=cohort,
-                                  isotropic_sampling=False,
+                                  isotropic_sampling=isotropic,
                                   sampler=HitAndRunSampler(burn_in=0, thinning=4, rng_mode="device"))
         return b.build()
 

@@ -158,3 +158,31 @@ def test_infeasible_start_and_empty_chord_are_reported():
                                       thinning=1, n_rounds=2, mode="batched", seeds=[1, 2])
     st = status.cpu().numpy()
     assert st[0] == 0 and st[1] == 2
+
+
+def test_device_draws_with_covariance_shaped_directions():
+    """Device draws with a direction spectrum move along u = Q diag(sqrt(l)) z:
+    chains stay feasible and their sample covariance is elongated along the
+    leading eigenvector, as the reference's covariance-shaped sampler is."""
+
+    from art.domain import BoxDomain
+    from art.sampling import HitAndRunSampler
+
+    region = BoxDomain.hypercube(2, -1.0, 1.0).as_region()
+    th = np.pi / 6
+    Q = np.array([[np.cos(th), -np.sin(th)], [np.sin(th), np.cos(th)]])
+    vals = np.array([1.0, 1e-4])
+    iso = HitAndRunSampler(burn_in=50, thinning=1, rng_mode="device")
+    aniso = HitAndRunSampler(burn_in=50, thinning=1, rng_mode="device", direction_eigenvectors=Q,
+                             direction_eigenvalues=vals)
+    X = aniso.sample(region, 4000, random_state=3, x0=np.zeros(2))
+    assert X.shape == (4000, 2) and np.all(region.contains(X))
+    steps = np.diff(X, axis=0)
+    steps = steps[np.linalg.norm(steps, axis=1) > 0]
+    ang = np.abs(steps @ Q[:, 1]) / np.linalg.norm(steps, axis=1)   # component along the small axis
+    assert np.median(ang) < 0.05
+    Y = iso.sample(region, 4000, random_state=3, x0=np.zeros(2))
+    sy = np.diff(Y, axis=0)
+    assert np.median(np.abs(sy @ Q[:, 1]) / np.linalg.norm(sy, axis=1)) > 0.3
+    again = aniso.sample(region, 4000, random_state=3, x0=np.zeros(2))
+    np.testing.assert_array_equal(X, again)
