@@ -33,6 +33,7 @@ struct HarArgs {
   const int64_t* row_offsets;
   const double* A;
   const double* b;
+  const double* maps;  // [n_poly][d][d] or NULL
   int64_t n_chains;
   const int32_t* polytope;
   double* x;
@@ -139,6 +140,19 @@ __global__ void __launch_bounds__(kHarThreads) har_kernel(HarArgs a) {
       normal_pair_f32(r, u0, u1);
       if (!h0) u0 = 0.0;
       if (!h1) u1 = 0.0;
+      if (a.maps) {  // covariance-shaped direction u = M z, z gathered across the team
+        const double* M = a.maps + (int64_t)pj * d * d;
+        double m0 = 0.0, m1 = 0.0;
+        for (int j = 0; j < d; ++j) {
+          const double za = __shfl_sync(0xffffffffu, u0, j >> 1, L);
+          const double zb = __shfl_sync(0xffffffffu, u1, j >> 1, L);
+          const double zj = (j & 1) ? zb : za;
+          if (h0) m0 = fma(M[(int64_t)i0 * d + j], zj, m0);
+          if (h1) m1 = fma(M[(int64_t)i1 * d + j], zj, m1);
+        }
+        u0 = m0;
+        u1 = m1;
+      }
     }
     bool skip = false;
     if (scalar) {
@@ -278,6 +292,7 @@ extern "C" int art_hit_and_run(const ArtPolytopes* P, const ArtChains* C, art_st
   }
   HarArgs a;
   a.n_poly = P->count; a.d = P->dim; a.lo = P->lo; a.hi = P->hi;
+  a.maps = P->direction_maps;
   a.row_offsets = P->row_offsets; a.A = P->A; a.b = P->b;
   a.n_chains = C->count; a.polytope = C->polytope; a.x = C->x; a.seeds = C->seeds;
   a.dirs = C->directions; a.unif = C->uniforms; a.mode = C->mode;
