@@ -72,8 +72,16 @@ __device__ __forceinline__ int team_or(int v) {
   return v;
 }
 
+// Oblique rows of a team's polytope live in shared memory (team stride
+// MAXK * d + 1 doubles, odd, so the teams of a warp use different banks);
+// row r's slack, bound and direction product are kept by lane r % L only.
+template <int L, int MAXK>
+__host__ __device__ constexpr size_t har_team_stride(int d) { return (size_t)MAXK * d + 1; }
+
 template <int L, int MAXK>
 __global__ void __launch_bounds__(kHarThreads) har_kernel(HarArgs a) {
+  extern __shared__ double s_rows[];
+  constexpr int OWN = (MAXK + L - 1) / L;  // rows owned by each lane
   const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t chain_raw = gt / L;
   const int lane = (int)(gt % L);
@@ -99,13 +107,23 @@ __global__ void __launch_bounds__(kHarThreads) har_kernel(HarArgs a) {
     hi0 = h0 ? a.hi[(int64_t)pj * d + i0] : 0.0;
     hi1 = h1 ? a.hi[(int64_t)pj * d + i1] : 0.0;
   }
-  double ar0[MAXK], ar1[MAXK], br[MAXK], so[MAXK];
+  double* Ar = s_rows + (size_t)(threadIdx.x / L) * har_team_stride<L, MAXK>(d);
+  for (int e = lane; e < MAXK * d; e += L) {
+    const int r = e / d, i = e - r * d;
+    Ar[e] = (r < k && status == 0) ? a.A[(rb + r) * d + i] : 0.0;
+  }
+  __syncwarp();
+  // this lane's coefficient of row r on its two coordinates
+  auto arow = [&](int r, double v0, double v1) {
+    return (h0 ? Ar[r * d + i0] * v0 : 0.0) + (h1 ? Ar[r * d + i1] * v1 : 0.0);
+  };
+  double br[OWN], so[OWN], au[OWN];
 #pragma unroll
-  for (int r = 0; r < MAXK; ++r) {
-    const bool on = r < k && status == 0;
-    ar0[r] = (on && h0) ? a.A[(rb + r) * d + i0] : 0.0;
-    ar1[r] = (on && h1) ? a.A[(rb + r) * d + i1] : 0.0;
-    br[r] = on ? a.b[rb + r] : 0.0;
+  for (int m = 0; m < OWN; ++m) {
+    const int r = m * L + lane;
+    br[m] = (r < MAXK && r < k && status == 0) ? a.b[rb + r] : 0.0;
+    so[m] = 0.0;
+    au[m] = 0.0;
   }
   // initial slacks s = b - A x (numba path: sampling.py:648)
   double shi0 = hi0 - x0, shi1 = hi1 - x1, slo0 = x0 - lo0, slo1 = x1 - lo1;
@@ -116,9 +134,11 @@ __global__ void __launch_bounds__(kHarThreads) har_kernel(HarArgs a) {
   }
 #pragma unroll
   for (int r = 0; r < MAXK; ++r) {
-    double ax = team_sum<L>(ar0[r] * x0 + ar1[r] * x1);
-    so[r] = br[r] - ax;
-    if (r < k && so[r] < -kFeasTol) bad_start = 1;
+    const double ax = team_sum<L>(arow(r, x0, x1));
+    if (r % L == lane) {
+      so[r / L] = br[r / L] - ax;
+      if (r < k && so[r / L] < -kFeasTol) bad_start = 1;
+    }
   }
   bad_start = team_or<L>(bad_start);
   if (bad_start && status == 0) status = 2;
@@ -163,11 +183,16 @@ __global__ void __launch_bounds__(kHarThreads) har_kernel(HarArgs a) {
       // recompute slacks from x (sampling.py:548-550)
       shi0 = hi0 - x0; shi1 = hi1 - x1; slo0 = x0 - lo0; slo1 = x1 - lo1;
 #pragma unroll
-      for (int r = 0; r < MAXK; ++r) so[r] = br[r] - team_sum<L>(ar0[r] * x0 + ar1[r] * x1);
+      for (int r = 0; r < MAXK; ++r) {
+        const double ax = team_sum<L>(arow(r, x0, x1));
+        if (r % L == lane) so[r / L] = br[r / L] - ax;
+      }
     }
-    double au[MAXK];
 #pragma unroll
-    for (int r = 0; r < MAXK; ++r) au[r] = team_sum<L>(ar0[r] * u0 + ar1[r] * u1);
+    for (int r = 0; r < MAXK; ++r) {
+      const double v = team_sum<L>(arow(r, u0, u1));
+      if (r % L == lane) au[r / L] = v;
+    }
     if (!skip) {
       const double pos_t = scalar ? kScalarParallelTol : 0.0;
       double tlo = -INFINITY, thi = INFINITY;
@@ -183,7 +208,7 @@ __global__ void __launch_bounds__(kHarThreads) har_kernel(HarArgs a) {
       }
 #pragma unroll
       for (int r = 0; r < MAXK; ++r)
-        if (r < k && lane == 0) box_row(so[r], au[r]);
+        if (r < k && r % L == lane) box_row(so[r / L], au[r / L]);
       tlo = team_max<L>(tlo);
       thi = team_min<L>(thi);
       infeasible = team_or<L>(infeasible);
@@ -209,7 +234,7 @@ __global__ void __launch_bounds__(kHarThreads) har_kernel(HarArgs a) {
           slo0 = __dsub_rn(slo0, __dmul_rn(t, -u0));
           slo1 = __dsub_rn(slo1, __dmul_rn(t, -u1));
 #pragma unroll
-          for (int r = 0; r < MAXK; ++r) so[r] = __dsub_rn(so[r], __dmul_rn(t, au[r]));
+          for (int m = 0; m < OWN; ++m) so[m] = __dsub_rn(so[m], __dmul_rn(t, au[m]));
         }
       }
     }
@@ -234,18 +259,33 @@ __global__ void __launch_bounds__(kHarThreads) har_kernel(HarArgs a) {
   }
 }
 
+template <int L, int MAXK>
+int launch_har_k(const HarArgs& a, unsigned grid, cudaStream_t s) {
+  const size_t smem = (size_t)(kHarThreads / L) * har_team_stride<L, MAXK>(a.d) * 8;
+  if (cudaFuncSetAttribute(har_kernel<L, MAXK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    set_error("art_hit_and_run: cannot reserve %zu bytes of shared memory", smem);
+    return ART_E_UNSUPPORTED;
+  }
+  cudaFuncSetAttribute(har_kernel<L, MAXK>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       (int)cudaSharedmemCarveoutMaxShared);
+  cudaGetLastError();
+  prof_begin("hit_and_run", s);
+  har_kernel<L, MAXK><<<grid, kHarThreads, smem, s>>>(a);
+  prof_end(s);
+  count_launch();
+  return check_launch("art_hit_and_run");
+}
+
 template <int L>
 int launch_har_l(const HarArgs& a, int maxk, cudaStream_t s) {
   const int64_t threads = a.n_chains * L;
   const unsigned grid = (unsigned)((threads + kHarThreads - 1) / kHarThreads);
-  prof_begin("hit_and_run", s);
-  if (maxk <= 4) har_kernel<L, 4><<<grid, kHarThreads, 0, s>>>(a);
-  else if (maxk <= 8) har_kernel<L, 8><<<grid, kHarThreads, 0, s>>>(a);
-  else if (maxk <= 16) har_kernel<L, 16><<<grid, kHarThreads, 0, s>>>(a);
-  else har_kernel<L, 32><<<grid, kHarThreads, 0, s>>>(a);
-  prof_end(s);
-  count_launch();
-  return check_launch("art_hit_and_run");
+  if (maxk <= 4) return launch_har_k<L, 4>(a, grid, s);
+  if (maxk <= 8) return launch_har_k<L, 8>(a, grid, s);
+  if (maxk <= 16) return launch_har_k<L, 16>(a, grid, s);
+  return launch_har_k<L, 32>(a, grid, s);
 }
 
 }  // namespace

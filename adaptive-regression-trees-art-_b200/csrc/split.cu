@@ -45,7 +45,7 @@ constexpr int kErrSlot = 2 + 2 * kBuckets;  // counts[kErrSlot]: a bounded wait 
 // min(kGangMax, ceil(n / kGangRows)) CTAs that take interleaved chunks and
 // add their pass sums in rank order through global scratch.  The gang size
 // depends on n alone, so a node's result never depends on its batch.
-constexpr int kGangRows = 65536;
+constexpr int kGangRows = 16384;
 constexpr int kGangMax = 16;
 // A gang forms when its last member is popped, which can wait for other
 // work items to finish: that wait is bounded by a longer limit than the

@@ -286,14 +286,14 @@ def test_per_node_min_side_equals_separate_calls():
 
 
 def test_gang_split_of_large_nodes_matches_oracle_and_is_batch_independent():
-    """Nodes above 65,536 rows (one restart) are split by gangs of CTAs that
+    """Nodes above 16,384 rows (one restart) are split by gangs of CTAs that
     add their pass sums in rank order: the result meets the per-node oracle
     and is bit-identical whether the node is split alone or in a batch."""
 
     from art.splitters import level_result_to_split, split_level
 
     rng = np.random.default_rng(21)
-    ns = [150_000, 700, 70_000]          # gangs of 3, 1 and 2 CTAs
+    ns = [150_000, 700, 70_000]          # gangs of 10, 1 and 5 CTAs
     d = 3
     Xs = [rng.uniform(-1, 1, (n, d)) for n in ns]
     ys = [np.sin(2 * X[:, 0]) + 0.5 * np.tanh(4 * (X[:, 1] - X[:, 2])) for X in Xs]
