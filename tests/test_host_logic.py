@@ -1,0 +1,86 @@
+"""Host-side logic that needs no GPU: the ctypes mirror of the C ABI structs,
+the autotuner's persistent table and candidate lists, and graph shape classes."""
+
+import ctypes as C
+import json
+import subprocess
+import sys
+
+import pytest
+
+from conftest import ROOT
+
+STRUCTS = ["ArtSegments", "ArtRidgeProblem", "ArtRidgeResult", "ArtSplitParams", "ArtSplitProblem",
+           "ArtSplitResult", "ArtPolytopes", "ArtChains"]
+
+
+def test_ctypes_structs_match_the_header_layout(tmp_path):
+    """sizeof and field offsets of every ABI struct, from gcc on include/art_b200.h,
+    equal the Python mirror's (a drifted mirror would pass garbage pointers)."""
+
+    sys.path.insert(0, str(ROOT / "adaptive-regression-trees-art-_b200"))
+    from art import _native as N
+
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "art_b200.h"', 'int main(void) {']
+    for name in STRUCTS:
+        lines.append(f'  printf("{name} %zu\\n", sizeof({name}));')
+        for fname, _ in getattr(N, name)._fields_:
+            lines.append(f'  printf("{name}.{fname} %zu\\n", offsetof({name}, {fname}));')
+    lines.append('  return 0; }')
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    out = dict(line.rsplit(" ", 1) for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                               check=True).stdout.splitlines())
+    for name in STRUCTS:
+        cls = getattr(N, name)
+        assert int(out[name]) == C.sizeof(cls), name
+        for fname, _ in cls._fields_:
+            assert int(out[f"{name}.{fname}"]) == getattr(cls, fname).offset, f"{name}.{fname}"
+
+
+def test_autotune_table_persists_and_is_keyed_by_device(tmp_path, monkeypatch):
+    sys.path.insert(0, str(ROOT / "adaptive-regression-trees-art-_b200"))
+    from art import autotune
+
+    path = tmp_path / "tune.json"
+    monkeypatch.setenv("ART_AUTOTUNE_CACHE", str(path))
+    monkeypatch.setattr(autotune, "device_key", lambda: "test-device|sm148|cc10.0")
+    monkeypatch.setattr(autotune, "_LOADED", False)
+    autotune.clear()
+    try:
+        assert autotune.cached_split_shape(16, 17, 16) == (0, 0)
+        assert autotune.cached_ridge_choice() == (0, None)
+        autotune._store(autotune._split_key(16, 17, 16), {"group_restarts": 8, "trial_steps": 2})
+        autotune._store(autotune._ridge_key(), {"tensor_min_features": 153, "fp64_factor": False})
+        saved = json.loads(path.read_text())
+        assert len(saved) == 2
+        autotune.clear()
+        monkeypatch.setattr(autotune, "_LOADED", False)
+        assert autotune.cached_split_shape(16, 17, 16) == (8, 2)       # reloaded from the file
+        assert autotune.cached_ridge_choice() == (153, False)
+        monkeypatch.setattr(autotune, "device_key", lambda: "other-device|sm132|cc9.0")
+        assert autotune.cached_split_shape(16, 17, 16) == (0, 0)       # another device: untuned
+    finally:
+        autotune.clear()
+
+
+@pytest.mark.parametrize("R,backtracks", [(1, 25), (2, 25), (16, 25), (16, 3)])
+def test_split_candidates_respect_thread_and_backtrack_limits(R, backtracks):
+    sys.path.insert(0, str(ROOT / "adaptive-regression-trees-art-_b200"))
+    from art import autotune
+
+    cands = autotune.split_candidates(R, backtracks)
+    assert cands and len(set(cands)) == len(cands)
+    for g, h in cands:
+        assert 1 <= g <= min(R, 16)
+        assert 1 <= h <= min(32, 256 // g, backtracks + 1)
+
+
+def test_graph_shape_classes_round_up_to_powers_of_two():
+    sys.path.insert(0, str(ROOT / "adaptive-regression-trees-art-_b200"))
+    from art.graphs import _pow2
+
+    assert [_pow2(v, 8) for v in (0, 1, 8, 9, 16, 17, 1000)] == [8, 8, 8, 16, 16, 32, 1024]
+    assert _pow2(5000, 4096) == 8192 and _pow2(10, 4096) == 4096
