@@ -316,7 +316,8 @@ class ServingEngine:
                                  n_restarts=1)
         res = split_level(sp, xs, ys, sro, dd, kinds[idx], temps, ridge, x_offsets=sxo, hard_refit=False,
                           node_keys=keys, max_dim=int(dd.max()), max_features=int(max(st.job.n_features for st, _ in sub)),
-                          min_side_points=min_side, group_restarts=0, trial_steps=0, stream=self.stream)
+                          min_side_points=min_side, group_restarts=0, trial_steps=0, ctas_per_sm=0,
+                          stream=self.stream)
         failure = res.failure.cpu().numpy()
         theta = res.theta
         ok = failure == 0

@@ -33,6 +33,9 @@ namespace art {
 namespace {
 
 constexpr int kSplitThreads = 256;
+// shared memory of one of two CTAs sharing an SM (228 KB less 1 KB reserved
+// per CTA, rounded down)
+constexpr size_t kHalfSmem = 110 * 1024;
 constexpr int kWarps = kSplitThreads / 32;
 constexpr int kMaxCH = 256;      // rows per chunk: a multiple of 32 up to this
 constexpr int kMaxP = 64;        // child model features
@@ -1191,8 +1194,11 @@ __device__ void SplitCta<TC>::run(int item_id, int rank, int members) {
   gang_end();
 }
 
-template <int TC>
-__global__ void __launch_bounds__(kSplitThreads, 1) split_kernel(SplitArgs a) {
+// MINB resident CTAs per SM: 1 keeps every register a thread wants and the
+// deepest row ring; 2 doubles the warps that hide the per-row latency of the
+// passes at the cost of a 128-register cap and half the shared memory
+template <int TC, int MINB>
+__global__ void __launch_bounds__(kSplitThreads, MINB) split_kernel(SplitArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_item;
   SplitCta<TC> cta(a, smem);
@@ -1413,7 +1419,7 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
       !(prm->armijo_c > 0.0 && prm->armijo_c < 1.0) || !(prm->alpha0 > 0.0) ||
       !(prm->alpha_min > 0.0) || prm->alpha_max < prm->alpha_min || prm->min_side_points < 1 ||
       !(prm->min_side_fraction >= 0.0 && prm->min_side_fraction < 0.5) || !(prm->anneal_ratio > 0.0) ||
-      prm->group_restarts < 0 || prm->trial_steps < 0) {
+      prm->group_restarts < 0 || prm->trial_steps < 0 || prm->ctas_per_sm < 0 || prm->ctas_per_sm > 2) {
     set_error("art_split_level: invalid splitter parameters");
     return ART_E_INVALID;
   }
@@ -1494,11 +1500,18 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
   prof_end(s);
   count_launch(); count_launch(); count_launch();
   // longest chunk (fewer block barriers per row) with a ring of at least 4
-  // stages that fits shared memory, then the deepest ring for that chunk
+  // stages (2 at two CTAs per SM) that fits shared memory, then the deepest
+  // ring for that chunk; two CTAs per SM fall back to one when even the
+  // shortest chunk does not fit half the SM's shared memory
+  int minb = prm->ctas_per_sm == 2 ? 2 : 1;
+  if (minb == 2 && split_layout(a.dmax, a.pmax, a.Rg, a.H, 1, 32).total > kHalfSmem) minb = 1;
+  const size_t chunk_budget = minb == 2 ? 100 * 1024 : 200 * 1024;
+  const size_t smem_budget = minb == 2 ? kHalfSmem : 227 * 1024;
+  const int min_stages = minb == 2 ? 2 : 4;
   a.CH = kMaxCH;
-  while (a.CH > 32 && split_layout(a.dmax, a.pmax, a.Rg, a.H, 4, a.CH).total > 200 * 1024) a.CH >>= 1;
+  while (a.CH > 32 && split_layout(a.dmax, a.pmax, a.Rg, a.H, min_stages, a.CH).total > chunk_budget) a.CH >>= 1;
   a.S = kMaxStages;
-  while (a.S > 1 && split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S, a.CH).total > 227 * 1024) --a.S;
+  while (a.S > 1 && split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S, a.CH).total > smem_budget) --a.S;
   const size_t smem = split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S, a.CH).total;
   if (smem > 227 * 1024) { set_error("art_split_level: shared memory %zu too large", smem); return ART_E_UNSUPPORTED; }
   auto launch = [&](auto kern) -> int {
@@ -1519,9 +1532,15 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
     return check_launch("split_level");
   };
   int rc;
-  if (TC == 8) rc = launch(split_kernel<8>);
-  else if (TC == 4) rc = launch(split_kernel<4>);
-  else rc = launch(split_kernel<2>);
+  if (minb == 2) {
+    if (TC == 8) rc = launch(split_kernel<8, 2>);
+    else if (TC == 4) rc = launch(split_kernel<4, 2>);
+    else rc = launch(split_kernel<2, 2>);
+  } else {
+    if (TC == 8) rc = launch(split_kernel<8, 1>);
+    else if (TC == 4) rc = launch(split_kernel<4, 1>);
+    else rc = launch(split_kernel<2, 1>);
+  }
   if (rc) return rc;
   prof_begin("split_select", s);
   split_select<<<(unsigned)((K + 127) / 128), 128, 0, s>>>(a, *out);

@@ -208,6 +208,11 @@ typedef struct ArtSplitParams {
                                    (0: the largest that fits, <= 16)         */
   int32_t trial_steps;          /* Armijo step sizes evaluated per trial pass
                                    (0: min(4, 256 / group, backtracks + 1))  */
+  int32_t ctas_per_sm;          /* 0 or 1: one CTA per SM with the deepest row
+                                   ring; 2: two CTAs per SM, each with at most
+                                   110 KB of shared memory and 128 registers a
+                                   thread (falls back to 1 when the level's
+                                   layout does not fit)                      */
 } ArtSplitParams;
 
 typedef struct ArtSplitProblem {

@@ -50,18 +50,19 @@ def test_autotune_table_persists_and_is_keyed_by_device(tmp_path, monkeypatch):
     monkeypatch.setattr(autotune, "_LOADED", False)
     autotune.clear()
     try:
-        assert autotune.cached_split_shape(16, 17, 16) == (0, 0)
+        assert autotune.cached_split_shape(16, 17, 16) == (0, 0, 0)
         assert autotune.cached_ridge_choice() == (0, None)
-        autotune._store(autotune._split_key(16, 17, 16), {"group_restarts": 8, "trial_steps": 2})
+        autotune._store(autotune._split_key(16, 17, 16), {"group_restarts": 8, "trial_steps": 2,
+                                                                  "ctas_per_sm": 2})
         autotune._store(autotune._ridge_key(), {"tensor_min_features": 153, "fp64_factor": False})
         saved = json.loads(path.read_text())
         assert len(saved) == 2
         autotune.clear()
         monkeypatch.setattr(autotune, "_LOADED", False)
-        assert autotune.cached_split_shape(16, 17, 16) == (8, 2)       # reloaded from the file
+        assert autotune.cached_split_shape(16, 17, 16) == (8, 2, 2)    # reloaded from the file
         assert autotune.cached_ridge_choice() == (153, False)
         monkeypatch.setattr(autotune, "device_key", lambda: "other-device|sm132|cc9.0")
-        assert autotune.cached_split_shape(16, 17, 16) == (0, 0)       # another device: untuned
+        assert autotune.cached_split_shape(16, 17, 16) == (0, 0, 0)    # another device: untuned
     finally:
         autotune.clear()
 
@@ -73,9 +74,11 @@ def test_split_candidates_respect_thread_and_backtrack_limits(R, backtracks):
 
     cands = autotune.split_candidates(R, backtracks)
     assert cands and len(set(cands)) == len(cands)
-    for g, h in cands:
+    for g, h, c in cands:
         assert 1 <= g <= min(R, 16)
         assert 1 <= h <= min(32, 256 // g, backtracks + 1)
+        assert c in (1, 2) and (c == 1 or g <= 8)
+    assert {c for _, _, c in cands} == {1, 2}
 
 
 def test_graph_shape_classes_round_up_to_powers_of_two():

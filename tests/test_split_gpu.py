@@ -164,10 +164,10 @@ def test_public_split_api_matches_oracle():
                                rtol=1e-8, atol=1e-10)
 
 
-@pytest.mark.parametrize("shape", [(1, 1), (2, 4), (3, 32), (8, 2)])
+@pytest.mark.parametrize("shape", [(1, 1, 1), (2, 4, 2), (3, 32, 1), (8, 2, 1), (8, 2, 2)])
 def test_every_launch_shape_matches_oracle(shape):
-    """Restarts per CTA and trial steps per pass regroup the work (and the
-    summation order of row sums): each shape meets the per-node oracle check
+    """Restarts per CTA, trial steps per pass and CTAs per SM regroup the work
+    (and the summation order of row sums): each shape meets the per-node oracle check
     of the default shape."""
 
     from art.splitters import level_result_to_split, split_level
@@ -183,7 +183,8 @@ def test_every_launch_shape_matches_oracle(shape):
         parent.append(float(np.mean((y - phi @ b) ** 2)))
     ro = np.concatenate([[0], np.cumsum(ns)])
     res = split_level(s, np.concatenate([X.reshape(-1) for X in Xs]), np.concatenate(ys), ro, [4] * K, kd, T, lam,
-                      parent_loss=parent, theta0=th0, group_restarts=shape[0], trial_steps=shape[1])
+                      parent_loss=parent, theta0=th0, group_restarts=shape[0], trial_steps=shape[1],
+                      ctas_per_sm=shape[2])
     p = S.Params(max_iters=iters, n_restarts=R, min_side_points=5)
     picks = (res.flags.cpu().numpy() >> 8) & 255
     for k in range(K):
@@ -285,10 +286,12 @@ def test_per_node_min_side_equals_separate_calls():
                                               getattr(alone, name).cpu().numpy()[k], err_msg=f"{name} {k}")
 
 
-def test_gang_split_of_large_nodes_matches_oracle_and_is_batch_independent():
+@pytest.mark.parametrize("ctas_per_sm", [1, 2])
+def test_gang_split_of_large_nodes_matches_oracle_and_is_batch_independent(ctas_per_sm):
     """Nodes above 16,384 rows (one restart) are split by gangs of CTAs that
     add their pass sums in rank order: the result meets the per-node oracle
-    and is bit-identical whether the node is split alone or in a batch."""
+    and is bit-identical whether the node is split alone or in a batch, at
+    one or two resident CTAs per SM."""
 
     from art.splitters import level_result_to_split, split_level
 
@@ -302,7 +305,8 @@ def test_gang_split_of_large_nodes_matches_oracle_and_is_batch_independent():
     s = splitter_for(O.AFFINE, T, lam, 1, iters, {"min_side_points": 1})
     ro = np.concatenate([[0], np.cumsum(ns)])
     x, y = np.concatenate([X.reshape(-1) for X in Xs]), np.concatenate(ys)
-    res = split_level(s, x, y, ro, [d] * 3, [O.AFFINE] * 3, T, lam, parent_loss=[1.0] * 3, theta0=th0)
+    res = split_level(s, x, y, ro, [d] * 3, [O.AFFINE] * 3, T, lam, parent_loss=[1.0] * 3, theta0=th0,
+                      group_restarts=0, trial_steps=0, ctas_per_sm=ctas_per_sm)
     p = S.Params(max_iters=iters, n_restarts=1, min_side_points=1)
     for k in range(3):
         opt = S.optimize(Xs[k], ys[k], th0[k][0], T, O.AFFINE, lam, p)
@@ -311,7 +315,7 @@ def test_gang_split_of_large_nodes_matches_oracle_and_is_batch_independent():
         assert out.n_iters == opt["n_iters"]
     for k in (0, 2):
         alone = split_level(s, Xs[k].reshape(-1), ys[k], [0, ns[k]], [d], [O.AFFINE], T, lam, parent_loss=[1.0],
-                            theta0=th0[k:k + 1])
+                            theta0=th0[k:k + 1], group_restarts=0, trial_steps=0, ctas_per_sm=ctas_per_sm)
         for name in ("theta", "loss", "n_right", "n_iters", "beta"):
             np.testing.assert_array_equal(getattr(alone, name).cpu().numpy()[0],
                                           getattr(res, name).cpu().numpy()[k], err_msg=f"{name} {k}")
