@@ -14,7 +14,7 @@
 // advances one chain; lane l owns coordinates 2l and 2l+1, so one Philox
 // block gives both of its normals.  Box rows (+e_i, -e_i) are applied
 // structurally: A u = +-u_i exactly, as in the reference's dense matmul.
-// Oblique rows are held in registers and reduced across the team.
+// Oblique rows are held in shared memory and reduced across the team.
 #include <algorithm>
 #include "common.cuh"
 
@@ -78,8 +78,13 @@ __device__ __forceinline__ int team_or(int v) {
 template <int L, int MAXK>
 __host__ __device__ constexpr size_t har_team_stride(int d) { return (size_t)MAXK * d + 1; }
 
+// Teams of 4 or more lanes on polytopes of up to 16 rows are held to two
+// resident CTAs per SM (128 registers a thread); narrower teams and longer
+// row lists take the registers they need.
+constexpr int har_min_ctas(int L, int MAXK) { return (L >= 4 && MAXK <= 16) ? 2 : 1; }
+
 template <int L, int MAXK>
-__global__ void __launch_bounds__(kHarThreads) har_kernel(HarArgs a) {
+__global__ void __launch_bounds__(kHarThreads, har_min_ctas(L, MAXK)) har_kernel(HarArgs a) {
   extern __shared__ double s_rows[];
   constexpr int OWN = (MAXK + L - 1) / L;  // rows owned by each lane
   const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -141,12 +146,21 @@ __global__ void __launch_bounds__(kHarThreads) har_kernel(HarArgs a) {
     }
   }
   bad_start = team_or<L>(bad_start);
+  const int kwarp = __reduce_max_sync(0xffffffffu, status == 0 ? k : 0);
   if (bad_start && status == 0) status = 2;
   const uint32_t key0 = a.seeds ? (uint32_t)a.seeds[chain] : 0u;
   const uint32_t key1 = a.seeds ? (uint32_t)(a.seeds[chain] >> 32) : 0u;
   const int total = a.burn_in + a.n_rounds * a.thinning;
   const int64_t C = a.n_chains;
   int64_t ucur = 0;  // uniform cursor (scalar mode skips draws on zero directions)
+  // next step that keeps a sample and its index: scalar mode keeps steps
+  // burn_in + j * thinning (none on a zero direction), batched mode the last
+  // step of each thinning block after burn_in
+  int keep_step = scalar ? a.burn_in : a.burn_in + a.thinning - 1;
+  int keep_idx = 0;
+  // one step per iteration: the body is long, and unrolling it only grows the
+  // code the warps fetch
+#pragma unroll 1
   for (int step = 0; step < total; ++step) {
     double u0, u1;
     if (a.dirs) {
@@ -188,8 +202,11 @@ __global__ void __launch_bounds__(kHarThreads) har_kernel(HarArgs a) {
         if (r % L == lane) so[r / L] = br[r / L] - ax;
       }
     }
+    // rows past the largest count in the warp are zero: skip them (a
+    // warp-uniform bound, so the team shuffles stay converged)
 #pragma unroll
     for (int r = 0; r < MAXK; ++r) {
+      if (r >= kwarp) break;
       const double v = team_sum<L>(arow(r, u0, u1));
       if (r % L == lane) au[r / L] = v;
     }
@@ -206,9 +223,13 @@ __global__ void __launch_bounds__(kHarThreads) har_kernel(HarArgs a) {
         if (h0) { box_row(shi0, u0); box_row(slo0, -u0); }
         if (h1) { box_row(shi1, u1); box_row(slo1, -u1); }
       }
+      // each lane walks only the rows it owns (r = m L + lane); min and max
+      // do not depend on the order
 #pragma unroll
-      for (int r = 0; r < MAXK; ++r)
-        if (r < k && r % L == lane) box_row(so[r / L], au[r / L]);
+      for (int m = 0; m < OWN; ++m) {
+        const int r = m * L + lane;
+        if (r < MAXK && r < k) box_row(so[m], au[m]);
+      }
       tlo = team_max<L>(tlo);
       thi = team_min<L>(thi);
       infeasible = team_or<L>(infeasible);
@@ -240,11 +261,10 @@ __global__ void __launch_bounds__(kHarThreads) har_kernel(HarArgs a) {
     }
     // sample bookkeeping
     int out = -1;
-    if (scalar) {
-      if (!skip && step >= a.burn_in && (step - a.burn_in) % a.thinning == 0)
-        out = (step - a.burn_in) / a.thinning;
-    } else if (step >= a.burn_in && (step - a.burn_in + 1) % a.thinning == 0) {
-      out = (step - a.burn_in + 1) / a.thinning - 1;
+    if (step == keep_step) {
+      if (!(scalar && skip)) out = keep_idx;
+      ++keep_idx;
+      keep_step += a.thinning;
     }
     if (out >= 0 && out < a.n_rounds && live) {
       double* sp = a.samples + ((int64_t)out * C + chain) * d;

@@ -1271,7 +1271,6 @@ __global__ void split_init_theta(SplitArgs a, double* theta0, int64_t stride) {
   const int64_t r0 = a.row_offsets[k], n = a.row_offsets[k + 1] - r0;
   const int64_t xoff = a.x_offsets[k];
   __shared__ double w[ART_MAX_DIM + 1];
-  __shared__ double s_lo, s_hi;
   if (threadIdx.x == 0) {
     double nrm2 = 0.0;
     // counter: (node k, restart) or, with per-node keys, (restart, node key):

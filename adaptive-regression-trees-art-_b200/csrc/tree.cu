@@ -21,7 +21,7 @@ __global__ void __launch_bounds__(kPartThreads)
   const int d = seg.dims[k];
   const bool do_split = split == nullptr || split[k] != 0;
   __shared__ double w[ART_MAX_DIM + 1];
-  __shared__ int64_t s_base_left, s_base_right, s_total_right;
+  __shared__ int64_t s_base_left, s_base_right;
   __shared__ int warp_tot[kPartThreads / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int i = tid; i <= d; i += kPartThreads) w[i] = theta[(int64_t)k * ts + i];
@@ -39,7 +39,6 @@ __global__ void __launch_bounds__(kPartThreads)
   if (tid == 0) {
     int64_t t = 0;
     for (int i = 0; i < kPartThreads / 32; ++i) t += warp_tot[i];
-    s_total_right = t;
     s_base_left = 0;
     s_base_right = n - t;
     if (n_right) n_right[k] = (int32_t)t;

@@ -186,3 +186,36 @@ def test_device_draws_with_covariance_shaped_directions():
     assert np.median(np.abs(sy @ Q[:, 1]) / np.linalg.norm(sy, axis=1)) > 0.3
     again = aniso.sample(region, 4000, random_state=3, x0=np.zeros(2))
     np.testing.assert_array_equal(X, again)
+
+
+@pytest.mark.parametrize("d", [3, 8, 16, 32])
+def test_chains_of_mixed_row_counts_share_warps_with_injected_draws(d):
+    """Teams of one warp run polytopes of 0 to 16 oblique rows (the row loop
+    stops at the warp's largest count; each lane bounds only its own rows):
+    every chain equals the oracle's batched transition on the same draws."""
+    from art.sampling import device_polytopes, hit_and_run_device
+
+    rng = np.random.default_rng(70 + d)
+    regs, starts = [], []
+    for j in range(40):
+        k = int(rng.integers(0, 17)) if j % 5 else 0
+        c = rng.uniform(-0.5, 0.5, d)
+        A = rng.normal(size=(k, d))
+        A /= np.maximum(np.linalg.norm(A, axis=1, keepdims=True), 1e-12)
+        b = A @ c + rng.uniform(0.05, 0.5, k)
+        Ab, bb = H.box_rows(*box(d))
+        regs.append((np.vstack([Ab, A]), np.concatenate([bb, b])))
+        starts.append(c)
+    C, steps = 96, 24
+    cp = rng.permutation(np.arange(C) % len(regs)).astype(np.int32)
+    x0 = np.array(starts)[cp]
+    dirs, unif = rng.normal(size=(C, steps, d)), rng.uniform(size=(C, steps))
+    samples, last, status = hit_and_run_device(device_polytopes(regs), cp, x0, burn_in=0, thinning=3,
+                                               n_rounds=steps // 3, mode="batched", directions=dirs,
+                                               uniforms=unif)
+    assert (status.cpu().numpy() == 0).all()
+    S = samples.cpu().numpy()
+    for c in range(C):
+        A, b = regs[cp[c]]
+        ref, _ = H.chains_batched(A, b, x0[c:c + 1], dirs[c:c + 1], unif[c:c + 1], 0, 3, steps // 3)
+        np.testing.assert_allclose(S[:, c, :], ref[:, 0, :], rtol=1e-12, atol=1e-12, err_msg=f"chain {c}")
