@@ -10,6 +10,11 @@ namespace art {
 
 __host__ __device__ __forceinline__ int pk(int i, int j) { return i * (i + 1) / 2 + j; }
 
+// 1 / v rounded to nearest: the same value as the division, with the
+// reciprocal intrinsics
+__device__ __forceinline__ float recip_rn(float v) { return __frcp_rn(v); }
+__device__ __forceinline__ double recip_rn(double v) { return __drcp_rn(v); }
+
 // Blocked right-looking Cholesky of the leading p x p block of packed A
 // (in place, lower factor).  All threads of the block must call it.  Returns
 // 0 or the 1-based index of the first pivot that was not positive (the
@@ -127,6 +132,11 @@ __device__ int chol_packed(T* A, int p, int* s_fail) {
 template <typename T>
 __device__ int chol_packed32(T* A, int p, int* s_fail) {
   constexpr int NB = 32, CT = 8;
+  // single precision (the preconditioner of the mixed form): pivots from the
+  // hardware reciprocal square root, columns scaled by it, the panel solve
+  // multiplied by the stored reciprocals; double precision divides exactly
+  constexpr bool kFast = sizeof(T) == 4;
+  __shared__ T s_inv[NB];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nthreads = blockDim.x;
   if (tid == 0) *s_fail = 0;
@@ -142,16 +152,24 @@ __device__ int chol_packed32(T* A, int p, int* s_fail) {
       for (int c = 0; c < NB; ++c) {
         if (c < jb && !fail) {
           const T dc = __shfl_sync(0xffffffffu, row[c], c);
-          if (!(dc > T(0)) || !isfinite((double)dc)) {
+          if (!(dc > T(0) && dc < T(INFINITY))) {  // not positive, or not finite
             fail = j0 + c + 1;
           } else {
-            const T lcc = sqrt(dc);
-            if (lane == c) row[c] = lcc;
-            else if (lane > c && lane < jb) row[c] = row[c] / lcc;
+            // no per-lane masks: rows and columns past jb are zero and stay
+            // zero, and entries above the diagonal (lane < k) are updated
+            // but never stored or read
+            if constexpr (kFast) {
+              const T inv = rsqrtf(dc);
+              row[c] = lane == c ? dc * inv : row[c] * inv;
+              if (lane == c) s_inv[c] = inv;
+            } else {
+              const T lcc = sqrt(dc);
+              row[c] = lane == c ? lcc : row[c] / lcc;
+            }
 #pragma unroll
             for (int k = c + 1; k < NB; ++k) {
               const T lkc = __shfl_sync(0xffffffffu, row[c], k);
-              if (k < jb && lane >= k && lane < jb) row[k] -= row[c] * lkc;
+              row[k] = fma(-row[c], lkc, row[k]);
             }
           }
         }
@@ -179,7 +197,8 @@ __device__ int chol_packed32(T* A, int p, int* s_fail) {
 #pragma unroll
           for (int k = 0; k < NB; ++k)
             if (k < c) sacc -= a[k] * lr[k];
-          a[c] = sacc / lr[c];
+          if constexpr (kFast) a[c] = sacc * s_inv[c];
+          else a[c] = sacc / lr[c];
         }
       }
 #pragma unroll
@@ -262,7 +281,7 @@ __device__ void tri_inv_packed32(T* A, int p, T* Y) {
 #pragma unroll
         for (int k = 0; k < NB; ++k)
           if (k < i) s = fma(row[k], x[k], s);
-        const T inv_d = T(1) / row[i];
+        const T inv_d = recip_rn(row[i]);
         x[i] = (i == lane) ? inv_d : (i > lane ? -s * inv_d : T(0));
       } else {
         x[i] = T(0);

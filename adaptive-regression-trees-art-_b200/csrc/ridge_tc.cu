@@ -7,8 +7,9 @@
 //     split it into TF32 hi + lo parts (hi = rna(v), lo = rna(v - hi): about
 //     22 significant bits together) and store both in the K-major
 //     core-matrix layout (8 rows x 16 bytes per core matrix, no swizzle).
-//     The same threads accumulate the exact FP64 h = Phi^T (q y) and
-//     diag(G) = sum q phi^2 (for the trace-scaled ridge, models.py:271).
+//     The same threads accumulate the FP64 h = sum phi (q y) and
+//     diag(G) = sum (sqrt(q) phi)^2 (for the trace-scaled ridge,
+//     models.py:271), one rounding per term.
 //  2. One thread issues tcgen05.mma kind::tf32 (TF32 x TF32 -> FP32 in TMEM):
 //     G' = Hi Hi^T + Hi Lo^T + Lo Hi^T with M = 128 feature rows per tile
 //     (tile 1: features 0..127 x 0..P16-1; tile 2 covers features >= 128),
@@ -168,7 +169,7 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
   TF* Gf = (TF*)(smem + lay.gram);
   double* vec = (double*)(smem + lay.vec);
   int16_t* fidx = (int16_t*)(smem + lay.fidx);
-  double* sq_q = (double*)(smem + lay.q);
+  double* sq_qy = (double*)(smem + lay.q);  // q_r y_r of the chunk's rows
   double* sq_s = (double*)(smem + lay.sq);
   unsigned char* op = smem + lay.op;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -235,6 +236,31 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
     for (int64_t c = 0; c < nchunks && !abort; ++c) {
       const int st = (int)(c & 1);
       const bool okl = mbar_wait(&load_bar[st], S.load_uses[st] & 1);
+      const int rows = (int)min((int64_t)kKC, it.n - c * kKC);
+      const double* xs = (const double*)(smem + lay.x[st] +
+                                         (((uintptr_t)(a.x + it.xoff + c * kKC * d)) & 15));
+      const double* ys = (const double*)(smem + lay.y[st] +
+                                         (((uintptr_t)(a.y + it.r0 + c * kKC)) & 15));
+      const double* ws = a.w ? (const double*)(smem + lay.w[st] +
+                                               (((uintptr_t)(a.w + it.r0 + c * kKC)) & 15))
+                             : nullptr;
+      // input checks and the per-row q y and sqrt(q) need only this chunk's
+      // rows, so they run while the tensor core may still hold the operand
+      // buffer (the previous chunk's generation finished reading them)
+      if (okl) {
+        for (int e = tid; e < rows * d; e += kTcThreads) bad |= isfinite(xs[e]) ? 0 : 1;
+        if (tid < kKC) {
+          double qv = 0.0;
+          if (tid < rows) {
+            bad |= isfinite(ys[tid]) ? 0 : 1;
+            const double wv = ws ? ws[tid] : 1.0;
+            if (!(wv >= 0.0) || !isfinite(wv)) bad |= 2;
+            qv = fmax(wv, a.weight_floor);
+          }
+          sq_qy[tid] = tid < rows ? qv * ys[tid] : 0.0;
+          sq_s[tid] = sqrt(qv);
+        }
+      }
       // one operand buffer: every MMA issued so far (chunks c-2 on barrier st,
       // c-1 on barrier st^1) must be done before it is rewritten; a drain
       // since then has already consumed those commits
@@ -246,27 +272,6 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
       S.load_uses[st]++;
       if (p0) S.mma_waits[st]++;
       if (p1) S.mma_waits[st ^ 1]++;
-      const int rows = (int)min((int64_t)kKC, it.n - c * kKC);
-      const double* xs = (const double*)(smem + lay.x[st] +
-                                         (((uintptr_t)(a.x + it.xoff + c * kKC * d)) & 15));
-      const double* ys = (const double*)(smem + lay.y[st] +
-                                         (((uintptr_t)(a.y + it.r0 + c * kKC)) & 15));
-      const double* ws = a.w ? (const double*)(smem + lay.w[st] +
-                                               (((uintptr_t)(a.w + it.r0 + c * kKC)) & 15))
-                             : nullptr;
-      for (int e = tid; e < rows * d; e += kTcThreads) bad |= isfinite(xs[e]) ? 0 : 1;
-      if (tid < kKC) {
-        double qv = 0.0;
-        if (tid < rows) {
-          bad |= isfinite(ys[tid]) ? 0 : 1;
-          const double wv = ws ? ws[tid] : 1.0;
-          if (!(wv >= 0.0) || !isfinite(wv)) bad |= 2;
-          qv = fmax(wv, a.weight_floor);
-        }
-        sq_q[tid] = qv;
-        sq_s[tid] = sqrt(qv);
-      }
-      __syncthreads();
       unsigned char* hi = op;
       unsigned char* lo = hi + kOpBytes;
       const int nitems = P16 * (kKC / 8);
@@ -284,10 +289,12 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
             if (r < rows && ia != -3) {
               const double* xr = xs + (int64_t)r * d;
               const double phi = (ia < 0 ? 1.0 : xr[ia]) * (ib < 0 ? 1.0 : xr[ib]);
-              const double qphi = sq_q[r] * phi;
-              hacc[s] = fma(qphi, ys[r], hacc[s]);
-              dacc[s] = fma(qphi, phi, dacc[s]);
-              v = (float)(sq_s[r] * phi);
+              // h += phi (q y) and diag += (sqrt(q) phi)^2: one product fewer
+              // and no separate y load per feature
+              const double sphi = sq_s[r] * phi;
+              hacc[s] = fma(phi, sq_qy[r], hacc[s]);
+              dacc[s] = fma(sphi, sphi, dacc[s]);
+              v = (float)sphi;
             }
             ph[e] = to_tf32(v);
             pl[e] = to_tf32(v - __uint_as_float(ph[e]));
