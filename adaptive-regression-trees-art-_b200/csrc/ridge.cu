@@ -106,6 +106,18 @@ struct Fp64Layout {
 
 __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 
+// Position of feature blk*TS + j in a row of the sqrt(q)*phi tile, and the
+// row stride for nb feature blocks.  Within a block the entries rotate by
+// the block index; for TS = 4, blocks are also shifted by 2 words per group
+// of four, so that, for any j, blocks 0..11 (every tile row or column index
+// a warp reads in one load) fall on 12 distinct 8-byte bank pairs.  (The
+// same kind of shift for TS = 8 measured slower and is not used.)
+__host__ __device__ inline int phi_skew(int ts, int blk) { return ts == 4 ? 2 * (blk >> 2) : 0; }
+__host__ __device__ inline int phi_pos(int ts, int blk, int j) {
+  return blk * ts + phi_skew(ts, blk) + ((j + blk) & (ts - 1));
+}
+__host__ __device__ inline int phi_stride(int ts, int nb) { return nb * ts + phi_skew(ts, nb + ts - 1); }
+
 __host__ __device__ inline Fp64Layout fp64_layout(int pmax, int dmax, int ts, int chunk) {
   Fp64Layout L;
   const int pa = pmax + 1;
@@ -118,7 +130,7 @@ __host__ __device__ inline Fp64Layout fp64_layout(int pmax, int dmax, int ts, in
     L.off_w[s] = o; o = align16(o + (size_t)chunk * 8 + 16);
   }
   L.off_bar = o; o = align16(o + 2 * 8);
-  L.off_phi = o; o = align16(o + (size_t)chunk * L.ldp * 8);
+  L.off_phi = o; o = align16(o + (size_t)chunk * phi_stride(ts, L.ldp / ts) * 8);
   L.off_q = o; o = align16(o + (size_t)chunk * 8);
   L.off_gram = o; o = align16(o + (size_t)pa * (pa + 1) / 2 * 8);
   L.off_fa = o; o = align16(o + (size_t)L.ldp * 2);
@@ -176,7 +188,8 @@ __global__ void __launch_bounds__(kRidgeThreads) ridge_fp64_kernel(RidgeArgs a, 
     const RidgeItem it = load_item(a, k);
     const int p = it.p, pa = p + 1, d = it.d;
     const int nb = (pa + TS - 1) / TS;
-    const int ldpi = nb * TS;
+    const int ldpi = nb * TS;              // features incl. padding
+    const int lds = phi_stride(TS, nb);    // phi row stride
     const int T = nb * (nb + 1) / 2;
     const int S = max(1, kRidgeThreads / T);
     for (int f = tid; f < ldpi; f += kRidgeThreads) {
@@ -228,8 +241,8 @@ __global__ void __launch_bounds__(kRidgeThreads) ridge_fp64_kernel(RidgeArgs a, 
         q[r] = sqrt(fmax(wv, a.weight_floor));
       }
       __syncthreads();
-      // phi[r][blk*TS + (j + blk) % TS] = sqrt(q_r) * feature(blk*TS + j): the
-      // per-block rotation spreads the lanes' loads over distinct banks.
+      // phi[r][phi_pos(blk, j)] = sqrt(q_r) * feature(blk*TS + j): the
+      // rotation and shift spread the tiles' loads over distinct banks.
       const int warp = tid >> 5, lane = tid & 31;
       for (int r = warp; r < rows; r += kRidgeThreads / 32) {
         const double* xr = xs + (int64_t)r * d;
@@ -241,19 +254,19 @@ __global__ void __launch_bounds__(kRidgeThreads) ridge_fp64_kernel(RidgeArgs a, 
           else if (ia == -2) v = sq * ys[r];
           else v = sq * ((ia < 0 ? 1.0 : xr[ia]) * (ib < 0 ? 1.0 : xr[ib]));
           const int blk = f / TS, j = f - blk * TS;
-          phi[r * ldpi + blk * TS + ((j + blk) & (TS - 1))] = v;
+          phi[r * lds + phi_pos(TS, blk, j)] = v;
         }
       }
       __syncthreads();
       if (tid == 0 && c + 2 < nchunks) issue_chunk(a, it, CHUNK, c + 2, smem, lay, st, &bars[st]);
       if (mine) {
         for (int r = slice; r < rows; r += S) {
-          const double* pr = phi + r * ldpi;
+          const double* pr = phi + r * lds;
           double av[TS], bv[TS];
 #pragma unroll
-          for (int i = 0; i < TS; ++i) av[i] = pr[I * TS + ((i + I) & (TS - 1))];
+          for (int i = 0; i < TS; ++i) av[i] = pr[phi_pos(TS, I, i)];
 #pragma unroll
-          for (int j = 0; j < TS; ++j) bv[j] = pr[J * TS + ((j + J) & (TS - 1))];
+          for (int j = 0; j < TS; ++j) bv[j] = pr[phi_pos(TS, J, j)];
 #pragma unroll
           for (int i = 0; i < TS; ++i)
 #pragma unroll
