@@ -261,6 +261,7 @@ def solve_weighted_ridge_batched(
     tensor_min_features: int | None = None,
     out: BatchedRidgeResult | None = None,
     stream=None,
+    host_slices: int | None = None,
 ) -> BatchedRidgeResult:
     """Solve K weighted ridge systems in one stream-ordered launch sequence.
 
@@ -276,11 +277,33 @@ def solve_weighted_ridge_batched(
     solves on the tensor cores (smaller systems take the FP64 kernels); None
     takes the autotuned choice for this device and batch, else the library
     default (33).
+    ``host_slices``: when ``x`` is in host memory (numpy, or a CPU tensor;
+    pinned for the copies to run asynchronously) and the systems' rows are
+    stored back to back, the batch is cut into this many slices of
+    contiguous systems of about equal rows.  Each slice's host-to-device
+    copy runs on a side stream while the previous slice is solved, so the
+    copies and the solves overlap.  None picks 8 for host inputs of at least
+    64 MB and 1 (one copy, then one solve) otherwise.  Results do not depend
+    on the slicing.
     """
 
     t = torch()
     lib = N.load_library()
     dev = require_cuda()
+    slices = host_slices
+    on_host = isinstance(x, np.ndarray) or (isinstance(x, t.Tensor) and x.device.type == "cpu")
+    if slices is None:
+        nbytes_x = int(x.nbytes) if isinstance(x, np.ndarray) else (int(x.numel() * x.element_size()) if on_host else 0)
+        slices = 8 if on_host and nbytes_x >= (64 << 20) else 1
+    if on_host and int(slices) > 1:
+        staged = _solve_host_staged(
+            x, y, weights, row_offsets, dims, features, ridge, x_offsets, int(slices), stream,
+            dict(weight_floor=weight_floor, solver=solver, precision=precision,
+                 auto_rcond_threshold=auto_rcond_threshold, max_features=max_features, max_dim=max_dim,
+                 condition=condition, fp64_factor=fp64_factor, tensor_min_features=tensor_min_features),
+            out)
+        if staged is not None:
+            return staged
     if solver == "svd":
         raise NotImplementedError("solver='svd' (LAPACK gelsd) is not part of the B200 path.")
     if solver not in _SOLVER_CODES:
@@ -337,6 +360,122 @@ def solve_weighted_ridge_batched(
     N.check(rc, "art_ridge_batched")
     # keep inputs alive until the stream has consumed them
     out._keepalive = (x, y, w, ro, xo, dims_t, feats, ridge_t)
+    return out
+
+
+_COPY_STREAMS: dict[int, object] = {}
+
+
+def _host_array(a, t, dtype):
+    """numpy / torch CPU -> CPU torch tensor (no copy when already suitable)."""
+
+    if isinstance(a, t.Tensor):
+        return a.to(dtype=dtype).contiguous()
+    return t.from_numpy(np.ascontiguousarray(a, dtype=_NP_OF[dtype]))
+
+
+_NP_OF: dict = {}
+
+
+def host_slice_bounds(row_offsets, x_offsets, dims, slices: int):
+    """System boundaries [0, k1, ..., K] of up to ``slices`` slices with about
+    equal rows, or None when the layout cannot be staged in slices: fewer
+    than two systems, or rows / x blocks not stored back to back from 0."""
+
+    ro = np.asarray(row_offsets, dtype=np.int64)
+    xo = np.asarray(x_offsets, dtype=np.int64)
+    d = np.asarray(dims, dtype=np.int64)
+    K = int(d.size)
+    if K < 2 or slices < 2 or ro.size != K + 1 or xo.size != K:
+        return None
+    ends = xo + np.diff(ro) * d
+    if ro[0] != 0 or xo[0] != 0 or np.any(np.diff(ro) < 0) or not np.array_equal(xo[1:], ends[:-1]):
+        return None
+    cuts = np.searchsorted(ro, np.linspace(0, ro[-1], slices + 1)[1:-1], side="left")
+    return np.unique(np.concatenate([[0], np.clip(cuts, 1, K - 1), [K]])).astype(np.int64)
+
+
+def _solve_host_staged(x, y, weights, row_offsets, dims, features, ridge, x_offsets, slices, stream, kw, out):
+    """Overlapped host-to-device staging for solve_weighted_ridge_batched.
+
+    Returns None (the caller then copies everything at once) when the
+    systems' rows and x blocks are not stored back to back from offset 0.
+    """
+
+    t = torch()
+    dev = require_cuda()
+    if not _NP_OF:
+        _NP_OF.update({t.float64: np.float64, t.int64: np.int64, t.int32: np.int32})
+    ro_h = np.asarray(row_offsets.cpu() if isinstance(row_offsets, t.Tensor) else row_offsets, dtype=np.int64)
+    dims_h = np.asarray(dims.cpu() if isinstance(dims, t.Tensor) else dims, dtype=np.int64)
+    feats_h = np.asarray(features.cpu() if isinstance(features, t.Tensor) else features, dtype=np.int32)
+    K = int(dims_h.size)
+    if ro_h.size != K + 1:
+        return None
+    xo_h = (ro_h[:-1] * dims_h if x_offsets is None else
+            np.asarray(x_offsets.cpu() if isinstance(x_offsets, t.Tensor) else x_offsets, dtype=np.int64))
+    bounds = host_slice_bounds(ro_h, xo_h, dims_h, slices)
+    if bounds is None:
+        return None
+    ends = xo_h + np.diff(ro_h) * dims_h
+    xh = _host_array(x, t, t.float64)
+    yh = _host_array(y, t, t.float64)
+    wh = None if weights is None else _host_array(weights, t, t.float64)
+    if xh.numel() < int(ends[-1]) or yh.numel() < int(ro_h[-1]) or (wh is not None and wh.numel() < int(ro_h[-1])):
+        raise ValueError("x, y and weights must cover every system's rows")
+    if kw.get("max_dim") is None:
+        kw["max_dim"] = int(dims_h.max())
+    if kw.get("max_features") is None:
+        kw["max_features"] = max(kind_feature_count(int(d), int(f)) for d, f in zip(dims_h, feats_h))
+    comp = t.cuda.current_stream(dev) if stream is None else stream
+    copy = _COPY_STREAMS.get(dev.index)
+    if copy is None:
+        copy = _COPY_STREAMS[dev.index] = t.cuda.Stream(device=dev)
+    with t.cuda.stream(comp):
+        xd = t.empty(xh.numel(), dtype=t.float64, device=dev)
+        yd = t.empty(yh.numel(), dtype=t.float64, device=dev)
+        wd = None if wh is None else t.empty(wh.numel(), dtype=t.float64, device=dev)
+        ro_d = t.from_numpy(ro_h).to(dev)
+        xo_d = t.from_numpy(xo_h).to(dev)
+        dims_d = t.from_numpy(dims_h.astype(np.int32)).to(dev)
+        feats_d = t.from_numpy(feats_h).to(dev)
+        ridge_d = to_device(np.broadcast_to(np.asarray(ridge, dtype=float), (K,)).copy()
+                            if not isinstance(ridge, t.Tensor) else ridge, t.float64, dev)
+        if ridge_d.numel() == 1:
+            ridge_d = ridge_d.expand(K).contiguous()
+        if out is None:
+            pm = int(kw["max_features"])
+            cond = kw.get("condition") or kw.get("solver") == "auto"
+            out = BatchedRidgeResult(
+                beta=t.full((K, pm), float("nan"), dtype=t.float64, device=dev),
+                ridge_effective=t.empty(K, dtype=t.float64, device=dev),
+                cond_estimate=t.empty(K, dtype=t.float64, device=dev) if cond else None,
+                status=t.empty(K, dtype=t.int32, device=dev),
+                info=t.empty(K, dtype=t.int32, device=dev),
+            )
+    for buf in (xd, yd, wd):
+        if buf is not None:
+            buf.record_stream(copy)
+    copy.wait_stream(comp)
+    pinned = xh.is_pinned()
+    for k0, k1 in zip(bounds[:-1].tolist(), bounds[1:].tolist()):
+        r0, r1, e0, e1 = int(ro_h[k0]), int(ro_h[k1]), int(xo_h[k0]), int(ends[k1 - 1])
+        with t.cuda.stream(copy):
+            xd[e0:e1].copy_(xh[e0:e1], non_blocking=pinned)
+            yd[r0:r1].copy_(yh[r0:r1], non_blocking=pinned)
+            if wd is not None:
+                wd[r0:r1].copy_(wh[r0:r1], non_blocking=pinned)
+            ev = t.cuda.Event()
+            ev.record(copy)
+        comp.wait_event(ev)
+        part = BatchedRidgeResult(
+            beta=out.beta[k0:k1], ridge_effective=out.ridge_effective[k0:k1],
+            cond_estimate=None if out.cond_estimate is None else out.cond_estimate[k0:k1],
+            status=out.status[k0:k1], info=out.info[k0:k1])
+        solve_weighted_ridge_batched(xd, yd, wd, ro_d[k0:k1 + 1], dims_d[k0:k1], feats_d[k0:k1], ridge_d[k0:k1],
+                                     x_offsets=xo_d[k0:k1], out=part, stream=comp, host_slices=1, **kw)
+    # the host buffers must outlive the queued copies
+    out._keepalive = (xh, yh, wh, xd, yd, wd, ro_d, xo_d, dims_d, feats_d, ridge_d)
     return out
 
 

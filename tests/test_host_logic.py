@@ -1,11 +1,13 @@
 """Host-side logic that needs no GPU: the ctypes mirror of the C ABI structs,
-the autotuner's persistent table and candidate lists, and graph shape classes."""
+the autotuner's persistent table and candidate lists, graph shape classes, and
+the slice boundaries of overlapped host staging."""
 
 import ctypes as C
 import json
 import subprocess
 import sys
 
+import numpy as np
 import pytest
 
 from conftest import ROOT
@@ -87,3 +89,25 @@ def test_graph_shape_classes_round_up_to_powers_of_two():
 
     assert [_pow2(v, 8) for v in (0, 1, 8, 9, 16, 17, 1000)] == [8, 8, 8, 16, 16, 32, 1024]
     assert _pow2(5000, 4096) == 8192 and _pow2(10, 4096) == 4096
+
+
+def test_host_slice_bounds_cut_at_system_edges_with_equal_rows():
+    sys.path.insert(0, str(ROOT / "adaptive-regression-trees-art-_b200"))
+    from art.models import host_slice_bounds
+
+    rng = np.random.default_rng(3)
+    n = rng.integers(1, 500, 1000)
+    d = rng.integers(1, 17, 1000)
+    ro = np.concatenate([[0], np.cumsum(n)])
+    xo = np.concatenate([[0], np.cumsum(n * d)[:-1]])
+    b = host_slice_bounds(ro, xo, d, 8)
+    assert b[0] == 0 and b[-1] == 1000 and np.all(np.diff(b) > 0) and len(b) == 9
+    rows = np.diff(ro[b])
+    assert rows.max() < 1.2 * ro[-1] / 8                       # about equal shares of the rows
+    assert host_slice_bounds(ro, xo, d, 1) is None               # one slice: no staging
+    assert host_slice_bounds(ro[:2], xo[:1], d[:1], 8) is None   # one system
+    gap = xo.copy(); gap[5:] += 3                                # x blocks not back to back
+    assert host_slice_bounds(ro, gap, d, 8) is None
+    assert host_slice_bounds(ro + 4, xo, d, 8) is None           # rows not from 0
+    few = host_slice_bounds(ro[:4], xo[:3], d[:3], 8)            # more slices than systems
+    assert few[0] == 0 and few[-1] == 3 and np.all(np.diff(few) > 0)

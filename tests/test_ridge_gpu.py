@@ -354,3 +354,32 @@ def test_autotuned_threshold_is_stored_and_used():
         _oracle_check(wl, out)
     finally:
         autotune.clear()
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_host_inputs_staged_in_slices_equal_one_copy(precision):
+    """Host (pinned) inputs cut into slices whose copies overlap the solves
+    give exactly the coefficients and statuses of one copy followed by one
+    solve, and of device-resident inputs."""
+    import torch
+
+    from art import _native as N
+    from art import workloads
+    from art.models import solve_weighted_ridge_batched
+
+    wl = workloads.ridge_systems(600, seed=9, n_min=32, n_max=900)
+    hx, hy, hw = (torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (wl.x, wl.y, wl.w))
+    args = (wl.row_offsets, wl.dims, wl.kinds, wl.ridge)
+    kw = dict(x_offsets=wl.x_offsets, precision=precision, max_features=wl.max_features, max_dim=wl.max_dim,
+              tensor_min_features=45)
+    one = solve_weighted_ridge_batched(hx, hy, hw, *args, host_slices=1, **kw)
+    staged = solve_weighted_ridge_batched(hx, hy, hw, *args, host_slices=7, **kw)
+    dev = solve_weighted_ridge_batched(hx.cuda(), hy.cuda(), hw.cuda(), *args, **kw)
+    for res in (staged, dev):
+        np.testing.assert_array_equal(res.status.cpu().numpy(), one.status.cpu().numpy())
+        np.testing.assert_array_equal(res.beta.cpu().numpy(), one.beta.cpu().numpy())
+        np.testing.assert_array_equal(res.ridge_effective.cpu().numpy(), one.ridge_effective.cpu().numpy())
+    assert (one.status.cpu().numpy() == 0).mean() > 0.95
+    # numpy inputs take the same staged path (synchronous copies)
+    np_staged = solve_weighted_ridge_batched(wl.x, wl.y, wl.w, *args, host_slices=3, **kw)
+    np.testing.assert_array_equal(np_staged.beta.cpu().numpy(), one.beta.cpu().numpy())
