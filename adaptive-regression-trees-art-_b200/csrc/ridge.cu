@@ -13,7 +13,9 @@
 //       cost first (log2 buckets of n*(p+1)^2), built on the device;
 //   [mixed] ridge_tc_kernel                : tcgen05 Gram + refinement;
 //   ridge_warp_kernel                      : FP64, (p+1) <= 24, warp per system;
-//   ridge_fp64_kernel<4>, <8>              : persistent FP64 work queues;
+//   ridge_fp64_kernel<4>, <8>              : persistent FP64 work queues
+//       (<4>: Gram on the FP64 tensor cores, mma.sync m8n8k4; <8>: 8x8
+//       FP64 register tiles);
 //   ridge_fp64_kernel<8> on the resolve list (mixed systems that did not
 //       converge); ridge_qr_kernel on the auto-solver fallback list.
 #include <stdarg.h>
@@ -106,22 +108,34 @@ struct Fp64Layout {
 
 __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 
-// Position of feature blk*TS + j in a row of the sqrt(q)*phi tile, and the
-// row stride for nb feature blocks.  Within a block the entries rotate by
-// the block index; for TS = 4, blocks are also shifted by 2 words per group
-// of four, so that, for any j, blocks 0..11 (every tile row or column index
-// a warp reads in one load) fall on 12 distinct 8-byte bank pairs.  (The
-// same kind of shift for TS = 8 measured slower and is not used.)
-__host__ __device__ inline int phi_skew(int ts, int blk) { return ts == 4 ? 2 * (blk >> 2) : 0; }
-__host__ __device__ inline int phi_pos(int ts, int blk, int j) {
-  return blk * ts + phi_skew(ts, blk) + ((j + blk) & (ts - 1));
+// Position of feature blk*TS + j in a row of the sqrt(q)*phi tile of the
+// 8x8 register-tile form, and its row stride: within a block the entries
+// rotate by the block index, which spreads a warp's loads over the banks.
+__host__ __device__ inline int phi_pos(int ts, int blk, int j) { return blk * ts + ((j + blk) & (ts - 1)); }
+__host__ __device__ inline int phi_stride(int ts, int nb) { return nb * ts; }
+
+// Row stride of the phi tile in the 4-feature-block kernel, which forms the
+// Gram with FP64 tensor-core MMAs (m8n8k4): 8-feature blocks, stride = 8
+// (mod 16) doubles so that a fragment load (4 rows x 8 features) touches
+// every bank pair exactly twice.
+__host__ __device__ inline int dmma_stride(int pa) {
+  const int nb8 = (pa + 7) / 8;
+  return 8 * nb8 + ((nb8 & 1) ? 0 : 8);
 }
-__host__ __device__ inline int phi_stride(int ts, int nb) { return nb * ts + phi_skew(ts, nb + ts - 1); }
+
+// D (8x8, two doubles per lane) += A (8x4) * B (4x8) in FP64 on the tensor
+// cores.  Lane l holds A[l/4][l%4], B[l%4][l/4] and D[l/4][2(l%4) + {0,1}].
+__device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
 
 __host__ __device__ inline Fp64Layout fp64_layout(int pmax, int dmax, int ts, int chunk) {
   Fp64Layout L;
   const int pa = pmax + 1;
-  L.ldp = ((pa + ts - 1) / ts) * ts;
+  // features incl. padding: 8-feature blocks in the tensor-core form (ts = 4)
+  L.ldp = ts == 4 ? ((pa + 7) / 8) * 8 : ((pa + ts - 1) / ts) * ts;
   L.chunk = chunk;
   size_t o = 0;
   for (int s = 0; s < 2; ++s) {
@@ -130,7 +144,8 @@ __host__ __device__ inline Fp64Layout fp64_layout(int pmax, int dmax, int ts, in
     L.off_w[s] = o; o = align16(o + (size_t)chunk * 8 + 16);
   }
   L.off_bar = o; o = align16(o + 2 * 8);
-  L.off_phi = o; o = align16(o + (size_t)chunk * phi_stride(ts, L.ldp / ts) * 8);
+  L.off_phi = o;
+  o = align16(o + (size_t)chunk * (ts == 4 ? dmma_stride(pa) : phi_stride(ts, L.ldp / ts)) * 8);
   L.off_q = o; o = align16(o + (size_t)chunk * 8);
   L.off_gram = o; o = align16(o + (size_t)pa * (pa + 1) / 2 * 8);
   L.off_fa = o; o = align16(o + (size_t)L.ldp * 2);
@@ -155,8 +170,9 @@ __device__ __forceinline__ void issue_chunk(const RidgeArgs& a, const RidgeItem&
   if (a.w) bulk_g2s(smem + lay.off_w[st], gw.base, gw.bytes, bar);
 }
 
+// TS = 4 (tensor-core Gram, 80 registers) is held to three CTAs per SM.
 template <int TS, int CHUNK>
-__global__ void __launch_bounds__(kRidgeThreads) ridge_fp64_kernel(RidgeArgs a, RidgeLists L,
+__global__ void __launch_bounds__(kRidgeThreads, TS == 4 ? 3 : 1) ridge_fp64_kernel(RidgeArgs a, RidgeLists L,
                                                                    int cls, int pcap) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_item, s_fail;
@@ -187,11 +203,13 @@ __global__ void __launch_bounds__(kRidgeThreads) ridge_fp64_kernel(RidgeArgs a, 
     const int k = L.list[(int64_t)cls * a.K + item];
     const RidgeItem it = load_item(a, k);
     const int p = it.p, pa = p + 1, d = it.d;
-    const int nb = (pa + TS - 1) / TS;
-    const int ldpi = nb * TS;              // features incl. padding
-    const int lds = phi_stride(TS, nb);    // phi row stride
+    // TS = 4: FP64 tensor-core tiles of 8 features; TS = 8: 8x8 register tiles
+    constexpr bool kDmma = TS == 4;
+    const int nb = kDmma ? (pa + 7) / 8 : (pa + TS - 1) / TS;
+    const int ldpi = kDmma ? 8 * nb : nb * TS;            // features incl. padding
+    const int lds = kDmma ? dmma_stride(pa) : phi_stride(TS, nb);  // phi row stride
     const int T = nb * (nb + 1) / 2;
-    const int S = max(1, kRidgeThreads / T);
+    const int S = kDmma ? 1 : max(1, kRidgeThreads / T);
     for (int f = tid; f < ldpi; f += kRidgeThreads) {
       int fa_, fb_;
       if (f < p) feature_factors(d, it.kind, f, fa_, fb_);
@@ -208,6 +226,16 @@ __global__ void __launch_bounds__(kRidgeThreads) ridge_fp64_kernel(RidgeArgs a, 
     for (int i = 0; i < TS; ++i)
 #pragma unroll
       for (int j = 0; j < TS; ++j) acc[i][j] = 0.0;
+    // tensor-core form: warp w owns 8x8 tiles w, w + 8, w + 16 (T <= 21)
+    const int wid = tid >> 5, wl = tid & 31;
+    double dacc[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    int tI[3], tJ[3];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      const int t2 = wid + 8 * m;
+      tI[m] = t2 < T ? tile_row(t2) : 0;
+      tJ[m] = t2 < T ? t2 - tI[m] * (tI[m] + 1) / 2 : 0;
+    }
     int bad = 0;
     const int64_t nchunks = (it.n + CHUNK - 1) / CHUNK;
     if (tid == 0) {
@@ -244,22 +272,37 @@ __global__ void __launch_bounds__(kRidgeThreads) ridge_fp64_kernel(RidgeArgs a, 
       // phi[r][phi_pos(blk, j)] = sqrt(q_r) * feature(blk*TS + j): the
       // rotation and shift spread the tiles' loads over distinct banks.
       const int warp = tid >> 5, lane = tid & 31;
-      for (int r = warp; r < rows; r += kRidgeThreads / 32) {
-        const double* xr = xs + (int64_t)r * d;
-        const double sq = q[r];
+      // the tensor-core form reads rows in groups of 4: pad with zero rows
+      const int rows_pad = kDmma ? (rows + 3) & ~3 : rows;
+      for (int r = warp; r < rows_pad; r += kRidgeThreads / 32) {
+        const bool live = r < rows;
+        const double* xr = xs + (int64_t)(live ? r : 0) * d;
+        const double sq = live ? q[r] : 0.0;
         for (int f = lane; f < ldpi; f += 32) {
           const int ia = fa[f], ib = fb[f];
           double v;
-          if (ia == -3) v = 0.0;
+          if (ia == -3 || !live) v = 0.0;
           else if (ia == -2) v = sq * ys[r];
           else v = sq * ((ia < 0 ? 1.0 : xr[ia]) * (ib < 0 ? 1.0 : xr[ib]));
-          const int blk = f / TS, j = f - blk * TS;
-          phi[r * lds + phi_pos(TS, blk, j)] = v;
+          if constexpr (kDmma) {
+            phi[r * lds + f] = v;
+          } else {
+            const int blk = f / TS, j = f - blk * TS;
+            phi[r * lds + phi_pos(TS, blk, j)] = v;
+          }
         }
       }
       __syncthreads();
       if (tid == 0 && c + 2 < nchunks) issue_chunk(a, it, CHUNK, c + 2, smem, lay, st, &bars[st]);
-      if (mine) {
+      if constexpr (kDmma) {
+        const int off = (wl & 3) * lds + (wl >> 2);
+        for (int k0 = 0; k0 < rows_pad; k0 += 4) {
+          const double* pr = phi + k0 * lds + off;
+#pragma unroll
+          for (int m = 0; m < 3; ++m)
+            if (wid + 8 * m < T) dmma_884(dacc[m], pr[8 * tI[m]], pr[8 * tJ[m]]);
+        }
+      } else if (mine) {
         for (int r = slice; r < rows; r += S) {
           const double* pr = phi + r * lds;
           double av[TS], bv[TS];
@@ -292,8 +335,21 @@ __global__ void __launch_bounds__(kRidgeThreads) ridge_fp64_kernel(RidgeArgs a, 
       const int bw = __syncthreads_or(bad & 2), bx = __syncthreads_or(bad & 1);
       bad = (bw ? 2 : 0) | (bx ? 1 : 0);
     }
+    if constexpr (kDmma) {  // each lower entry belongs to one warp's tile
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        if (wid + 8 * m >= T) continue;
+        const int r = 8 * tI[m] + (wl >> 2);
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int cc = 8 * tJ[m] + 2 * (wl & 3) + e;
+          if (r < pa && cc <= r) G[pk(r, cc)] = dacc[m][e];
+        }
+      }
+      __syncthreads();
+    }
     // deterministic slice reduction into the packed augmented Gram
-    for (int s = 0; s < S; ++s) {
+    for (int s = 0; s < (kDmma ? 0 : S); ++s) {
       if (mine && slice == s) {
 #pragma unroll
         for (int i = 0; i < TS; ++i)
