@@ -366,15 +366,12 @@ def solve_weighted_ridge_batched(
 _COPY_STREAMS: dict[int, object] = {}
 
 
-def _host_array(a, t, dtype):
-    """numpy / torch CPU -> CPU torch tensor (no copy when already suitable)."""
+def _host_f64(a, t):
+    """numpy / torch CPU array -> contiguous float64 CPU tensor (no copy when already suitable)."""
 
     if isinstance(a, t.Tensor):
-        return a.to(dtype=dtype).contiguous()
-    return t.from_numpy(np.ascontiguousarray(a, dtype=_NP_OF[dtype]))
-
-
-_NP_OF: dict = {}
+        return a.to(dtype=t.float64).contiguous()
+    return t.from_numpy(np.ascontiguousarray(a, dtype=np.float64))
 
 
 def host_slice_bounds(row_offsets, x_offsets, dims, slices: int):
@@ -404,8 +401,6 @@ def _solve_host_staged(x, y, weights, row_offsets, dims, features, ridge, x_offs
 
     t = torch()
     dev = require_cuda()
-    if not _NP_OF:
-        _NP_OF.update({t.float64: np.float64, t.int64: np.int64, t.int32: np.int32})
     ro_h = np.asarray(row_offsets.cpu() if isinstance(row_offsets, t.Tensor) else row_offsets, dtype=np.int64)
     dims_h = np.asarray(dims.cpu() if isinstance(dims, t.Tensor) else dims, dtype=np.int64)
     feats_h = np.asarray(features.cpu() if isinstance(features, t.Tensor) else features, dtype=np.int32)
@@ -418,9 +413,9 @@ def _solve_host_staged(x, y, weights, row_offsets, dims, features, ridge, x_offs
     if bounds is None:
         return None
     ends = xo_h + np.diff(ro_h) * dims_h
-    xh = _host_array(x, t, t.float64)
-    yh = _host_array(y, t, t.float64)
-    wh = None if weights is None else _host_array(weights, t, t.float64)
+    xh = _host_f64(x, t)
+    yh = _host_f64(y, t)
+    wh = None if weights is None else _host_f64(weights, t)
     if xh.numel() < int(ends[-1]) or yh.numel() < int(ro_h[-1]) or (wh is not None and wh.numel() < int(ro_h[-1])):
         raise ValueError("x, y and weights must cover every system's rows")
     if kw.get("max_dim") is None:
