@@ -40,6 +40,7 @@ INFO_FP64_RESOLVE = 8
 INFO_REFINE_CAP = 16
 INFO_COND_FAILED = 32
 INFO_REFINE_SHIFT = 8
+MEDIAN_NN_MAX_SET = 4096
 RIDGE_OPT_FP64_FACTOR = 1
 
 MAX_FEATURES = 160
@@ -146,6 +147,7 @@ SIGNATURES = {
     "art_partition_rows": (C.c_int, [C.POINTER(ArtSegments), P, P, I64, P, P, P, P]),
     "art_segment_residuals": (C.c_int, [C.POINTER(ArtSegments), P, P, P, I64, P, P, P]),
     "art_tree_predict": (C.c_int, [I32, I64, P, P, I64, P, I64, P, I64, P, P, P, P]),
+    "art_median_nn_distance": (C.c_int, [I64, P, P, P, P, P, I32, F64, P, P]),
     "art_last_error": (C.c_char_p, []),
     "art_abi_version": (C.c_int, []),
     "art_launch_count": (C.c_uint64, []),

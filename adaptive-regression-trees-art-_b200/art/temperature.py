@@ -2,6 +2,9 @@
 
 T = c * median nearest-neighbour distance of (at most ``max_points``
 subsampled) node samples, or c * median pairwise distance * n^(-1/d).
+``nn_method="device"`` computes the nearest-neighbour distances and their
+median on the GPU (``art_median_nn_distance``, exact brute force in FP64), and
+``median_nn_distance_batched`` does it for many point sets in one launch.
 """
 
 from __future__ import annotations
@@ -13,7 +16,7 @@ from typing import Literal
 import numpy as np
 
 TemperatureMode = Literal["median_nn", "median_pairwise_scaled"]
-NearestNeighborMethod = Literal["kdtree", "bruteforce"]
+NearestNeighborMethod = Literal["kdtree", "bruteforce", "device"]
 TemperatureStrategy = Literal["splitter", "fixed", "tune_root", "tune_node"]
 DEFAULT_TEMPERATURE_GRID = (1e-4, 5e-4, 0.001, 0.005, 0.01, 0.05, 0.1, 0.5, 1.0)
 
@@ -69,8 +72,10 @@ def median_nearest_neighbor_distance(X, method: NearestNeighborMethod = "kdtree"
         raise ValueError(f"X must have shape (n, d), got {X.shape}.")
     if X.shape[0] < 2:
         raise ValueError("At least two points are required.")
-    if method not in ("kdtree", "bruteforce"):
-        raise ValueError("method must be 'kdtree' or 'bruteforce'.")
+    if method not in ("kdtree", "bruteforce", "device"):
+        raise ValueError("method must be 'kdtree', 'bruteforce' or 'device'.")
+    if method == "device":
+        return float(median_nn_distance_batched([X])[0].item())
     if method == "kdtree":
         try:
             from scipy.spatial import cKDTree
@@ -82,6 +87,48 @@ def median_nearest_neighbor_distance(X, method: NearestNeighborMethod = "kdtree"
     D = pairwise_distances(X)
     np.fill_diagonal(D, np.inf)
     return float(np.median(np.min(D, axis=1)))
+
+
+def median_nn_distance_batched(point_sets, c: float = 1.0, stream=None):
+    """c * median nearest-neighbour distance of each point set, on the GPU.
+
+    ``point_sets`` is a list of (m_k, d_k) arrays (numpy or torch), each at
+    most ``MEDIAN_NN_MAX_SET`` points.  Returns a float64 CUDA tensor of K
+    values, NaN for sets of fewer than two points.  Distances are exact FP64
+    brute force, so they equal the kd-tree query's up to the summation order
+    of the squared coordinates.
+    """
+
+    from . import _native as N
+    from ._device import ptr, require_cuda, stream_handle, to_device, torch
+
+    t = torch()
+    dev = require_cuda()
+    lib = N.load_library()
+    if not (c > 0.0):
+        raise ValueError("c must be positive.")
+    sets = [np.asarray(P.cpu() if isinstance(P, t.Tensor) else P, dtype=float) for P in point_sets]
+    K = len(sets)
+    for P in sets:
+        if P.ndim != 2:
+            raise ValueError(f"X must have shape (n, d), got {P.shape}.")
+    sizes = np.array([P.shape[0] for P in sets], dtype=np.int64)
+    if K and sizes.max() > N.MEDIAN_NN_MAX_SET:
+        raise ValueError(f"at most {N.MEDIAN_NN_MAX_SET} points per set are supported")
+    out = t.empty(K, dtype=t.float64, device=dev)
+    if K == 0:
+        return out
+    dims = np.array([P.shape[1] for P in sets], dtype=np.int32)
+    x_off = np.concatenate([[0], np.cumsum(sizes * dims)[:-1]]).astype(np.int64)
+    s_off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    rows = np.concatenate([np.arange(m, dtype=np.int64) for m in sizes]) if sizes.sum() else np.zeros(1, np.int64)
+    xd = to_device(np.concatenate([P.reshape(-1) for P in sets]) if sizes.sum() else np.zeros(1), t.float64, dev)
+    xo, dd, so, rr = (to_device(a, None, dev) for a in (x_off, dims, s_off, rows))
+    rc = lib.art_median_nn_distance(K, ptr(xd), ptr(xo), ptr(dd), ptr(so), ptr(rr), int(sizes.max()), float(c),
+                                    ptr(out), stream_handle(stream))
+    N.check(rc, "art_median_nn_distance")
+    out._keepalive = (xd, xo, dd, so, rr)
+    return out
 
 
 def median_pairwise_distance(X) -> float:

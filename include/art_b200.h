@@ -357,6 +357,25 @@ ART_API int art_tree_predict(int32_t dim, int64_t n_nodes, const int32_t* child,
                      const double* x, int32_t* leaf, double* pred, art_stream_t stream);
 
 /* ======================================================================== */
+/*  Temperature estimate                                                     */
+/* ======================================================================== */
+/* Median nearest-neighbour distance of K point sets, times c: the
+ * "median_nn" mode of estimate_temperature (temperature.py:116-137, with
+ * median_nearest_neighbor_distance 73-101).  The reference's kd-tree query
+ * (k = 2) is replaced by an exact brute-force search in FP64.  Set k holds
+ * rows sample_rows[sample_offsets[k] .. sample_offsets[k+1]) (row indices
+ * into the row-major points at x + x_offsets[k], dims[k] columns each); the
+ * caller draws the subsample (subsample_points, temperature.py:47-62).
+ * temperature[k] = c * median over i of min over j != i of ||x_i - x_j||;
+ * NaN for sets of fewer than two points.  max_set (the host-known largest
+ * set) must not exceed ART_MEDIAN_NN_MAX_SET.                               */
+#define ART_MEDIAN_NN_MAX_SET 4096
+ART_API int art_median_nn_distance(int64_t count, const double* x, const int64_t* x_offsets,
+                           const int32_t* dims, const int64_t* sample_offsets,
+                           const int64_t* sample_rows, int32_t max_set, double c,
+                           double* temperature, art_stream_t stream);
+
+/* ======================================================================== */
 /*  Misc                                                                     */
 /* ======================================================================== */
 ART_API const char* art_last_error(void);  /* thread-local text of the last error  */

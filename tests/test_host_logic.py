@@ -111,3 +111,12 @@ def test_host_slice_bounds_cut_at_system_edges_with_equal_rows():
     assert host_slice_bounds(ro + 4, xo, d, 8) is None           # rows not from 0
     few = host_slice_bounds(ro[:4], xo[:3], d[:3], 8)            # more slices than systems
     assert few[0] == 0 and few[-1] == 3 and np.all(np.diff(few) > 0)
+
+
+def test_temperature_method_names_are_checked_before_any_device_work():
+    sys.path.insert(0, str(ROOT / "adaptive-regression-trees-art-_b200"))
+    from art.temperature import median_nearest_neighbor_distance
+
+    with pytest.raises(ValueError):
+        median_nearest_neighbor_distance(np.zeros((4, 2)), method="ball_tree")
+    assert median_nearest_neighbor_distance(np.array([[0.0, 0.0], [3.0, 4.0], [3.0, 4.5]]), method="bruteforce") == 0.5
