@@ -158,6 +158,7 @@ class RegressionTreeBuilder:
     level_dispatch: bool = True
     cuda_graphs: bool = True
     cohort_top_up: bool = True
+    batched_temperature_tuning: bool = True
     verbose: bool = False
 
     oracle_queries: int = field(default=0, init=False)
@@ -606,11 +607,26 @@ class RegressionTreeBuilder:
         comparison_seed = self._next_seed()
         temperature_seed = self._next_seed()
         candidates, best = [], None
-        for c in config.c_values:
-            T = self._temperature_for_c(X_fit, c, random_seed=temperature_seed)
+        temps = [self._temperature_for_c(X_fit, c, random_seed=temperature_seed) for c in config.c_values]
+        batched = None
+        if self.batched_temperature_tuning and fit_design is None and hasattr(self.splitter, "split_temperatures"):
+            # every candidate starts from the same restarts (one seed): one
+            # launch with a node per candidate gives each candidate's split
+            s = copy.deepcopy(self.splitter)
+            s.random_state = comparison_seed
+            s._timing_profile = self._timing_profile
+            with self._timing_context("splitter"):
+                batched = s.split_temperatures(X_fit, y_fit, temps, parent_model, parent_mse,
+                                               hard_refit=self.hard_refits)
+        for i, (c, T) in enumerate(zip(config.c_values, temps)):
             try:
-                result = self._run_splitter(X_fit, y_fit, parent_model, parent_mse, T, fit_design,
-                                            random_seed=comparison_seed)
+                if batched is not None:
+                    if isinstance(batched[i], SplitNotFoundError):
+                        raise batched[i]
+                    result = batched[i]
+                else:
+                    result = self._run_splitter(X_fit, y_fit, parent_model, parent_mse, T, fit_design,
+                                                random_seed=comparison_seed)
             except SplitNotFoundError as exc:
                 candidates.append({"c": c, "temperature": T, "validation_mse": np.inf, "failure_reason": exc.reason})
                 continue

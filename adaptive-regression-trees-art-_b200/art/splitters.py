@@ -387,6 +387,42 @@ class SoftObliqueSplitter:
                           hard_refit=hard_refit, traces=True)
         return level_result_to_split(self, res, 0, X.shape[0], float(parent_loss), hard_refit)
 
+    def split_temperatures(self, X: np.ndarray, y: np.ndarray, temperatures, parent_model: RegressionModel,
+                           parent_loss: float, *, hard_refit: bool = True) -> list:
+        """``split`` at several temperatures in one device launch.
+
+        Entry i is what ``split`` returns with ``temperature = temperatures[i]``
+        and this splitter's random state (the same restart starts for every
+        temperature), or the SplitNotFoundError it raises.  The candidates
+        run as nodes of one level over copies of the rows; a node's result
+        does not depend on the other nodes of its level, so each entry is
+        bit-identical to its own ``split`` call.
+        """
+
+        X = np.asarray(X, dtype=float)
+        y = np.asarray(y, dtype=float).reshape(-1)
+        self._validate_inputs(X, y)
+        if not hard_refit and self.n_restarts != 1:
+            raise ValueError("Skipping hard refits requires n_restarts == 1.")
+        temps = np.asarray(temperatures, dtype=float).reshape(-1)
+        K, (n, d) = temps.size, X.shape
+        if K == 0:
+            return []
+        kind = _model_kind(self.model_template)
+        rng = self._rng()
+        R = max(1, self.n_restarts)
+        theta0 = np.stack([self._initialize_theta(X, rng) for _ in range(R)])[None]
+        res = split_level(self, np.tile(X.reshape(-1), K), np.tile(y, K), np.arange(K + 1) * n, [d] * K,
+                          [kind] * K, temps, self.model_template.ridge, parent_loss=[float(parent_loss)] * K,
+                          theta0=np.repeat(theta0, K, axis=0), hard_refit=hard_refit, traces=True)
+        out = []
+        for k in range(K):
+            try:
+                out.append(level_result_to_split(self, res, k, n, float(parent_loss), hard_refit))
+            except SplitNotFoundError as exc:
+                out.append(exc)
+        return out
+
 
 def level_result_to_split(s: SoftObliqueSplitter, res: LevelResult, k: int, n: int, parent_loss: float,
                           hard_refit: bool) -> SplitResult:

@@ -73,3 +73,37 @@ def test_tree_predict_device_routing_matches_host_walk():
     X[0] = [0.0, 0.1]        # exactly on the inner plane: goes right
     host = np.array([tree.leaf_for_point(x).predict_one(x) for x in X])
     np.testing.assert_allclose(tree.predict(X), host, rtol=1e-13, atol=1e-13)
+
+
+@pytest.mark.parametrize("strategy,nn_method", [("tune_node", "kdtree"), ("tune_root", "device")])
+def test_batched_temperature_tuning_equals_one_split_per_candidate(strategy, nn_method):
+    """Temperature tuning runs the grid of c as nodes of one split launch; the
+    tree, its tuned c and every candidate's validation score equal those of
+    one splitter call per candidate (the reference's loop)."""
+    from art import (AffineRidgeModel, BoxDomain, HitAndRunSampler, RegressionTreeBuilder, SoftObliqueSplitter,
+                     SplitNode, TemperatureConfig)
+
+    f = target_from(TG["t0_target"])
+
+    def build(batched):
+        model = AffineRidgeModel(ridge=1e-6, solver="normal")
+        splitter = SoftObliqueSplitter(model, 0.05, max_iters=30, n_restarts=2, min_side_points=8,
+                                       min_side_fraction=0.0)
+        b = RegressionTreeBuilder(
+            domain=BoxDomain.hypercube(2, -1.0, 1.0), oracle=f, model_template=model, splitter=splitter,
+            error_threshold=0.02, max_depth=2, sample_count=150, isotropic_sampling=False,
+            temperature_config=TemperatureConfig(strategy=strategy, c_values=(0.01, 0.05, 0.2, 1.0),
+                                                 nn_method=nn_method),
+            random_state=77, oracle_vectorized=True, store_diagnostics=True,
+            sampler=HitAndRunSampler(burn_in=0, thinning=5), batched_temperature_tuning=batched)
+        return b.build()
+
+    a, b = build(True), build(False)
+    na, nb = list(a.tree.iter_nodes()), list(b.tree.iter_nodes())
+    assert [n.node_id for n in na] == [n.node_id for n in nb] and len(na) > 1
+    assert a.oracle_queries == b.oracle_queries
+    for x, y in zip(na, nb):
+        if isinstance(x, SplitNode):
+            np.testing.assert_array_equal(np.r_[x.w, x.z], np.r_[y.w, y.z])
+        for key in ("temperature_c", "temperature", "temperature_candidate_scores"):
+            assert repr(x.metadata.get(key)) == repr(y.metadata.get(key)), key
