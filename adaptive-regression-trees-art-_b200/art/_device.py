@@ -45,6 +45,8 @@ def to_device(array, dtype=None, device=None):
         out = array.to(device=device, dtype=dtype if dtype is not None else array.dtype)
         return out.contiguous()
     arr = np.ascontiguousarray(array, dtype=None if dtype is None else _np_dtype(dtype))
+    if not arr.flags.writeable:  # read-only views (broadcasts, loaded buffers): torch wants a writable array
+        arr = arr.copy()
     return t.from_numpy(arr).to(device=device, non_blocking=False).contiguous()
 
 
