@@ -7,6 +7,7 @@ streams.  Importing the package needs no GPU; calling a device entry point
 does, and raises if no CUDA device or built library is present.
 """
 
+from ._batched_optimizer import BatchedOptimizerWorkspace, optimize_batch
 from .builder import LevelSplitDispatcher, RegressionTreeBuilder, TreeBuildResult
 from .domain import BoxDomain, PolytopeRegion, split_region
 from .metrics import (

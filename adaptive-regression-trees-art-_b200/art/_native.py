@@ -30,6 +30,7 @@ FEATURES_POLY2_NOBIAS = 4
 SOLVER_NORMAL = 0
 SOLVER_AUTO = 1
 SOLVER_QR = 2
+SOLVER_SVD = 3
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 
@@ -40,6 +41,8 @@ INFO_FP64_RESOLVE = 8
 INFO_REFINE_CAP = 16
 INFO_COND_FAILED = 32
 INFO_REFINE_SHIFT = 8
+INFO_SVD = 64
+INFO_RANK_SHIFT = 16
 MEDIAN_NN_MAX_SET = 4096
 RIDGE_OPT_FP64_FACTOR = 1
 

@@ -30,7 +30,7 @@ RIDGE_SOLVERS: tuple[RidgeSolver, ...] = ("auto", "normal", "qr", "svd")
 DEFAULT_AUTO_RCOND_THRESHOLD = 1e-10
 MODEL_CONDITION_WARNING_THRESHOLD = 1e10
 Precision = Literal["fp64", "mixed"]
-_SOLVER_CODES = {"normal": N.SOLVER_NORMAL, "auto": N.SOLVER_AUTO, "qr": N.SOLVER_QR}
+_SOLVER_CODES = {"normal": N.SOLVER_NORMAL, "auto": N.SOLVER_AUTO, "qr": N.SOLVER_QR, "svd": N.SOLVER_SVD}
 _PRECISION_CODES = {"fp64": N.PRECISION_FP64, "mixed": N.PRECISION_MIXED}
 
 
@@ -304,8 +304,6 @@ def solve_weighted_ridge_batched(
             out)
         if staged is not None:
             return staged
-    if solver == "svd":
-        raise NotImplementedError("solver='svd' (LAPACK gelsd) is not part of the B200 path.")
     if solver not in _SOLVER_CODES:
         raise ValueError(f"solver must be one of {RIDGE_SOLVERS}, got {solver!r}.")
     if precision not in _PRECISION_CODES:
@@ -521,6 +519,13 @@ def _result_from_row(beta, ridge_eff, cond, status, info, p, solver) -> RidgeSol
     solver_used: ResolvedRidgeSolver = "cholesky"
     estimator: ConditionEstimator | None = None
     cond_estimate: float | None = None
+    if info & N.INFO_SVD:
+        # solver="svd", or auto whose QR solution was not finite (models.py:426-442)
+        return RidgeSolveResult(
+            coefficients=np.asarray(beta[:p], dtype=float).copy(), solver_requested=solver, solver_used="svd",
+            condition_estimator="svd_2norm", cond_estimate=float(cond) if cond is not None else None,
+            ridge_effective=float(ridge_eff), rank=(int(info) >> N.INFO_RANK_SHIFT) & 0xFF,
+            fallback_reason="qr_nonfinite" if info & N.INFO_QR_FALLBACK else None)
     if info & N.INFO_QR_FALLBACK:
         solver_used = "qr"
         if info & N.INFO_CHOLESKY_FAILED:

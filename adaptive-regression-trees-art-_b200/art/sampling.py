@@ -19,7 +19,7 @@ from __future__ import annotations
 
 import ctypes as C
 from dataclasses import dataclass, field, replace
-from typing import Literal, Protocol, Sequence, runtime_checkable
+from typing import ClassVar, Literal, Protocol, Sequence, runtime_checkable
 
 import numpy as np
 
@@ -437,11 +437,25 @@ class BatchedHitAndRunSampler(HitAndRunSampler):
 
     n_chains: int = 20
     rng_mode: RngMode = "device"
+    # layout of the reference's draws: step-major (BatchedHitAndRunSampler,
+    # NumbaBatchedHitAndRunSampler) or chain-major (the parallel numba form)
+    _chain_major: ClassVar[bool] = False
 
     def sample(self, region: PolytopeRegion, n: int, random_state: RandomState = None,
                x0: np.ndarray | None = None) -> np.ndarray:
+        """sampling.py:643-813.  ``rng_mode="reference"`` draws every
+        direction and chord uniform from ``random_state`` exactly as the
+        reference class does (the same generator calls, in the same order
+        and layout, including the tail round for ``n`` not a multiple of the
+        chain count) and injects them, so the samples equal the reference's
+        to rounding; ``"device"`` keys counter-based device draws per chain."""
+
         if n < 0:
             raise ValueError("n must be nonnegative.")
+        if self.burn_in < 0:
+            raise ValueError("burn_in must be nonnegative.")
+        if self.thinning < 0:
+            raise ValueError("thinning must be nonnegative.")
         if self.n_chains < 1:
             raise ValueError("n_chains must be at least 1.")
         n = int(n)
@@ -455,7 +469,7 @@ class BatchedHitAndRunSampler(HitAndRunSampler):
         full_rounds, remainder = divmod(n, n_chains)
         polys = device_polytopes([region])
         if self.rng_mode == "reference":
-            raise NotImplementedError("batched chains use device draws; inject draws via hit_and_run_device")
+            return self._sample_reference_draws(polys, points, rng, d, stride, full_rounds, remainder, n)
         vecs, sqrt_vals = self._direction_spectrum(d)
         if vecs is not None:  # covariance-shaped directions: u = vecs diag(sqrt_vals) z on the device
             polys = device_polytopes([region], maps=[vecs * sqrt_vals[None, :]])
@@ -466,6 +480,56 @@ class BatchedHitAndRunSampler(HitAndRunSampler):
             n_rounds=rounds, mode="batched", seeds=seeds)
         _raise_status(status.cpu().numpy())
         return samples.reshape(-1, d)[:n].cpu().numpy()
+
+    def _sample_reference_draws(self, polys, points, rng, d, stride, full_rounds, remainder, n):
+        n_chains = points.shape[0]
+        steps = self.burn_in + full_rounds * stride
+        dirs, unif = self._reference_draws(rng, n_chains, steps, d)
+        tail = self._reference_draws(rng, remainder, stride, d) if remainder else None
+        samples, last, status = hit_and_run_device(
+            polys, np.zeros(n_chains, np.int32), points, burn_in=self.burn_in, thinning=stride,
+            n_rounds=full_rounds, mode="batched", directions=dirs, uniforms=unif)
+        _raise_status(status.cpu().numpy())
+        out = [samples.reshape(-1, d)]
+        if tail is not None:
+            # the first `remainder` chains take one more thinned round (burn-in 0)
+            extra, _, status = hit_and_run_device(
+                polys, np.zeros(remainder, np.int32), last[:remainder], burn_in=0, thinning=stride,
+                n_rounds=1, mode="batched", directions=tail[0], uniforms=tail[1])
+            _raise_status(status.cpu().numpy())
+            out.append(extra.reshape(-1, d))
+        return torch().cat(out)[:n].cpu().numpy()
+
+    def _reference_draws(self, rng, n_chains: int, steps: int, d: int):
+        """Directions (chains, steps, d) and uniforms (chains, steps), chain-major,
+        from the generator calls of _draw_random_arrays (sampling.py:864-873,
+        983-1025) and _shape_directions."""
+
+        if self._chain_major and getattr(self, "parallel_random", False):
+            if self.random_threads < 1:
+                raise ValueError("random_threads must be at least 1.")
+            workers = min(self.random_threads, n_chains)
+            dirs = np.empty((n_chains, steps, d))
+            unif = np.empty((n_chains, steps))
+            seeds = rng.integers(0, np.iinfo(np.uint64).max, size=workers, dtype=np.uint64)
+            block, extra = divmod(n_chains, workers)
+            start = 0
+            for w, seed in enumerate(seeds):
+                stop = start + block + (w < extra)
+                g = np.random.Generator(np.random.SFC64(int(seed)))
+                g.standard_normal(out=dirs[start:stop])
+                g.random(out=unif[start:stop])
+                start = stop
+        elif self._chain_major:
+            dirs = rng.normal(size=(n_chains, steps, d))
+            unif = rng.random(size=(n_chains, steps))
+        else:
+            dirs = rng.normal(size=(steps, n_chains, d)).transpose(1, 0, 2)
+            unif = rng.random(size=(steps, n_chains)).T
+        vecs, sqrt_vals = self._direction_spectrum(d)
+        if vecs is not None:
+            dirs = (dirs * sqrt_vals) @ vecs.T
+        return np.ascontiguousarray(dirs), np.ascontiguousarray(unif)
 
     def _initial_points(self, region, n_chains, rng, x0):
         """sampling.py:826-862."""
@@ -499,6 +563,7 @@ class ParallelNumbaBatchedHitAndRunSampler(NumbaBatchedHitAndRunSampler):
     n_chains: int = 50
     parallel_random: bool = True
     random_threads: int = 10
+    _chain_major: ClassVar[bool] = True
 
 
 @dataclass

@@ -30,6 +30,9 @@ from .models import (
 )
 from .timing import BuildTimingProfile, SplitterTimingProfile
 
+# largest total size of the row copies one split_temperatures launch holds
+TEMPERATURE_BATCH_BYTES = 256 << 20
+
 Optimizer = Literal["b200", "cpu", "hybrid_gram", "cupy_qr", "cupy_cholesky", "cupy_batched_cholesky"]
 OPTIMIZERS = ("b200", "cpu", "hybrid_gram", "cupy_qr", "cupy_cholesky", "cupy_batched_cholesky")
 
@@ -412,15 +415,21 @@ class SoftObliqueSplitter:
         rng = self._rng()
         R = max(1, self.n_restarts)
         theta0 = np.stack([self._initialize_theta(X, rng) for _ in range(R)])[None]
-        res = split_level(self, np.tile(X.reshape(-1), K), np.tile(y, K), np.arange(K + 1) * n, [d] * K,
-                          [kind] * K, temps, self.model_template.ridge, parent_loss=[float(parent_loss)] * K,
-                          theta0=np.repeat(theta0, K, axis=0), hard_refit=hard_refit, traces=True)
+        # each candidate node holds its own copy of the rows: launches take at
+        # most TEMPERATURE_BATCH_BYTES of copies (at least one candidate each)
+        per = max(1, int(TEMPERATURE_BATCH_BYTES // max(1, n * (d + 1) * 8)))
         out = []
-        for k in range(K):
-            try:
-                out.append(level_result_to_split(self, res, k, n, float(parent_loss), hard_refit))
-            except SplitNotFoundError as exc:
-                out.append(exc)
+        for c0 in range(0, K, per):
+            c = temps[c0:c0 + per]
+            Kc = c.size
+            res = split_level(self, np.tile(X.reshape(-1), Kc), np.tile(y, Kc), np.arange(Kc + 1) * n, [d] * Kc,
+                              [kind] * Kc, c, self.model_template.ridge, parent_loss=[float(parent_loss)] * Kc,
+                              theta0=np.repeat(theta0, Kc, axis=0), hard_refit=hard_refit, traces=True)
+            for k in range(Kc):
+                try:
+                    out.append(level_result_to_split(self, res, k, n, float(parent_loss), hard_refit))
+                except SplitNotFoundError as exc:
+                    out.append(exc)
         return out
 
 

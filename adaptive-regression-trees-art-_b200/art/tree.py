@@ -2,8 +2,9 @@
 
 ``RegressionTree.predict`` routes all points on the GPU (``art_tree_predict``):
 the tree is flattened to child/plane/coefficient arrays and every point walks
-it independently, with the side decided by the sign of a compensated
-w . x - z (>= 0 goes right).  Save/load keep the reference's joblib artifact
+it independently, with the side decided by the sign of the exact value of
+w . x - z (>= 0 goes right; compensated and, near the plane, exact
+expansion arithmetic on the device).  Save/load keep the reference's joblib artifact
 (type "art.regression_tree", version 1).
 """
 
@@ -263,3 +264,44 @@ class RegressionTree:
             return n.depth if isinstance(n, LeafNode) else max(depth(n.left), depth(n.right))
 
         return 0 if self.root is None else depth(self.root)
+
+
+def partition_rows(x, row_offsets, dims, theta, *, split=None, x_offsets=None, stream=None):
+    """Stable node-sorted partition of every segment's rows by its plane, on the GPU.
+
+    Segment k owns rows ``row_offsets[k]:row_offsets[k+1]`` (inputs at
+    ``x_offsets[k]``, ``dims[k]`` columns) and is split by
+    ``theta[k] = [w, z]``: a row goes right when the exact value of
+    w . x - z is >= 0 (builder.py:487-500).  Returns ``(perm, n_right)`` as
+    device tensors: perm lists, per segment, its left rows then its right
+    rows (global row indices, input order kept on each side); segments with
+    ``split[k] == 0`` keep their rows (all left, n_right 0).
+    """
+
+    from . import _native as N
+    from ._device import ptr, require_cuda, stream_handle, to_device, torch
+
+    t = torch()
+    dev = require_cuda()
+    lib = N.load_library()
+    ro = to_device(row_offsets, t.int64, dev)
+    dd = to_device(dims, t.int32, dev)
+    K = int(dd.numel())
+    xo = to_device(ro[:-1] * dd.to(t.int64) if x_offsets is None else x_offsets, t.int64, dev)
+    xs = to_device(x, t.float64, dev)
+    th = to_device(theta, t.float64, dev)
+    if th.dim() != 2 or th.shape[0] != K:
+        raise ValueError("theta must have shape (K, d_max + 1)")
+    sp = None if split is None else to_device(np.asarray(split, np.int8) if not isinstance(split, t.Tensor) else split,
+                                              t.int8, dev)
+    kinds = t.zeros(K, dtype=t.int32, device=dev)
+    total = int(ro[-1].item()) if K else 0
+    perm = t.empty(max(total, 1), dtype=t.int64, device=dev)
+    n_right = t.empty(max(K, 1), dtype=t.int32, device=dev)
+    if K:
+        seg = N.ArtSegments(K, ptr(ro), ptr(xo), ptr(dd), ptr(kinds))
+        N.check(lib.art_partition_rows(C.byref(seg), ptr(xs), ptr(th), int(th.shape[1]), ptr(sp), ptr(perm),
+                                       ptr(n_right), stream_handle(stream)), "art_partition_rows")
+    perm, n_right = perm[:total], n_right[:K]
+    perm._keepalive = (ro, dd, xo, xs, th, sp, kinds)
+    return perm, n_right

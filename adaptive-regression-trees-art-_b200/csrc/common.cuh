@@ -198,19 +198,70 @@ __device__ __forceinline__ void two_sum(double a, double b, double& s, double& e
 }
 // Compensated w.x - z (Dot2): about twice working precision, so the sign
 // matches the exact sign except for scores within ~1e-30 relative of 0.
-__device__ inline double dot2_score(const double* x, const double* w, int d, double z) {
-  double s = 0.0, c = 0.0;
+// `mag` receives sum |x_i w_i| + |z|, the scale of Dot2's error bound.
+__device__ inline double dot2_score(const double* x, const double* w, int d, double z, double* mag = nullptr) {
+  double s = 0.0, c = 0.0, m = 0.0;
   for (int i = 0; i < d; ++i) {
     double p, e, t, f;
     two_prod(x[i], w[i], p, e);
     two_sum(s, p, t, f);
     s = t;
     c = __dadd_rn(c, __dadd_rn(f, e));
+    m = __dadd_rn(m, fabs(p));
   }
   double t, f;
   two_sum(s, -z, t, f);
   c = __dadd_rn(c, f);
+  if (mag) *mag = __dadd_rn(m, fabs(z));
   return __dadd_rn(t, c);
+}
+
+// Exact sign of x.w - z for the rare scores Dot2 cannot resolve: every
+// product is split exactly (p + e, TwoProduct) and the 2d + 1 terms are
+// summed exactly into a nonoverlapping expansion (Shewchuk, "Adaptive
+// precision floating-point arithmetic and fast robust geometric predicates",
+// Discrete Comput. Geom. 1997: Grow-Expansion with zero elimination); the
+// expansion's largest component carries the sign of the exact sum.  Exact
+// for inputs whose products do not underflow (|x_i w_i| above ~1e-292).
+__device__ __noinline__ bool exact_score_nonnegative(const double* x, const double* w, int d, double z) {
+  double h[2 * ART_MAX_DIM + 2];
+  int m = 0;
+  auto grow = [&](double b) {
+    double q = b;
+    int k = 0;
+    for (int i = 0; i < m; ++i) {
+      double sum, err;
+      two_sum(q, h[i], sum, err);
+      q = sum;
+      if (err != 0.0) h[k++] = err;
+    }
+    if (q != 0.0) h[k++] = q;
+    m = k;
+  };
+  for (int i = 0; i < d && i < ART_MAX_DIM; ++i) {
+    double p, e;
+    two_prod(x[i], w[i], p, e);
+    grow(p);
+    grow(e);
+  }
+  grow(-z);
+  return m == 0 || h[m - 1] > 0.0;
+}
+
+// Side of a split for routing and partitions: (x.w - z) >= 0 evaluated
+// exactly, i.e. the sign of the real number x.w - z (a point exactly on the
+// plane goes right, as numpy's >= 0 sends an exact zero).  Dot2 decides
+// whenever its result exceeds its error bound (Ogita, Rump & Oishi:
+// |res - s| <= u|s| + gamma_{2n}^2 sum|p_i|, taken here with a factor 8 of
+// slack); the expansion decides the rest.
+__device__ inline bool right_side(const double* x, const double* w, int d, double z) {
+  double mag;
+  const double r = dot2_score(x, w, d, z, &mag);
+  const double u = 1.1102230246251565e-16;  // 2^-53
+  const double n = 2.0 * d + 2.0;
+  const double bound = 8.0 * n * n * u * u * mag;
+  if (fabs(r) > bound) return r >= 0.0;
+  return exact_score_nonnegative(x, w, d, z);
 }
 
 }  // namespace art

@@ -23,13 +23,18 @@
 #include <string.h>
 #include <algorithm>
 
+#include <atomic>
+
 #include "ridge.cuh"
 
 namespace art {
 
 // ====================================================================== plan
 __device__ __forceinline__ int plan_class(const RidgeArgs& a, int p) {
-  if (a.precision == ART_PRECISION_MIXED && p >= a.tensor_min_p) return CLS_TENSOR;
+  // direct least-squares solvers never take the normal equations, so their
+  // systems skip the tensor-core Gram (Gram-only calls keep it)
+  const bool direct = a.solver == ART_SOLVER_QR || a.solver == ART_SOLVER_SVD;
+  if (a.precision == ART_PRECISION_MIXED && p >= a.tensor_min_p && (a.gram_out || !direct)) return CLS_TENSOR;
   if (a.gram_out) return -1;  // Gram-only calls cover tensor-class systems only
   if (p + 1 <= kWarpMaxAug) return CLS_WARP;
   return (p + 1 <= kSmallMaxAug) ? CLS_SMALL : CLS_LARGE;
@@ -376,7 +381,23 @@ __global__ void __launch_bounds__(kRidgeThreads, TS == 4 ? 3 : 1) ridge_fp64_ker
 // the fallback of solve_weighted_ridge's auto solver (models.py:334-357,
 // _solve_augmented_ridge 374-448).  Rank-revealing pivoting (gelsy) is not
 // used: the regularised problem has full column rank whenever lambda > 0.
+// solver="svd" (and auto, when the QR solution is not finite) continues
+// from R with the Jacobi SVD below (gelsd's minimum-norm solution).
 constexpr int kQrChunk = 32;
+
+__device__ __forceinline__ int ru(int i, int j, int pa) {  // packed upper, row-major
+  return i * pa - i * (i - 1) / 2 + (j - i);
+}
+
+// SVD stage (solver="svd", or auto after a non-finite QR solution): the
+// factor R is expanded in place to M = R^T, dense column-major p x p, over
+// the packed R; the rotated right-hand side and the per-column scales
+// follow it.
+__host__ __device__ inline size_t svd_vec_off(int pmax) {
+  const size_t pa = (size_t)pmax + 1;
+  const size_t packed = pa * (pa + 1) / 2, dense = (size_t)pmax * pmax;
+  return align16((packed > dense ? packed : dense) * 8);
+}
 
 __host__ __device__ inline size_t qr_smem(int pmax, int dmax) {
   const int pa = pmax + 1;
@@ -387,17 +408,130 @@ __host__ __device__ inline size_t qr_smem(int pmax, int dmax) {
   o = align16(o + (size_t)kQrChunk * dmax * 8);     // x chunk
   o = align16(o + (size_t)(pa + 1) * 8);            // solution
   o = align16(o + (size_t)pa * 4);                  // factor indices
-  return o;
+  const size_t svd = svd_vec_off(pmax) + 2 * align16((size_t)pmax * 8);
+  return o > svd ? o : svd;
 }
 
-__device__ __forceinline__ int ru(int i, int j, int pa) {  // packed upper, row-major
-  return i * pa - i * (i - 1) / 2 + (j - i);
+// Minimum-norm least-squares solution from the triangular factor R (packed
+// upper, pa = p + 1 columns, the last holding c = Q^T b) by a one-sided
+// Jacobi SVD (Hestenes) of M = R^T, the LAPACK gelsd answer of
+// _solve_augmented_ridge (models.py:374-448) up to rounding:
+//   rotations J make the columns of M J orthogonal, M J = U' S, so
+//   R = J S U'^T and  x = U' S^+ J^T c = sum_i m_i (J^T c)_i / s_i^2,
+//   with s_i = ||m_i|| and singular values s_i <= eps * s_max dropped
+//   (scipy's lstsq default cond = eps).  J^T c is accumulated by applying
+//   every rotation to c, so J itself is never stored.
+// Column pairs are visited in round-robin (circle) order, p/2 disjoint pairs
+// per step, one warp per pair; sweeps stop when no pair needed a rotation
+// (|m_i . m_j| <= sqrt(p) eps ||m_i|| ||m_j||) or after kSvdMaxSweeps.
+// Writes the p coefficients to out (global memory: every shared byte of
+// the kernel may be in use) and returns in s_res the largest and smallest
+// singular value, the rank and whether a coefficient is not finite.
+constexpr int kSvdMaxSweeps = 60;
+
+__device__ void jacobi_svd_solve(double* R, int p, double* dv, double* cf, double* out, double* s_res) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nwarps = kRidgeThreads / 32;
+  const int pa = p + 1;
+  double* M = R;  // the same storage, expanded in place
+  __shared__ int s_rot;
+  for (int j = tid; j < p; j += kRidgeThreads) dv[j] = R[ru(j, p, pa)];
+  __syncthreads();
+  // row j of R -> column j of M, last row first: the column's slots never
+  // overlap a packed row not yet moved, and c was saved above
+  for (int j = p - 1; j >= 0; --j) {
+    double v = 0.0;
+    if (tid < p && tid >= j) v = R[ru(j, tid, pa)];
+    __syncthreads();
+    if (tid < p) M[(size_t)j * p + tid] = v;
+    __syncthreads();
+  }
+  const double eps = 2.220446049250313e-16;
+  const double tol = sqrt((double)p) * eps;
+  const int n2 = (p + 1) & ~1;  // players of the circle schedule (one dummy when p is odd)
+  for (int sweep = 0; sweep < kSvdMaxSweeps && n2 > 1; ++sweep) {
+    if (tid == 0) s_rot = 0;
+    __syncthreads();
+    for (int step = 0; step < n2 - 1; ++step) {
+      for (int q = warp; q < n2 / 2; q += nwarps) {
+        int i, j;
+        if (q == 0) { i = step; j = n2 - 1; }
+        else { i = (step + q) % (n2 - 1); j = (step - q + (n2 - 1)) % (n2 - 1); }
+        if (i >= p || j >= p) continue;
+        double* mi = M + (size_t)i * p;
+        double* mj = M + (size_t)j * p;
+        double al = 0.0, be = 0.0, ga = 0.0;
+        for (int k = lane; k < p; k += 32) {
+          const double u = mi[k], v = mj[k];
+          al = fma(u, u, al);
+          be = fma(v, v, be);
+          ga = fma(u, v, ga);
+        }
+        al = warp_sum(al);
+        be = warp_sum(be);
+        ga = warp_sum(ga);
+        if (ga != 0.0 && fabs(ga) > tol * sqrt(al) * sqrt(be)) {
+          const double zeta = (be - al) / (2.0 * ga);
+          const double t = copysign(1.0, zeta) / (fabs(zeta) + hypot(1.0, zeta));
+          const double c = 1.0 / sqrt(fma(t, t, 1.0)), s = c * t;
+          for (int k = lane; k < p; k += 32) {
+            const double u = mi[k], v = mj[k];
+            mi[k] = c * u - s * v;
+            mj[k] = s * u + c * v;
+          }
+          if (lane == 0) {
+            const double u = dv[i], v = dv[j];
+            dv[i] = c * u - s * v;
+            dv[j] = s * u + c * v;
+            s_rot = 1;
+          }
+        }
+      }
+      __syncthreads();
+    }
+    const int any = s_rot;
+    __syncthreads();
+    if (!any) break;
+  }
+  for (int i = warp; i < p; i += nwarps) {
+    double s2 = 0.0;
+    for (int k = lane; k < p; k += 32) s2 = fma(M[(size_t)i * p + k], M[(size_t)i * p + k], s2);
+    s2 = warp_sum(s2);
+    if (lane == 0) cf[i] = sqrt(s2);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double smax = 0.0, smin = __longlong_as_double(0x7ff0000000000000ll);
+    for (int i = 0; i < p; ++i) { smax = fmax(smax, cf[i]); smin = fmin(smin, cf[i]); }
+    int rank = 0;
+    for (int i = 0; i < p; ++i) {
+      const double si = cf[i];
+      const bool keep = si > eps * smax;
+      rank += keep ? 1 : 0;
+      cf[i] = keep ? dv[i] / (si * si) : 0.0;
+    }
+    s_res[0] = smax;
+    s_res[1] = smin;
+    s_res[2] = (double)rank;
+  }
+  __syncthreads();
+  int nonfinite = 0;
+  for (int k = tid; k < p; k += kRidgeThreads) {
+    double x = 0.0;
+    for (int i = 0; i < p; ++i) x = fma(M[(size_t)i * p + k], cf[i], x);
+    nonfinite |= !isfinite(x);
+    out[k] = x;
+  }
+  nonfinite = __syncthreads_or(nonfinite);
+  if (tid == 0) s_res[3] = nonfinite ? 1.0 : 0.0;
+  __syncthreads();
 }
 
 __global__ void __launch_bounds__(kRidgeThreads) ridge_qr_kernel(RidgeArgs a, RidgeLists L) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_item;
   __shared__ double s_tau;
+  __shared__ double s_svd[4];
   const int pa_max = a.pmax + 1;
   double* R = (double*)smem;
   double* V = (double*)(smem + align16((size_t)pa_max * (pa_max + 1) / 2 * 8));
@@ -487,26 +621,46 @@ __global__ void __launch_bounds__(kRidgeThreads) ridge_qr_kernel(RidgeArgs a, Ri
         __syncthreads();
       }
     }
-    // back substitution R beta = c, c = R[:, p]
-    if (tid < 32) {
-      for (int i = lane; i < p; i += 32) sol[i] = R[ru(i, p, pa)];
-      __syncwarp();
-      for (int j = p - 1; j >= 0; --j) {
-        if (lane == 0) sol[j] = sol[j] / R[ru(j, j, pa)];
+    bool use_svd = a.solver == ART_SOLVER_SVD;
+    if (!use_svd) {
+      // back substitution R beta = c, c = R[:, p]
+      if (tid < 32) {
+        for (int i = lane; i < p; i += 32) sol[i] = R[ru(i, p, pa)];
         __syncwarp();
-        const double bj = sol[j];
-        for (int i = lane; i < j; i += 32) sol[i] -= R[ru(i, j, pa)] * bj;
-        __syncwarp();
+        for (int j = p - 1; j >= 0; --j) {
+          if (lane == 0) sol[j] = sol[j] / R[ru(j, j, pa)];
+          __syncwarp();
+          const double bj = sol[j];
+          for (int i = lane; i < j; i += 32) sol[i] -= R[ru(i, j, pa)] * bj;
+          __syncwarp();
+        }
+      }
+      __syncthreads();
+      int nonfinite = 0;
+      for (int i = tid; i < p; i += kRidgeThreads) nonfinite |= !isfinite(sol[i]);
+      nonfinite = __syncthreads_or(nonfinite);
+      // auto: a non-finite QR solution is re-solved by the SVD (models.py:426-438)
+      if (nonfinite && a.solver == ART_SOLVER_AUTO) {
+        use_svd = true;
+      } else {
+        for (int i = tid; i < p; i += kRidgeThreads) a.beta[(int64_t)k * a.beta_stride + i] = sol[i];
+        if (tid == 0) a.status[k] = nonfinite ? -3 : 0;
+        __syncthreads();
+        continue;
       }
     }
-    __syncthreads();
-    int nonfinite = 0;
-    for (int i = tid; i < p; i += kRidgeThreads) {
-      nonfinite |= !isfinite(sol[i]);
-      a.beta[(int64_t)k * a.beta_stride + i] = sol[i];
+    // SVD path: the vectors live past the expanded M (which covers the QR
+    // work arrays, sol included)
+    double* dv = (double*)(smem + svd_vec_off(a.pmax));
+    double* cf = dv + align16((size_t)a.pmax * 8) / 8;
+    jacobi_svd_solve(R, p, dv, cf, a.beta + (int64_t)k * a.beta_stride, s_svd);
+    if (tid == 0) {
+      a.status[k] = s_svd[3] != 0.0 ? -3 : 0;
+      const double smax = s_svd[0], smin = s_svd[1];
+      if (a.cond) a.cond[k] = smin > 0.0 ? smax / smin : __longlong_as_double(0x7ff0000000000000ll);
+      if (a.info)
+        a.info[k] = a.info[k] | ART_INFO_SVD | ((uint32_t)s_svd[2] << ART_INFO_RANK_SHIFT);
     }
-    nonfinite = __syncthreads_or(nonfinite);
-    if (tid == 0) a.status[k] = nonfinite ? -3 : 0;
     __syncthreads();
   }
 }
@@ -603,7 +757,7 @@ static int ridge_entry(const ArtRidgeProblem* pr, const ArtRidgeResult* res, flo
     return ART_E_INVALID;
   }
   if (pr->solver != ART_SOLVER_NORMAL && pr->solver != ART_SOLVER_AUTO &&
-      pr->solver != ART_SOLVER_QR) {
+      pr->solver != ART_SOLVER_QR && pr->solver != ART_SOLVER_SVD) {
     set_error("art_ridge_batched: unknown solver %d", pr->solver);
     return ART_E_INVALID;
   }
@@ -698,7 +852,7 @@ static int ridge_entry(const ArtRidgeProblem* pr, const ArtRidgeResult* res, flo
       if (rc) return rc;
     }
   }
-  if (a.solver == ART_SOLVER_AUTO || a.solver == ART_SOLVER_QR) {
+  if (a.solver == ART_SOLVER_AUTO || a.solver == ART_SOLVER_QR || a.solver == ART_SOLVER_SVD) {
     const size_t sm = qr_smem(a.pmax, a.dmax);
     if (sm > 227 * 1024) {
       set_error("ridge_qr: shared memory %zu bytes exceeds the 227 KB limit", sm);
@@ -731,7 +885,14 @@ extern "C" int art_ridge_batched(const ArtRidgeProblem* pr, const ArtRidgeResult
 // array so that the call itself allocates nothing.
 static constexpr size_t kNoallocBytes = ws_layout(ART_RIDGE_NOALLOC_MAX_COUNT).total;
 static __device__ __align__(256) unsigned char g_ridge_noalloc_ws[kNoallocBytes];
-static void* g_noalloc_addr[64];
+// Device address of the array per device ordinal, resolved on a device's
+// first call.  Host threads may race on the first call; each resolves the
+// same address, and the release/acquire pair publishes it.  The cache
+// assumes the device's primary context (the one the runtime API uses): after
+// cudaDeviceReset the module is reloaded and the address may change, so a
+// caller that resets a device must not call this entry point again in the
+// same process.
+static std::atomic<void*> g_noalloc_addr[64];
 
 extern "C" size_t art_ridge_noalloc_scratch_bytes(void) { return kNoallocBytes; }
 
@@ -749,16 +910,16 @@ extern "C" int art_ridge_batched_noalloc(const ArtRidgeProblem* pr, const ArtRid
     return ART_E_DEVICE;
   }
   // Resolved once per device; the first call on a device may load the module.
-  if (!g_noalloc_addr[dev]) {
-    void* addr = nullptr;
+  void* addr = g_noalloc_addr[dev].load(std::memory_order_acquire);
+  if (!addr) {
     if (cudaGetSymbolAddress(&addr, g_ridge_noalloc_ws) != cudaSuccess || !addr) {
       cudaGetLastError();
       set_error("art_ridge_batched_noalloc: cannot resolve the scratch address");
       return ART_E_LAUNCH;
     }
-    g_noalloc_addr[dev] = addr;
+    g_noalloc_addr[dev].store(addr, std::memory_order_release);
   }
-  return ridge_entry(pr, res, nullptr, 0, g_noalloc_addr[dev], kNoallocBytes, stream);
+  return ridge_entry(pr, res, nullptr, 0, addr, kNoallocBytes, stream);
 }
 
 extern "C" int art_ridge_gram(const ArtRidgeProblem* pr, float* gram, int64_t gram_stride,

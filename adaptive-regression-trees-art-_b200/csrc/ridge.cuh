@@ -125,11 +125,11 @@ __device__ inline bool finish_fp64(const RidgeArgs& a, const RidgeLists& L, int 
     __syncthreads();
     return false;
   }
-  if (a.solver == ART_SOLVER_QR) {  // explicit QR: no normal equations solve
+  if (a.solver == ART_SOLVER_QR || a.solver == ART_SOLVER_SVD) {  // explicit QR: no normal equations solve
     if (tid == 0) {
       if (a.ridge_eff) a.ridge_eff[k] = lam;
       if (a.cond) a.cond[k] = nan;
-      if (a.info) a.info[k] = info0 | ART_INFO_QR_FALLBACK;
+      if (a.info) a.info[k] = info0 | (a.solver == ART_SOLVER_SVD ? 0u : ART_INFO_QR_FALLBACK);
       a.status[k] = 0;
       push_list(L, a.K, CLS_QR, k);
     }

@@ -119,11 +119,11 @@ __device__ void warp_finish(const RidgeArgs& a, const RidgeLists& L, int k, cons
     warp_write_failed(a, k, p, (bad & 2) ? -1 : -2, lam, 0u);
     return;
   }
-  if (a.solver == ART_SOLVER_QR) {
+  if (a.solver == ART_SOLVER_QR || a.solver == ART_SOLVER_SVD) {
     if (lane == 0) {
       if (a.ridge_eff) a.ridge_eff[k] = lam;
       if (a.cond) a.cond[k] = nan;
-      if (a.info) a.info[k] = ART_INFO_QR_FALLBACK;
+      if (a.info) a.info[k] = a.solver == ART_SOLVER_SVD ? 0u : ART_INFO_QR_FALLBACK;
       a.status[k] = 0;
       push_list(L, a.K, CLS_QR, k);
     }

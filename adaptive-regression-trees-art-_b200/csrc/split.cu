@@ -452,7 +452,7 @@ struct SplitCta {
         if (r < it.rn && S(r, RS_ACTIVE) != 0.0) {
           if (hard) {
             const double* w = th + r * dt();
-            const bool right = dot2_score(xp + row * xps, w, it.d, w[it.d]) >= 0.0;
+            const bool right = right_side(xp + row * xps, w, it.d, w[it.d]);
             qL = right ? 0.0 : 1.0;
             qR = right ? 1.0 : 0.0;
             // integer-valued sums below 2^53 are exact in any order
@@ -773,7 +773,7 @@ __device__ bool SplitCta<TC>::gang_begin(int item_id, int rank, int members) {
   if (members == 1) return true;
   int4* rec = a.gang_rec + item_id;
   if (tid == 0) {
-    int slot = -1;
+    int slot = -1, taken = -1;  // taken: the slot rank 0 holds, kept after a failed formation
     const uint64_t t0 = globaltimer_ns();
     if (rank == 0) {
       for (uint32_t spin = 0; slot < 0; ++spin) {
@@ -782,6 +782,7 @@ __device__ bool SplitCta<TC>::gang_begin(int item_id, int rank, int members) {
         if (slot < 0 && (spin & 63u) == 63u && globaltimer_ns() - t0 > kWaitNs) break;
       }
       if (slot >= 0) {
+        taken = slot;
         __threadfence();
         atomicExch(&rec->x, slot + 1);
       }
@@ -810,6 +811,9 @@ __device__ bool SplitCta<TC>::gang_begin(int item_id, int rank, int members) {
     if (slot < 0) {
       atomicExch(&rec->w, 1);
       atomicExch(&a.counts[kErrSlot], 1);
+      // the level is lost; give the slot back so later gangs of this launch
+      // do not wait out their limits for it
+      if (taken >= 0) atomicExch(&a.slot_flags[taken], 0);
     }
     s_slot = slot;
   }
@@ -1138,7 +1142,7 @@ __device__ void SplitCta<TC>::run(int item_id, int rank, int members) {
         double eL2 = 0.0, eR2 = 0.0;
         if (r < it.rn && S(r, RS_ACTIVE) != 0.0) {
           const double* w = th + r * dt();
-          const bool right = dot2_score(xp + row * xps, w, d, w[d]) >= 0.0;
+          const bool right = right_side(xp + row * xps, w, d, w[d]);
           const double e = ys[row] - fitted((right ? br : bl) + r * a.pmax, row);
           (right ? eR2 : eL2) = e * e;
         }

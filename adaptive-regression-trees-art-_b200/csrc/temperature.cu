@@ -9,7 +9,9 @@
 // distance).  The set's distances are ranked in shared memory (ties broken
 // by index) to place each at its sorted position, and the median is the
 // middle value, or the mean of the two middle values for an even count, as
-// numpy's median.  The result is c * median.
+// numpy's median.  The result is c * median.  A set larger than the
+// caller's max_set (which sized the shared arrays) gives NaN, as a set of
+// fewer than two points does, and touches no shared memory.
 #include "common.cuh"
 
 namespace art {
@@ -21,15 +23,17 @@ __global__ void __launch_bounds__(kTempThreads) median_nn_kernel(int64_t count, 
                                                                  const int64_t* x_offsets,
                                                                  const int32_t* dims,
                                                                  const int64_t* sample_offsets,
-                                                                 const int64_t* sample_rows, double c,
-                                                                 double* out) {
+                                                                 const int64_t* sample_rows, int max_set,
+                                                                 double c, double* out) {
   extern __shared__ double s_nn[];  // [max_set] distances, then [max_set] sorted
   const int tid = threadIdx.x;
   for (int64_t k = blockIdx.x; k < count; k += gridDim.x) {
     const int64_t s0 = sample_offsets[k];
     const int m = (int)(sample_offsets[k + 1] - s0);
     const int d = dims[k];
-    if (m < 2) {
+    // fewer than two points, or more than the shared arrays were sized for
+    // (a caller's max_set below its largest set): NaN, and no shared access
+    if (m < 2 || m > max_set) {
       if (tid == 0) out[k] = __longlong_as_double(0x7ff8000000000000ll);
       continue;
     }
@@ -102,7 +106,7 @@ extern "C" int art_median_nn_distance(
   const int64_t grid = count < 65535 ? count : 65535;
   prof_begin("median_nn", s);
   median_nn_kernel<<<(unsigned)grid, kTempThreads, smem, s>>>(count, x, x_offsets, dims, sample_offsets,
-                                                              sample_rows, c, temperature);
+                                                              sample_rows, max_set, c, temperature);
   prof_end(s);
   count_launch();
   return check_launch("median_nn");

@@ -2,9 +2,11 @@
 // batched tree routing + leaf prediction.
 //
 // Routing rule everywhere: w . x - z >= 0 goes right (builder.py:494,
-// tree.py:159, splitters.py:618).  The score is a compensated dot product
-// (Dot2), so the side is that of the exact value of w . x - z except within
-// a few ulps of the plane; numpy's own rounded X @ w can disagree only there.
+// tree.py:159, splitters.py:618).  The side is the sign of the exact value
+// of w . x - z (right_side: a compensated dot product, and exact expansion
+// arithmetic for the rare scores within its error bound); numpy's own
+// rounded X @ w - z can disagree only where its rounding error exceeds
+// |w . x - z|.
 #include "common.cuh"
 
 namespace art {
@@ -30,8 +32,7 @@ __global__ void __launch_bounds__(kPartThreads)
   int local = 0;
   if (do_split)
     for (int64_t r = tid; r < n; r += kPartThreads) {
-      double sc = dot2_score(x + xoff + r * d, w, d, w[d]);
-      local += sc >= 0.0;
+      local += right_side(x + xoff + r * d, w, d, w[d]) ? 1 : 0;
     }
   int tot = warp_sum(local);
   if (lane == 0) warp_tot[warp] = tot;
@@ -48,7 +49,7 @@ __global__ void __launch_bounds__(kPartThreads)
   for (int64_t base = 0; base < n; base += kPartThreads) {
     const int64_t r = base + tid;
     int right = 0;
-    if (r < n && do_split) right = dot2_score(x + xoff + r * d, w, d, w[d]) >= 0.0;
+    if (r < n && do_split) right = right_side(x + xoff + r * d, w, d, w[d]) ? 1 : 0;
     const unsigned bal = __ballot_sync(0xffffffffu, right);
     const unsigned inb = __ballot_sync(0xffffffffu, r < n);
     const int wr = __popc(bal), wl = __popc(inb & ~bal);
@@ -95,8 +96,7 @@ __global__ void predict_kernel(int d, int64_t n_nodes, const int32_t* child, con
   int node = 0;
   for (int64_t guard = 0; guard < n_nodes && child[2 * node] >= 0; ++guard) {
     const double* t = theta + (int64_t)node * ts;
-    const double sc = dot2_score(xr, t, d, t[d]);
-    node = child[2 * node + (sc >= 0.0 ? 1 : 0)];
+    node = child[2 * node + (right_side(xr, t, d, t[d]) ? 1 : 0)];
   }
   if (leaf) leaf[i] = node;
   if (pred) pred[i] = leaf_predict(xr, d, features[node], coef + (int64_t)node * cs);

@@ -70,6 +70,11 @@ typedef struct CUstream_st* art_stream_t; /* == cudaStream_t */
 #define ART_SOLVER_AUTO 1    /* Cholesky + rcond; rcond < threshold or failure
                                 -> FP64 Householder QR on [sqrt(W)Phi; sqrt(l)I] */
 #define ART_SOLVER_QR 2      /* FP64 Householder QR directly (solver="qr")    */
+#define ART_SOLVER_SVD 3     /* FP64 Householder QR, then a one-sided Jacobi SVD
+                                of R: the minimum-norm least-squares solution,
+                                singular values <= eps * max dropped
+                                (solver="svd", LAPACK gelsd in the reference,
+                                models.py:374-448); cond = s_max / s_min     */
 
 /* ---- precision forms ---------------------------------------------------- */
 #define ART_PRECISION_FP64 0   /* plain form: FP64 Gram, FP64 Cholesky        */
@@ -86,6 +91,11 @@ typedef struct CUstream_st* art_stream_t; /* == cudaStream_t */
 #define ART_INFO_FP64_RESOLVE 8u       /* mixed form re-solved in FP64         */
 #define ART_INFO_REFINE_CAP 16u        /* refinement hit its iteration cap     */
 #define ART_INFO_COND_FAILED 32u       /* condition estimate failed            */
+#define ART_INFO_SVD 64u               /* the Jacobi SVD produced the solution
+                                          (solver="svd", or auto after a
+                                          non-finite QR solution)             */
+/* bits 16..23 (SVD path only): the numerical rank of the augmented design  */
+#define ART_INFO_RANK_SHIFT 16
 /* bits 8..15: FP64 refinement passes used by the mixed form (0 otherwise)  */
 #define ART_INFO_REFINE_SHIFT 8
 
@@ -331,8 +341,10 @@ ART_API int art_hit_and_run(const ArtPolytopes* polytopes, const ArtChains* chai
 /* ======================================================================== */
 /* Stable node-sorted partition of each item's rows by the sign of
  * w_k . x - z_k (>= 0 -> right), builder.py:487-500 / splitters.py:618.
- * The score is a compensated dot product, so its sign is that of the exact
- * value except within a few ulps of the plane.  Writes, per item, the left
+ * The side is the sign of the exact value of w . x - z (a compensated dot
+ * product, with exact expansion arithmetic where that cannot decide), so a
+ * point lands on the side exact arithmetic gives; numpy's rounded score can
+ * differ only where its rounding error exceeds |w . x - z|.  Writes, per item, the left
  * rows then the right rows as indices into the input rows (perm), and
  * n_right[k].  theta is [K][theta_stride] = [w, z]; items with split[k]==0
  * are copied unchanged (all left).                                           */
@@ -368,7 +380,8 @@ ART_API int art_tree_predict(int32_t dim, int64_t n_nodes, const int32_t* child,
  * caller draws the subsample (subsample_points, temperature.py:47-62).
  * temperature[k] = c * median over i of min over j != i of ||x_i - x_j||;
  * NaN for sets of fewer than two points.  max_set (the host-known largest
- * set) must not exceed ART_MEDIAN_NN_MAX_SET.                               */
+ * set) must not exceed ART_MEDIAN_NN_MAX_SET; it sizes the kernel's shared
+ * arrays, and a set larger than max_set gets NaN (it is not processed).    */
 #define ART_MEDIAN_NN_MAX_SET 4096
 ART_API int art_median_nn_distance(int64_t count, const double* x, const int64_t* x_offsets,
                            const int32_t* dims, const int64_t* sample_offsets,

@@ -53,9 +53,9 @@ def solve_weighted_ridge(design, y, weights, ridge, weight_floor=1e-12, solver="
     y = np.asarray(y, dtype=float).reshape(-1)
     weights = np.asarray(weights, dtype=float).reshape(-1)
     safe = np.maximum(weights, float(weight_floor))                      # :245-247
-    if solver == "qr":
+    if solver in ("qr", "svd"):                                          # :359-371
         ridge_eff = float(ridge) * float(np.sum((design * np.sqrt(safe)[:, None]) ** 2)) / design.shape[1]
-        return _augmented(design, y, safe, ridge_eff, solver, "qr", None, None, None)
+        return _augmented(design, y, safe, ridge_eff, solver, solver, None, None, None)
     gram = design.T @ (design * safe[:, None])                           # :253
     rhs = design.T @ (y * safe)                                          # :254
     ridge_eff = float(ridge) * float(np.trace(gram)) / gram.shape[0]      # :271, :209-215
@@ -95,8 +95,18 @@ def _augmented(design, y, safe, ridge_eff, requested, used, estimator, cond, rea
     if ridge_eff > 0.0:
         A = np.vstack([A, np.sqrt(ridge_eff) * np.eye(design.shape[1])])
         b = np.concatenate([b, np.zeros(design.shape[1])])
-    coef, _, rank, sv = linalg.lstsq(A, b, lapack_driver="gelsy" if used == "qr" else "gelsd",
-                                     check_finite=False)
+    try:
+        coef, _, rank, sv = linalg.lstsq(A, b, lapack_driver="gelsy" if used == "qr" else "gelsd",
+                                         check_finite=False)
+    except linalg.LinAlgError:                                           # :412-424
+        if requested != "auto" or used != "qr":
+            raise
+        return _augmented(design, y, safe, ridge_eff, requested, "svd", None, None, "qr_failed")
+    if requested == "auto" and used == "qr" and not np.all(np.isfinite(coef)):  # :426-438
+        return _augmented(design, y, safe, ridge_eff, requested, "svd", None, None, "qr_nonfinite")
+    if used == "svd":                                                    # :440-442, 455-461
+        estimator = "svd_2norm"
+        cond = None if sv is None or sv.size == 0 else (np.inf if sv[-1] <= 0.0 else float(sv[0] / sv[-1]))
     return dict(coefficients=coef, solver_requested=requested, solver_used=used,
                 condition_estimator=estimator, cond_estimate=cond, ridge_effective=ridge_eff,
                 rank=int(rank), fallback_reason=reason)

@@ -66,6 +66,24 @@ def ridge_cases(ref):
     base = rng.normal(size=120)
     X = np.column_stack([base, base + 1e-7 * rng.normal(size=120), rng.normal(size=120)])
     cases.append((X, rng.normal(size=120), np.ones(120), O.POLY1_NOBIAS, 0.0, "auto"))
+    # direct least-squares solvers (gelsy / gelsd on the augmented system),
+    # drawn from their own stream so the cases above keep their inputs
+    rng2 = np.random.default_rng(20240602)
+    for n, d, kind, lam, solver, weighted in [
+        (90, 3, O.AFFINE, 1e-6, "qr", True),
+        (120, 4, O.POLY2, 1e-5, "svd", True),
+        (400, 8, O.POLY2, 1e-3, "svd", True),
+        (60, 2, O.AFFINE, 0.0, "svd", False),
+        (300, 16, O.AFFINE, 1e-8, "svd", True),
+    ]:
+        X = rng2.uniform(-1, 1, (n, d))
+        y = np.sin(3 * X[:, 0]) + X[:, -1] ** 2 + 0.01 * rng2.normal(size=n)
+        w = rng2.uniform(0.0, 1.0, n) ** 2 if weighted else np.ones(n)
+        cases.append((X, y, w, kind, lam, solver))
+    # rank-deficient design without ridge: gelsd's minimum-norm solution
+    base = rng2.uniform(-1, 1, (80, 2))
+    X = np.column_stack([base, base[:, 0] + base[:, 1]])
+    cases.append((X, rng2.normal(size=80), np.ones(80), O.POLY1_NOBIAS, 0.0, "svd"))
     out = {}
     for i, (X, y, w, kind, lam, solver) in enumerate(cases):
         phi = O.features(X, kind)
@@ -84,7 +102,8 @@ def ridge_cases(ref):
         out[f"c{i}_X"] = X
         out[f"c{i}_y"] = y
         out[f"c{i}_w"] = w
-        out[f"c{i}_meta"] = np.array([kind, lam, {"normal": 0, "auto": 1}[solver]], dtype=float)
+        out[f"c{i}_meta"] = np.array([kind, lam, {"normal": 0, "auto": 1, "qr": 2, "svd": 3}[solver]], dtype=float)
+        out[f"c{i}_rank"] = np.array(-1 if res.rank is None else int(res.rank))
         out[f"c{i}_beta"] = res.coefficients
         out[f"c{i}_ridge_eff"] = np.array(res.ridge_effective)
         out[f"c{i}_solver_used"] = np.array(res.solver_used)
@@ -259,6 +278,54 @@ def har_cases(ref):
     print("har cases:", len(specs), len(sspecs))
 
 
+SAMPLER_SPECS = [
+    # (seed, class, d, k oblique rows, n, kwargs, x0 kind: none / point / pool, spectrum)
+    (501, "BatchedHitAndRunSampler", 3, 2, 30, dict(burn_in=5, thinning=3, n_chains=7), "pool", False),
+    (502, "NumbaBatchedHitAndRunSampler", 5, 4, 23, dict(burn_in=0, thinning=2, n_chains=5), "pool", False),
+    (503, "ParallelNumbaBatchedHitAndRunSampler", 4, 3, 40,
+     dict(burn_in=4, thinning=2, n_chains=9, random_threads=4), "point", False),
+    (504, "ParallelNumbaBatchedHitAndRunSampler", 3, 2, 17,
+     dict(burn_in=2, thinning=1, n_chains=6, parallel_random=False), "pool", True),
+    (505, "BatchedHitAndRunSampler", 2, 1, 12, dict(burn_in=3, thinning=0, n_chains=4), "none", True),
+]
+
+
+def sampler_cases(ref):
+    """The reference's batched sampler classes end to end (their own draws)."""
+
+    from oracle import sampling as H
+
+    out = {}
+    for i, (seed, cls, d, k, n, kw, x0kind, spectrum) in enumerate(SAMPLER_SPECS):
+        rng = np.random.default_rng(seed)
+        Ao, bo, c = har_polytope(rng, d, k)
+        Ab, bb = H.box_rows(-np.ones(d), np.ones(d))
+        A, b = np.vstack([Ab, Ao]), np.concatenate([bb, bo])
+        region = ref.domain.PolytopeRegion(A, b)
+        if x0kind == "pool":
+            pool = c[None, :] + 0.02 * rng.uniform(-1, 1, (5, d))
+        elif x0kind == "point":
+            pool = c[None, :].copy()
+        else:
+            pool = np.zeros((0, d))
+        extra = dict(kw)
+        if spectrum:
+            Q, _ = np.linalg.qr(rng.normal(size=(d, d)))
+            extra.update(direction_eigenvectors=Q, direction_eigenvalues=rng.uniform(0.1, 2.0, d))
+        sampler = getattr(ref.sampling, cls)(**extra)
+        x0 = None if x0kind == "none" else (pool[0] if x0kind == "point" else pool)
+        samples = sampler.sample(region, n, random_state=seed + 7, x0=x0)
+        out[f"m{i}_A"], out[f"m{i}_b"], out[f"m{i}_pool"] = A, b, pool
+        out[f"m{i}_spec"] = np.array(repr((seed, cls, d, k, n, kw, x0kind)))
+        if spectrum:
+            out[f"m{i}_vecs"] = extra["direction_eigenvectors"]
+            out[f"m{i}_vals"] = extra["direction_eigenvalues"]
+        out[f"m{i}_samples"] = samples
+    out["count"] = np.array(len(SAMPLER_SPECS))
+    np.savez_compressed(HERE / "har_sampler_golden.npz", **out)
+    print("sampler cases:", len(SAMPLER_SPECS))
+
+
 def c1_target(seed):
     """Sum of 3 Gaussian bumps + tanh ridge (the C1 target family)."""
     rng = np.random.default_rng(seed)
@@ -325,6 +392,41 @@ def tree_cases(ref):
         print(f"tree {i}: {res.tree.num_nodes()} nodes, {res.oracle_queries} queries")
     out["count"] = np.array(len(TREE_SPECS))
     np.savez_compressed(HERE / "tree_golden.npz", **out)
+
+
+def c1tree_cases(ref):
+    """One build at the C1 configuration: d = 2, 4096 samples per node, depth
+    <= 6, at least 32 points per side, T = 0.05 absolute, 100 iterations,
+    affine ridge leaves with lambda = 1e-6 (DFS, the reference's default)."""
+
+    seed = 411
+    f, params = c1_target(seed)
+    model = ref.models.AffineRidgeModel(ridge=1e-6, solver="normal")
+    splitter = ref.splitters.SoftObliqueSplitter(model, 0.05, max_iters=100, n_restarts=1, min_side_points=32,
+                                                 min_side_fraction=0.0)
+    builder = ref.builder.RegressionTreeBuilder(
+        domain=ref.domain.BoxDomain.hypercube(2, -1.0, 1.0), oracle=f, model_template=model,
+        splitter=splitter, error_threshold=0.02, max_depth=6, sample_count=4096, isotropic_sampling=False,
+        temperature_config=ref.temperature.TemperatureConfig(strategy="splitter"), random_state=seed,
+        oracle_vectorized=True, traversal="dfs", sampler=ref.sampling.HitAndRunSampler(burn_in=0, thinning=5))
+    res = builder.build()
+    rows = flatten_tree(ref, res.tree)
+    out = {
+        "ids": np.array([r[0] for r in rows]),
+        "status": np.array([r[1] for r in rows]),
+        "theta": np.array([r[2] if r[2] is not None else np.full(3, np.nan) for r in rows]),
+        "coef": np.array([r[3] if r[3] is not None else np.full(3, np.nan) for r in rows]),
+        "nsamples": np.array([-1 if r[4] is None else r[4] for r in rows]),
+        "queries": np.array(res.oracle_queries),
+        "target": np.concatenate([np.ravel(p) for p in params[:4]] + [[params[4]]]),
+        "seed": np.array(seed),
+    }
+    Xt = np.random.default_rng(seed + 1).uniform(-1, 1, (4000, 2))
+    out["Xtest"] = Xt
+    out["pred"] = res.tree.predict(Xt)
+    out["ytest"] = f(Xt)
+    np.savez_compressed(HERE / "tree_c1_golden.npz", **out)
+    print(f"C1 tree: {res.tree.num_nodes()} nodes, {res.oracle_queries} queries")
 
 
 def main():

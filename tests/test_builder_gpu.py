@@ -107,3 +107,40 @@ def test_batched_temperature_tuning_equals_one_split_per_candidate(strategy, nn_
             np.testing.assert_array_equal(np.r_[x.w, x.z], np.r_[y.w, y.z])
         for key in ("temperature_c", "temperature", "temperature_candidate_scores"):
             assert repr(x.metadata.get(key)) == repr(y.metadata.get(key)), key
+
+
+def test_c1_configuration_build_matches_reference_tree():
+    """One tree at the C1 configuration (d = 2, 4,096 samples per node, depth
+    <= 6, at least 32 points per side, T = 0.05, 100 iterations, affine ridge
+    leaves with lambda = 1e-6), built by the reference (tests/golden/
+    tree_c1_golden.npz) and here with the same random_state: identical node
+    ids, statuses and oracle query counts, split planes and leaf
+    coefficients within 1e-8, and held-out predictions within 1e-8, so the
+    held-out RMSE agrees to far better than 1e-6 relative."""
+    from art import (AffineRidgeModel, BoxDomain, HitAndRunSampler, RegressionTreeBuilder, SoftObliqueSplitter,
+                     SplitNode, TemperatureConfig)
+
+    G = np.load(GOLDEN / "tree_c1_golden.npz")
+    f = target_from(G["target"])
+    model = AffineRidgeModel(ridge=1e-6, solver="normal")
+    splitter = SoftObliqueSplitter(model, 0.05, max_iters=100, n_restarts=1, min_side_points=32,
+                                   min_side_fraction=0.0)
+    builder = RegressionTreeBuilder(
+        domain=BoxDomain.hypercube(2, -1.0, 1.0), oracle=f, model_template=model, splitter=splitter,
+        error_threshold=0.02, max_depth=6, sample_count=4096, isotropic_sampling=False,
+        temperature_config=TemperatureConfig(strategy="splitter"), random_state=int(G["seed"]),
+        oracle_vectorized=True, traversal="dfs", sampler=HitAndRunSampler(burn_in=0, thinning=5))
+    res = builder.build()
+    nodes = list(res.tree.iter_nodes())
+    assert [n.node_id for n in nodes] == list(G["ids"])
+    assert [n.status for n in nodes] == list(G["status"])
+    assert res.oracle_queries == int(G["queries"])
+    for n, th, cf in zip(nodes, G["theta"], G["coef"]):
+        if isinstance(n, SplitNode):
+            np.testing.assert_allclose(np.r_[n.w, n.z], th, rtol=1e-8, atol=1e-10)
+        else:
+            np.testing.assert_allclose(n.model.coef_, cf, rtol=1e-8, atol=1e-10)
+    pred = res.tree.predict(G["Xtest"])
+    np.testing.assert_allclose(pred, G["pred"], rtol=1e-8, atol=1e-10)
+    rmse = lambda p: float(np.sqrt(np.mean((p - G["ytest"]) ** 2)))
+    assert abs(rmse(pred) - rmse(G["pred"])) <= 1e-6 * rmse(G["pred"])

@@ -120,3 +120,29 @@ def test_temperature_method_names_are_checked_before_any_device_work():
     with pytest.raises(ValueError):
         median_nearest_neighbor_distance(np.zeros((4, 2)), method="ball_tree")
     assert median_nearest_neighbor_distance(np.array([[0.0, 0.0], [3.0, 4.0], [3.0, 4.5]]), method="bruteforce") == 0.5
+
+
+def test_batched_optimizer_settings_validation_matches_reference_rules():
+    """_cuda_batched_optimizer.py:59-85: model type, degree, line-search refits, parameter ranges."""
+    import pytest
+
+    from art import AffineRidgeModel, PolynomialRidgeModel, SoftObliqueSplitter
+    from art._batched_optimizer import _batch_data, _dimensions, _node_ids, _validate_settings
+
+    ok = SoftObliqueSplitter(AffineRidgeModel(ridge=1e-6), 0.1)
+    _validate_settings(ok, 3, True)
+    with pytest.raises(ValueError):
+        _validate_settings(SoftObliqueSplitter(PolynomialRidgeModel(degree=3), 0.1), 3, True)
+    with pytest.raises(ValueError):
+        _validate_settings(SoftObliqueSplitter(AffineRidgeModel(), 0.1, rho=1.0), 3, True)
+    with pytest.raises(ValueError):
+        _validate_settings(ok, 3, "yes")
+    with pytest.raises(ValueError):
+        _dimensions(4, 0, 2)
+    with pytest.raises(ValueError):
+        _node_ids([1, 1], 4)
+    assert list(_node_ids([2, 0], 4)) == [2, 0]
+    with pytest.raises(ValueError):
+        _batch_data(np.zeros((2, 3)), np.zeros(2), 1.0)
+    with pytest.raises(ValueError):
+        _batch_data(np.zeros((2, 3, 1)), np.zeros((2, 3)), 0.0)

@@ -36,21 +36,85 @@ def golden_cases():
     for i in range(int(g["count"])):
         kind, lam, solver = g[f"c{i}_meta"]
         yield dict(X=g[f"c{i}_X"], y=g[f"c{i}_y"], w=g[f"c{i}_w"], kind=int(kind), ridge=float(lam),
-                   solver=("normal", "auto")[int(solver)], beta=g[f"c{i}_beta"],
-                   ridge_eff=float(g[f"c{i}_ridge_eff"]), solver_used=str(g[f"c{i}_solver_used"]))
+                   solver=("normal", "auto", "qr", "svd")[int(solver)], beta=g[f"c{i}_beta"],
+                   ridge_eff=float(g[f"c{i}_ridge_eff"]), solver_used=str(g[f"c{i}_solver_used"]),
+                   cond=float(g[f"c{i}_cond"]), rank=int(g[f"c{i}_rank"]))
 
 
 @pytest.mark.parametrize("case", list(golden_cases()), ids=lambda c: f"{c['solver']}-k{c['kind']}-n{len(c['y'])}")
 def test_single_solves_match_reference_golden(case):
+    """Every reference solver (normal, auto with its QR fallback, qr, svd):
+    coefficients at max(1e-10, 1e-14 cond); for svd also the rank and the
+    2-norm condition number of the augmented design (1e-9 relative: the
+    singular values of R against LAPACK's of the whole design).  A rank-
+    deficient svd case (ridge 0, a column equal to the sum of two others)
+    compares gelsd's minimum-norm solution at 1e-9."""
     from art import models
 
     res = models._solve_single(case["X"], case["y"], case["w"], case["ridge"], case["kind"],
                                weight_floor=1e-12, solver=case["solver"], auto_rcond_threshold=1e-10)
     phi = O.features(case["X"], case["kind"])
-    c = cond_of(phi, case["w"], case["ridge"])
-    assert rel_err(res.coefficients, case["beta"]) <= tol_for(c)
+    if case["solver_used"] == "svd" and case["rank"] < phi.shape[1]:
+        tol = 1e-9
+    else:
+        tol = tol_for(cond_of(phi, case["w"], case["ridge"]))
+    assert rel_err(res.coefficients, case["beta"]) <= tol
     assert res.ridge_effective == pytest.approx(case["ridge_eff"], rel=1e-12, abs=1e-300)
     assert res.solver_used == case["solver_used"]
+    if case["solver_used"] == "svd":
+        assert res.rank == case["rank"]
+        assert res.condition_estimator == "svd_2norm"
+        if np.isfinite(case["cond"]) and case["rank"] == phi.shape[1]:
+            assert res.cond_estimate == pytest.approx(case["cond"], rel=1e-9)
+
+
+def test_batched_svd_solver_matches_gelsd_on_mixed_segments():
+    """solver="svd" over a batch of every feature class (9 to 153 features):
+    the Jacobi SVD of R against the oracle's gelsd, at max(1e-10, 1e-14 cond)."""
+    from art import _native as N
+    from art.models import solve_weighted_ridge_batched
+
+    wl = make_batch(K=48, seed=23, n_max=400)
+    out = solve_weighted_ridge_batched(wl.x, wl.y, wl.w, wl.row_offsets, wl.dims, wl.kinds, wl.ridge,
+                                       x_offsets=wl.x_offsets, solver="svd", precision="fp64",
+                                       max_features=wl.max_features, max_dim=wl.max_dim, condition=True)
+    beta, status = out.beta.cpu().numpy(), out.status.cpu().numpy()
+    info, cond = out.info.cpu().numpy(), out.cond_estimate.cpu().numpy()
+    assert set(wl.kinds.tolist()) and max(int(p) for p in wl.dims) == 16
+    for k in range(wl.count):
+        r0, r1 = wl.row_offsets[k], wl.row_offsets[k + 1]
+        d = int(wl.dims[k])
+        X = wl.x[wl.x_offsets[k]: wl.x_offsets[k] + (r1 - r0) * d].reshape(-1, d)
+        phi = O.features(X, int(wl.kinds[k]))
+        p = phi.shape[1]
+        ref = O.solve_weighted_ridge(phi, wl.y[r0:r1], wl.w[r0:r1], wl.ridge[k], solver="svd")
+        assert status[k] == 0 and info[k] & N.INFO_SVD
+        assert (int(info[k]) >> N.INFO_RANK_SHIFT) & 0xFF == ref["rank"]
+        c = cond_of(phi, wl.w[r0:r1], wl.ridge[k])
+        assert rel_err(beta[k, :p], ref["coefficients"]) <= tol_for(c), (k, p, c)
+        assert cond[k] == pytest.approx(ref["cond_estimate"], rel=1e-8)
+
+
+def test_auto_falls_back_to_svd_when_the_qr_solution_is_not_finite():
+    """A zero feature column and no ridge: the Cholesky fails, the unpivoted
+    QR meets a zero pivot, and the auto solver re-solves by the SVD
+    (models.py:426-438).  The zero column's coefficient is 0 and the others
+    equal the reference's least-squares solution."""
+    from art import _native as N
+    from art.models import solve_weighted_ridge_batched
+
+    rng = np.random.default_rng(31)
+    X = np.column_stack([rng.uniform(-1, 1, 50), np.zeros(50), rng.uniform(-1, 1, 50)])
+    y = X[:, 0] - 2 * X[:, 2] + 0.01 * rng.normal(size=50)
+    out = solve_weighted_ridge_batched(X.reshape(-1), y, None, [0, 50], [3], [N.FEATURES_POLY1_NOBIAS], [0.0],
+                                       solver="auto", precision="fp64", max_features=3, max_dim=3, condition=True)
+    info = int(out.info.cpu().numpy()[0])
+    assert out.status.cpu().numpy()[0] == 0
+    assert info & N.INFO_SVD and info & N.INFO_QR_FALLBACK
+    assert (info >> N.INFO_RANK_SHIFT) & 0xFF == 2
+    ref = O.solve_weighted_ridge(X, y, np.ones(50), 0.0, solver="svd")["coefficients"]
+    np.testing.assert_allclose(out.beta.cpu().numpy()[0], ref, rtol=1e-10, atol=1e-12)
+    assert out.beta.cpu().numpy()[0, 1] == 0.0
 
 
 def make_batch(K=96, seed=7, n_max=700):

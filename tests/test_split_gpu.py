@@ -319,3 +319,110 @@ def test_gang_split_of_large_nodes_matches_oracle_and_is_batch_independent(ctas_
         for name in ("theta", "loss", "n_right", "n_iters", "beta"):
             np.testing.assert_array_equal(getattr(alone, name).cpu().numpy()[0],
                                           getattr(res, name).cpu().numpy()[k], err_msg=f"{name} {k}")
+
+
+def c3_nodes(seed, ns, d=16):
+    """Nodes of the C3 configuration: x uniform in a random axis box inside
+    [-1,1]^16 (sides U[0.25,1]*2), y = 8 Gaussian bumps (widths U(0.1,0.6),
+    amplitudes N(0,1)) + a linear trend with N(0,1) coefficients."""
+    rng = np.random.default_rng(seed)
+    Xs, ys = [], []
+    for n in ns:
+        side = rng.uniform(0.25, 1.0, d) * 2
+        lo = rng.uniform(-1, 1 - side)
+        X = lo + side * rng.uniform(0, 1, (n, d))
+        cen = rng.uniform(-1, 1, (8, d))
+        wid = rng.uniform(0.1, 0.6, 8)
+        amp = rng.normal(size=8)
+        r2 = ((X[:, None, :] - cen[None]) ** 2).sum(-1)
+        y = (amp * np.exp(-r2 / (2 * wid ** 2))).sum(1) + X @ rng.normal(size=d)
+        Xs.append(X)
+        ys.append(y)
+    return Xs, ys, rng
+
+
+def test_c3_shape_fp64_level_matches_oracle_at_1e10():
+    """The C3 split configuration at full shape on a few nodes: d = 16, 16
+    restarts, exactly 60 projected-gradient steps (grad_atol = grad_rtol = 0),
+    temperature annealed 0.2 -> 0.02, affine child fits with lambda = 1e-6,
+    FP64 form.  For every node, each restart's trajectory is restated by the
+    oracle; the device's chosen restart must be an argmin of the hard loss
+    (to 1e-9) and its split parameters, soft-loss history and hard loss must
+    equal the oracle's at 1e-10 relative, with identical iteration counts,
+    stop reasons and partition counts."""
+    from art.splitters import level_result_to_split, split_level
+
+    ns = [600, 1100, 257]
+    Xs, ys, rng = c3_nodes(33, ns)
+    K, R, d, iters, lam = len(ns), 16, 16, 60, 1e-6
+    th0 = np.array([[S.initialize_theta(X, rng) for _ in range(R)] for X in Xs])
+    extra = {"min_side_points": 8, "min_side_fraction": 0.0, "grad_atol": 0.0, "grad_rtol": 0.0}
+    s = splitter_for(O.AFFINE, 0.2, lam, R, iters, extra)
+    parent = []
+    for X, y in zip(Xs, ys):
+        phi = O.features(X, O.AFFINE)
+        b = O.solve_weighted_ridge(phi, y, np.ones(len(y)), lam)["coefficients"]
+        parent.append(float(np.mean((y - phi @ b) ** 2)))
+    ro = np.concatenate([[0], np.cumsum(ns)])
+    res = split_level(s, np.concatenate([X.reshape(-1) for X in Xs]), np.concatenate(ys), ro, [d] * K,
+                      [O.AFFINE] * K, 0.2, lam, parent_loss=parent, theta0=th0, anneal_ratio=0.1, traces=True)
+    p = S.Params(max_iters=iters, n_restarts=R, anneal_ratio=0.1, **extra)
+    picks = (res.flags.cpu().numpy() >> 8) & 255
+    for k in range(K):
+        per = []
+        for r in range(R):
+            opt = S.optimize(Xs[k], ys[k], th0[k][r], 0.2, O.AFFINE, lam, p)
+            try:
+                hr = S.hard_result(Xs[k], ys[k], opt["theta"], O.AFFINE, lam, parent[k], p, True)
+            except ValueError:
+                hr = {"loss": np.inf}
+            hr.update(opt)
+            per.append(hr)
+        best = min(h["loss"] for h in per)
+        ref = per[int(picks[k])]
+        assert ref["loss"] <= best * (1 + 1e-9)
+        out = level_result_to_split(s, res, k, ns[k], parent[k], True)
+        np.testing.assert_allclose(np.r_[out.w, out.z], np.r_[ref["w"], ref["z"]], rtol=1e-10, atol=1e-12)
+        assert out.n_iters == ref["n_iters"] == iters and out.stop_reason == ref["stop_reason"]
+        assert out.n_right == ref["n_right"]
+        np.testing.assert_allclose(out.metadata["soft_loss_history"], ref["losses"], rtol=1e-10, atol=1e-14)
+        np.testing.assert_allclose(out.loss, ref["loss"], rtol=1e-10)
+
+
+def test_mixed_form_objective_along_its_trajectory_within_1e5():
+    """The mixed form (single-precision gates, FP64 sums and solves): at every
+    iterate of its own trajectory, the soft objective it reports is within
+    1e-5 relative of the FP64 oracle's objective at that same theta.  The
+    iterates are read by re-running with max_iters = 1, 2, ... (without an
+    anneal the trajectory prefix does not depend on max_iters).  The split
+    parameters after the first step (same start) differ from the FP64 form's
+    by at most 1e-4 relative."""
+    from art.splitters import split_level
+
+    ns, Xs, ys, th0, kd = random_level(6, K=6, R=1, kinds=(O.AFFINE,))
+    K, d, T, lam, M = len(ns), 4, 0.15, 1e-6, 12
+    ro = np.concatenate([[0], np.cumsum(ns)])
+    x, y = np.concatenate([X.reshape(-1) for X in Xs]), np.concatenate(ys)
+    extra = {"min_side_points": 1, "min_side_fraction": 0.0}
+
+    def run(prec, iters):
+        s = splitter_for(O.AFFINE, T, lam, 1, iters, extra)
+        s.precision = prec
+        return split_level(s, x, y, ro, [d] * K, kd, T, lam, parent_loss=[1.0] * K, theta0=th0, traces=True,
+                           hard_refit=True)
+
+    full = run("mixed", M)
+    trace = full.trace_loss.cpu().numpy()[:, 0, :]
+    iters = full.n_iters.cpu().numpy()
+    worst = 0.0
+    for m in range(0, M + 1):
+        th = run("mixed", m).theta.cpu().numpy()
+        for k in range(K):
+            if m > iters[k]:
+                continue
+            obj = S.Objective(Xs[k], ys[k], T, O.AFFINE, lam, 1e-12)
+            ref = obj.evaluate(th[k, : d + 1])["loss"]
+            worst = max(worst, abs(trace[k, m] - ref) / abs(ref))
+    assert worst <= 1e-5, worst
+    one_m, one_f = run("mixed", 1).theta.cpu().numpy(), run("fp64", 1).theta.cpu().numpy()
+    assert np.max(np.abs(one_m - one_f) / np.maximum(np.abs(one_f), 1e-3)) <= 1e-4

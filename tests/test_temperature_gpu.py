@@ -59,3 +59,32 @@ def test_estimate_temperature_device_equals_kdtree(d):
         t_kd = estimate_temperature(X, "median_nn", c=0.1, max_points=512, random_state=seed, nn_method="kdtree")
         t_dev = estimate_temperature(X, "median_nn", c=0.1, max_points=512, random_state=seed, nn_method="device")
         np.testing.assert_allclose(t_dev, t_kd, rtol=1e-13, atol=0.0)
+
+
+def test_max_set_below_a_set_size_gives_nan_for_that_set_only():
+    """A C caller that passes max_set smaller than one of its sets: that set
+    gets NaN (it is not processed, so the shared arrays sized by max_set are
+    never overrun) and the other sets are unaffected.  The inputs are valid
+    device buffers; only the size bound is too small."""
+    import torch
+
+    from art import _native as N
+    from art._device import ptr
+
+    rng = np.random.default_rng(7)
+    sets = [rng.uniform(-1, 1, (40, 3)), rng.uniform(-1, 1, (300, 3)), rng.uniform(-1, 1, (12, 3))]
+    sizes = np.array([len(P) for P in sets], np.int64)
+    dev = torch.device("cuda", 0)
+    x = torch.tensor(np.concatenate([P.reshape(-1) for P in sets]), dtype=torch.float64, device=dev)
+    xo = torch.tensor(np.r_[0, np.cumsum(sizes * 3)[:-1]], dtype=torch.int64, device=dev)
+    dims = torch.full((3,), 3, dtype=torch.int32, device=dev)
+    so = torch.tensor(np.r_[0, np.cumsum(sizes)], dtype=torch.int64, device=dev)
+    rows = torch.tensor(np.concatenate([np.arange(m) for m in sizes]), dtype=torch.int64, device=dev)
+    out = torch.full((3,), -1.0, dtype=torch.float64, device=dev)
+    lib = N.load_library()
+    rc = lib.art_median_nn_distance(3, ptr(x), ptr(xo), ptr(dims), ptr(so), ptr(rows), 64, 1.0, ptr(out), None)
+    assert rc == 0
+    got = out.cpu().numpy()
+    assert np.isnan(got[1])
+    np.testing.assert_allclose(got[0], brute_median_nn(sets[0]), rtol=1e-13, atol=0.0)
+    np.testing.assert_allclose(got[2], brute_median_nn(sets[2]), rtol=1e-13, atol=0.0)

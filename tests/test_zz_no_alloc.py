@@ -17,16 +17,17 @@ from conftest import gpu_available
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not gpu_available(), reason="needs a CUDA device")]
 
 
-def _batch(K, seed, solver, precision):
+def _batch(K, seed, solver, precision, n_max=600, device=None):
     import torch
 
     from art import _native as N
     from art import workloads
     from art.models import _PRECISION_CODES, _SOLVER_CODES
 
-    wl = workloads.ridge_systems(K, seed=seed, n_min=1, n_max=600)
+    wl = workloads.ridge_systems(K, seed=seed, n_min=1, n_max=n_max, device=device)
     dev = torch.device("cuda", torch.cuda.current_device())
-    t = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a)).to(device=dev, dtype=dt)
+    t = lambda a, dt: (a if isinstance(a, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(a))).to(
+        device=dev, dtype=dt).contiguous()
     keep = dict(x=t(wl.x, torch.float64), y=t(wl.y, torch.float64), w=t(wl.w, torch.float64),
                 ro=t(wl.row_offsets, torch.int64), xo=t(wl.x_offsets, torch.int64),
                 dims=t(wl.dims, torch.int32), feats=t(wl.kinds, torch.int32),
@@ -59,12 +60,12 @@ def _host(out):
     return {k: v.cpu().numpy() for k, v in out.items()}
 
 
-def _solve_both(lib, K, seed, solver, precision):
+def _solve_both(lib, K, seed, solver, precision, n_max=600, device=None):
     import torch
 
     from art import _native as N
 
-    prob, keep, P = _batch(K, seed, solver, precision)
+    prob, keep, P = _batch(K, seed, solver, precision, n_max, device)
     stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     res_a, out_a = _result(K, P)
     res_b, out_b = _result(K, P)
@@ -84,6 +85,17 @@ def test_noalloc_equals_workspace_entry_on_two_calls_in_a_row(lib, solver, preci
         for key in ("beta", "lam", "status", "info"):
             np.testing.assert_array_equal(a[key], b[key], err_msg=f"{key} K={K}")
         assert (a["status"] == 0).mean() > 0.5
+
+
+def test_noalloc_at_the_scratch_limit_equals_workspace_entry(lib):
+    """Exactly ART_RIDGE_NOALLOC_MAX_COUNT small systems: the whole fixed
+    scratch is in use, twice in a row."""
+    from art import _native as N
+
+    for seed in (21, 22):
+        a, b = _solve_both(lib, N.RIDGE_NOALLOC_MAX_COUNT, seed, "auto", "fp64", n_max=24, device="cuda")
+        for key in ("beta", "lam", "status", "info"):
+            np.testing.assert_array_equal(a[key], b[key], err_msg=f"{key} seed={seed}")
 
 
 def test_noalloc_rejects_batches_beyond_the_fixed_scratch(lib):
