@@ -34,7 +34,10 @@ def build_bfs(builder: "RegressionTreeBuilder", work: "_NodeWork",
         ready = []
         # children about to be prepared get their samples in one launch, with
         # the builder's draws taken in the same order as one at a time
-        builder._top_up_cohort([queue[i] for i in range(min(len(queue), builder.node_batch_size))])
+        cohort = [queue[i] for i in range(min(len(queue), builder.node_batch_size))]
+        builder._top_up_cohort(cohort)
+        # and their node models in one batched solve
+        builder._fit_cohort(cohort)
         while queue and len(ready) < builder.node_batch_size:
             job = queue.popleft()
             leaf = builder._prepare_node(job)

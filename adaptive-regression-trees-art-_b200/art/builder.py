@@ -95,6 +95,7 @@ class _NodeWork:
     topped: bool = False                      # samples already topped up (cohort launch)
     topup_error: Exception | None = None      # the top-up's failure, raised at prepare
     topup_pending: tuple | None = None        # cohort top-up awaiting its oracle values
+    fit_cache: tuple | None = None            # (model, predictions) or (exception, None) from a cohort fit
 
 
 @dataclass
@@ -159,6 +160,11 @@ class RegressionTreeBuilder:
     cuda_graphs: bool = True
     cohort_top_up: bool = True
     batched_temperature_tuning: bool = True
+    batched_fits: bool = True
+    fit_precision: Literal["fp64", "mixed"] = "fp64"
+    refinement_rounds: int = 0
+    refinement_points: int = 1024
+    refinement_leaves: int = 4
     verbose: bool = False
 
     oracle_queries: int = field(default=0, init=False)
@@ -213,6 +219,10 @@ class RegressionTreeBuilder:
             raise TypeError("SoftObliqueSplitter requires a model with fit_weighted support.")
         if self.validation_fraction > 0.0 and self._metric_name() != "max_pointwise_relative_error":
             raise ValueError("validation_fraction requires max_pointwise_relative_error.")
+        if self.fit_precision not in ("fp64", "mixed"):
+            raise ValueError("fit_precision must be 'fp64' or 'mixed'.")
+        if self.refinement_rounds < 0 or self.refinement_points < 1 or self.refinement_leaves < 1:
+            raise ValueError("refinement needs rounds >= 0, points >= 1 and leaves >= 1.")
         if self.temperature_config is None:
             self.temperature_config = TemperatureConfig()
         if (self.temperature_config.strategy in ("tune_root", "tune_node") and self._target_samples < 4):
@@ -248,13 +258,10 @@ class RegressionTreeBuilder:
         y_root = self._query_oracle(X_root)
         work = _NodeWork(root_region, _NodeSamples(X_root, y_root, 0, X_root.shape[0], meta), depth=0,
                          node_id="root")
-        if self.traversal == "dfs":
-            root = self._build_node(work)
-        else:
-            from ._batched_builder import build_bfs
-
-            dispatch = LevelSplitDispatcher(self) if self.level_dispatch else None
-            root = build_bfs(self, work, dispatch)
+        self._leaf_samples = {} if self.refinement_rounds else None
+        root = self._grow(work)
+        for _ in range(self.refinement_rounds):
+            root = self._refine_round(root)
         tree = RegressionTree(root=root, oracle_queries=self.oracle_queries, metadata={
             "error_metric": self._metric_name(), "error_threshold": self.error_threshold,
             "effective_dimension": self._effective_dimension, "splitter": type(self.splitter).__name__,
@@ -272,6 +279,51 @@ class RegressionTreeBuilder:
         tree.metadata["build_timing"] = timing
         return TreeBuildResult(tree=tree, oracle_queries=self.oracle_queries,
                                restarts_on_failure=self.restarts_on_failure, build_timing=timing)
+
+    def _grow(self, work: _NodeWork) -> TreeNode:
+        if self.traversal == "dfs":
+            return self._build_node(work)
+        from ._batched_builder import build_bfs
+
+        dispatch = LevelSplitDispatcher(self) if self.level_dispatch else None
+        return build_bfs(self, work, dispatch)
+
+    def _refine_round(self, root: TreeNode) -> TreeNode:
+        """One adaptive refinement round (the reference has no driver for this).
+
+        The ``refinement_leaves`` leaves with the largest fit error (ties in
+        depth-first order) get ``refinement_points`` new samples between them
+        (the first ones one more when the count does not divide), drawn by the
+        builder's sampler inside each leaf's region from one of its samples
+        and queried from the oracle.  Each leaf, in that order, is then
+        rebuilt from its samples plus the new ones through the builder's own
+        node policy (fit, stopping rules, split, children topped up to the
+        target count), and the subtree replaces it.
+        """
+
+        tree = RegressionTree(root=root)
+        leaves = [n for n in tree.iter_nodes() if isinstance(n, LeafNode)]
+        order = sorted(range(len(leaves)), key=lambda i: -float(leaves[i].metadata.get("fit_error", 0.0)))
+        chosen = [leaves[i] for i in order[: self.refinement_leaves]]
+        base, extra = divmod(self.refinement_points, len(chosen))
+        for q, leaf in enumerate(chosen):
+            smp = self._leaf_samples[leaf.node_id]
+            m = base + (1 if q < extra else 0)
+            if m == 0:
+                continue
+            x0 = smp.X[int(self._rng.integers(0, smp.X.shape[0]))]
+            X_new, meta = self._sample_region(leaf.region, m, x0=x0, sampler=self.sampler)
+            y_new = self._query_oracle(X_new)
+            work = _NodeWork(leaf.region, _NodeSamples(np.vstack([smp.X, X_new]), np.concatenate([smp.y, y_new]),
+                                                       smp.X.shape[0], m, meta), depth=leaf.depth, node_id=leaf.node_id)
+            sub = self._grow(work)
+            path = RegressionTree(root=root).path_to_node(leaf.node_id)
+            if len(path) == 1:
+                root = sub
+            else:
+                parent = path[-2]
+                setattr(parent, "left" if parent.left is leaf else "right", sub)
+        return root
 
     # ---------------------------------------------------------------- nodes
     def _build_node(self, work: _NodeWork) -> TreeNode:
@@ -313,7 +365,9 @@ class RegressionTreeBuilder:
             work.metadata = {**self._node_metadata(samples, fit_error, work.parent_mse, work.model),
                              **work.convergence}
         else:
-            work.model, fit_error, work.parent_mse, work.metadata = self._fit_full_node_model(samples, work.prepared)
+            cached, work.fit_cache = work.fit_cache, None
+            work.model, fit_error, work.parent_mse, work.metadata = self._fit_full_node_model(
+                samples, work.prepared, cached=cached)
         if fit_error <= self.error_threshold:
             return self._work_leaf(work, "tolerance_met")
         if work.depth >= self.max_depth:
@@ -717,6 +771,14 @@ class RegressionTreeBuilder:
         return None  # features are generated on chip from X
 
     def _fit_node_model(self, X, y, prepared):
+        if prepared is None and self.fit_precision == "mixed":
+            from .models import fit_models_batched
+
+            with self._timing_context("model_refit"):
+                model = fit_models_batched(self.model_template, [X], [y], precision="mixed")[0]
+                if isinstance(model, Exception):
+                    raise model
+                return model, model.predict(X)
         model = self.model_template.clone()
         with self._timing_context("model_refit"):
             if prepared is None:
@@ -724,6 +786,33 @@ class RegressionTreeBuilder:
                 return model, model.predict(X)
             model.fit_design(prepared, y)
             return model, model.predict_design(prepared)
+
+    def _fit_cohort(self, jobs) -> None:
+        """Fit the node models of a BFS cohort in one batched solve.
+
+        Each job whose samples are final (the root, or a child whose cohort
+        top-up succeeded) gets ``fit_cache``: the model and its predictions
+        that ``_fit_node_model`` would return, or the exception it would
+        raise.  Jobs that still need their own top-up, validation fits or a
+        host design matrix keep the per-node path.  The solves are the
+        single-node solves, batched, so the tree does not change.
+        """
+
+        if not self.batched_fits or self.validation_fraction > 0.0:
+            return
+        if isinstance(self.model_template, PolynomialRidgeModel) and self.model_template.degree > 2:
+            return
+        ready = [j for j in jobs if j.fit_cache is None and (
+            j.parent is None or (j.topped and j.topup_error is None and j.topup_pending is None))]
+        if len(ready) < 2:
+            return
+        from .models import fit_models_batched
+
+        with self._timing_context("model_refit"):
+            models = fit_models_batched(self.model_template, [j.samples.X for j in ready],
+                                        [j.samples.y for j in ready], precision=self.fit_precision)
+            for j, m in zip(ready, models):
+                j.fit_cache = (m, None) if isinstance(m, Exception) else (m, m.predict(j.samples.X))
 
     def _fit_convergence_model(self, X, y, prepared):
         n_val = min(max(1, int(round(self.validation_fraction * X.shape[0]))), X.shape[0] - 1)
@@ -733,8 +822,13 @@ class RegressionTreeBuilder:
         pred = model.predict(X) if prepared is None else model.predict_design(prepared)
         return model, pred, fit_idx.size
 
-    def _fit_full_node_model(self, samples, prepared, extra_metadata=None):
-        model, pred = self._fit_node_model(samples.X, samples.y, prepared)
+    def _fit_full_node_model(self, samples, prepared, extra_metadata=None, cached=None):
+        if cached is not None:
+            model, pred = cached
+            if isinstance(model, Exception):
+                raise model
+        else:
+            model, pred = self._fit_node_model(samples.X, samples.y, prepared)
         fit_error = float(self.error_metric(samples.y, pred))
         fit_mse = mean_squared_error(samples.y, pred)
         meta = self._node_metadata(samples, fit_error, fit_mse, model)
@@ -765,6 +859,8 @@ class RegressionTreeBuilder:
                 "fit_fallback_reason": g("fallback_reason"), "warnings": warnings, **samples.sampling_metadata}
 
     def _make_leaf(self, model, region, depth, node_id, status, metadata, samples) -> LeafNode:
+        if getattr(self, "_leaf_samples", None) is not None:
+            self._leaf_samples[node_id] = samples
         meta = dict(metadata)
         if self.store_leaf_representative:
             meta["sample_centroid"] = np.mean(samples.X, axis=0)

@@ -825,3 +825,60 @@ def segment_residuals(x, y, row_offsets, dims, features, beta, *, x_offsets=None
                                       stream_handle(stream)), "art_segment_residuals")
     sse._keepalive = (x, y, ro, xo, dims_t, feats, b)
     return sse, ssy
+
+
+def fit_models_batched(template, Xs, ys, *, precision: Precision = "fp64", stream=None) -> list:
+    """Unweighted fits of one model template to several datasets in one launch.
+
+    Entry k is ``template.clone().fit(Xs[k], ys[k])`` -- the same trace-scaled
+    ridge solve, solver policy and diagnostics as the single-node fit -- or
+    the exception that call raises.  All systems go to the device together in
+    one ``art_ridge_batched`` call (the mixed form refines its solutions to
+    the FP64 form's tolerance), so a tree level costs one launch sequence and
+    one read of the results instead of one of each per node.
+    """
+
+    if not Xs:
+        return []
+    if isinstance(template, PolynomialRidgeModel) and template.degree not in (1, 2):
+        raise ValueError("batched fits support affine and degree 1/2 polynomial models")
+    kind = template.kind() if isinstance(template, PolynomialRidgeModel) else N.FEATURES_AFFINE
+    Xs = [_as_2d(X) for X in Xs]
+    ys = [np.asarray(y, dtype=float).reshape(-1) for y in ys]
+    d = Xs[0].shape[1]
+    if any(X.shape[1] != d for X in Xs) or any(X.shape[0] != y.shape[0] for X, y in zip(Xs, ys)):
+        raise ValueError("every dataset needs the same dimension and one y per row")
+    p = kind_feature_count(d, kind)
+    ro = np.concatenate([[0], np.cumsum([X.shape[0] for X in Xs])]).astype(np.int64)
+    K = len(Xs)
+    out = solve_weighted_ridge_batched(
+        np.concatenate([X.reshape(-1) for X in Xs]), np.concatenate(ys), None, ro, [d] * K, [kind] * K,
+        [float(template.ridge)] * K, weight_floor=1e-12, solver=template.solver, precision=precision,
+        auto_rcond_threshold=template.auto_rcond_threshold, max_features=p, max_dim=d, condition=True,
+        stream=stream)
+    beta, lam = out.beta.cpu().numpy(), out.ridge_effective.cpu().numpy()
+    cond, status, info = out.cond_estimate.cpu().numpy(), out.status.cpu().numpy(), out.info.cpu().numpy()
+    models = []
+    for k in range(K):
+        st = int(status[k])
+        if st > 0:
+            models.append(np.linalg.LinAlgError(
+                "Normal-equation Cholesky factorization failed; use solver='auto', "
+                "solver='qr', or solver='svd', or increase ridge regularization."))
+            continue
+        if st in (-1, -2):
+            models.append(ValueError("design, y and weights must be finite and weights nonnegative."))
+            continue
+        if st == -3:
+            models.append(np.linalg.LinAlgError("Ridge solve produced non-finite coefficients."))
+            continue
+        if st < 0:
+            models.append(RuntimeError(f"art_ridge_batched status {st}"))
+            continue
+        m = template.clone()
+        m.solve_result_ = _result_from_row(beta[k], lam[k], cond[k], st, int(info[k]), p, template.solver)
+        m.coef_ = m.solve_result_.coefficients
+        if isinstance(m, PolynomialRidgeModel):
+            m._set_transformer(d)
+        models.append(m)
+    return models

@@ -223,7 +223,7 @@ __device__ inline double dot2_score(const double* x, const double* w, int d, dou
 // Discrete Comput. Geom. 1997: Grow-Expansion with zero elimination); the
 // expansion's largest component carries the sign of the exact sum.  Exact
 // for inputs whose products do not underflow (|x_i w_i| above ~1e-292).
-__device__ __noinline__ bool exact_score_nonnegative(const double* x, const double* w, int d, double z) {
+static __device__ __noinline__ bool exact_score_nonnegative(const double* x, const double* w, int d, double z) {
   double h[2 * ART_MAX_DIM + 2];
   int m = 0;
   auto grow = [&](double b) {

@@ -76,6 +76,10 @@ class Node:
     n_samples: int = 0
     left: "Node | None" = None
     right: "Node | None" = None
+    fit_error: float = 0.0
+    region: tuple | None = None        # (A, b) of a leaf, kept for refinement
+    X: np.ndarray | None = None        # a leaf's samples, kept for refinement
+    y: np.ndarray | None = None
 
 
 @dataclass
@@ -93,6 +97,9 @@ class Builder:
     burn_in: int = 0
     thinning: int = 5
     random_state: int = 0
+    refinement_rounds: int = 0
+    refinement_points: int = 1024
+    refinement_leaves: int = 4
     queries: int = field(default=0, init=False)
 
     def next_seed(self):
@@ -110,7 +117,30 @@ class Builder:
         b = np.concatenate([self.hi, -self.lo])
         X = np.random.default_rng(self.next_seed()).uniform(self.lo, self.hi, size=(self.sample_count, d))
         y = self.query(X)
-        return self._node(A, b, X, y, 0, "root", parent=False)
+        root = self._node(A, b, X, y, 0, "root", parent=False)
+        for _ in range(self.refinement_rounds):
+            root = self._refine_round(root)
+        return root
+
+    def _refine_round(self, root):
+        """The refinement round of the GPU builder (RegressionTreeBuilder._refine_round):
+        the leaves of largest fit error get new hit-and-run samples and are
+        rebuilt from all their samples through the node policy."""
+        leaves = [n for n in iter_nodes(root) if n.left is None]
+        order = sorted(range(len(leaves)), key=lambda i: -leaves[i].fit_error)
+        chosen = [leaves[i] for i in order[: self.refinement_leaves]]
+        base, extra = divmod(self.refinement_points, len(chosen))
+        for q, leaf in enumerate(chosen):
+            m = base + (1 if q < extra else 0)
+            if m == 0:
+                continue
+            A, b, X, y = leaf.region[0], leaf.region[1], leaf.X, leaf.y
+            x0 = X[int(self.rng.integers(0, X.shape[0]))]
+            Xn = hit_and_run(A, b, x0, m, self.burn_in, self.thinning, self.next_seed())
+            sub = self._node(A, b, np.vstack([X, Xn]), np.concatenate([y, self.query(Xn)]), leaf.depth,
+                             leaf.node_id, parent=False)
+            root = _replace(root, leaf, sub)
+        return root
 
     def _fit(self, X, y):
         phi = R.features(X, self.kind)
@@ -142,10 +172,14 @@ class Builder:
                 X, y = np.vstack([X, Xn]), np.concatenate([y, self.query(Xn)])
         beta, pred, high_cond = self._fit(X, y)
         err = relative_l2_error(y, pred)
+
+        def leaf(status):
+            return Node(node_id, depth, status, coef=beta, n_samples=len(y), fit_error=err, region=(A, b), X=X, y=y)
+
         if err <= self.error_threshold:
-            return Node(node_id, depth, "tolerance_met", coef=beta, n_samples=len(y))
+            return leaf("tolerance_met")
         if depth >= self.max_depth:
-            return Node(node_id, depth, "max_depth", coef=beta, n_samples=len(y))
+            return leaf("max_depth")
         parent_mse = float(np.mean((y - pred) ** 2))
         hard = self.params.n_restarts != 1                               # builder.py:264-269
         split_rng = np.random.default_rng(self.next_seed())              # _run_splitter random_state
@@ -154,12 +188,12 @@ class Builder:
             res = S.split(X, y, starts, self.temperature, self.kind, self.ridge, parent_mse, self.params,
                           hard_refit=hard)
         except ValueError as exc:
-            return Node(node_id, depth, str(exc), coef=beta, n_samples=len(y))
+            return leaf(str(exc))
         failures = ("line_search_failed", "max_line_search_failures", "alpha_min_reached", "non_descent_direction")
         if not np.all(np.isfinite(np.r_[res["w"], res["z"]])):
-            return Node(node_id, depth, "nonfinite_split", coef=beta, n_samples=len(y))
+            return leaf("nonfinite_split")
         if res["stop_reason"] in failures and res["n_iters"] == 0:
-            return Node(node_id, depth, "optimizer_failed_without_progress", coef=beta, n_samples=len(y))
+            return leaf("optimizer_failed_without_progress")
         w, z = res["w"], float(res["z"])
         node = Node(node_id, depth, "split_with_warnings" if self._warnings(res, high_cond) else "split", w=w, z=z,
                     n_samples=len(y))
@@ -167,6 +201,17 @@ class Builder:
         node.left = self._node(np.vstack([A, w]), np.r_[b, z], X[~right], y[~right], depth + 1, f"{node_id}/L")
         node.right = self._node(np.vstack([A, -w]), np.r_[b, -z], X[right], y[right], depth + 1, f"{node_id}/R")
         return node
+
+
+def _replace(root: Node, old: Node, new: Node) -> Node:
+    if root is old:
+        return new
+    for n in iter_nodes(root):
+        if n.left is old:
+            n.left = new
+        elif n.right is old:
+            n.right = new
+    return root
 
 
 def iter_nodes(node: Node):
