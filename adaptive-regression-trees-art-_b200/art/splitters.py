@@ -448,6 +448,9 @@ def level_result_to_split(s: SoftObliqueSplitter, res: LevelResult, k: int, n: i
         "converged": bool(host["flags"] & 1), "final_alpha": host["final_alpha"],
         "temperature": s.temperature, "restart": pick, "hard_refit": hard_refit,
         "required_side_points": s._required_side_points(n),
+        # splitters.py:567-572
+        "alpha_min_saturated": bool(s.adaptive_alpha and host["final_alpha"] <= s.alpha_min),
+        "alpha_max_saturated": bool(s.adaptive_alpha and host["final_alpha"] >= s.alpha_max),
     }
     if res.trace_loss is not None:
         it = host["n_iters"]

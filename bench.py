@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--systems", type=int, default=65536)
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
-    ap.add_argument("--cpu-per-class", type=int, default=1024,
+    ap.add_argument("--cpu-per-class", type=int, default=256,
                     help="systems per feature class in the timed CPU sample")
     ap.add_argument("--fp64-factor", action="store_true",
                     help="mixed form factors the tensor-core Gram in FP64")
@@ -67,7 +67,7 @@ def parse():
                     help="comma-separated legs to run after the headline")
     ap.add_argument("--split-nodes", type=int, default=4096)
     ap.add_argument("--har-chains", type=int, default=16384)
-    ap.add_argument("--tree-builds", type=int, default=3)
+    ap.add_argument("--tree-builds", type=int, default=2)
     ap.add_argument("--serve-jobs", type=int, default=40)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default launch shapes")
@@ -145,6 +145,103 @@ def peaks():
         d = json.loads(p.read_text())
         return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
     return 6650.0, 1590.0, "fallback"
+
+
+# B200 dense FP64 (vector and tensor), NVIDIA's published figure; the pool's
+# measured peaks cover HBM and bf16 only, so FP64 fractions are "of spec".
+FP64_SPEC_TFLOPS = 37.0
+
+
+def cpu_split_rate(wl, nodes=4, restarts=16, iters=60, seed=0):
+    """The oracle's projected-gradient loop (the reference's CPU split path)
+    on a sample of the level's nodes: ``nodes`` nodes spaced in n, ``restarts``
+    restarts each, the level's 60 annealed steps.  Returns restart-steps/s
+    for the level's mean n (the CPU cost of a restart-step is linear in n:
+    row-restart-steps/s divided by the mean rows per node), cores, the sample
+    text and the seconds spent."""
+
+    from threadpoolctl import threadpool_limits
+
+    from oracle import ridge as O
+    from oracle import split as S
+
+    cores = len(os.sched_getaffinity(0))
+    x = wl.x.cpu().numpy() if hasattr(wl.x, "cpu") else np.asarray(wl.x)
+    y = wl.y.cpu().numpy() if hasattr(wl.y, "cpu") else np.asarray(wl.y)
+    th0 = wl.theta0.cpu().numpy() if hasattr(wl.theta0, "cpu") else np.asarray(wl.theta0)
+    n = np.diff(wl.row_offsets)
+    order = np.argsort(n, kind="stable")
+    pick = order[np.linspace(0, n.size - 1, nodes + 2).round().astype(int)[1:-1]]
+    p = S.Params(max_iters=iters, n_restarts=restarts, grad_atol=0.0, grad_rtol=0.0, min_side_points=8,
+                 min_side_fraction=0.0, anneal_ratio=0.1)
+    rows_steps, t_all = 0.0, 0.0
+    with threadpool_limits(limits=cores):
+        for k in pick:
+            r0, r1 = int(wl.row_offsets[k]), int(wl.row_offsets[k + 1])
+            X = x[r0 * wl.d: r1 * wl.d].reshape(-1, wl.d)
+            yy = y[r0:r1]
+            t0 = time.perf_counter()
+            for r in range(restarts):
+                opt = S.optimize(X, yy, th0[k, r], float(wl.temperature[k]), O.AFFINE, float(wl.ridge[k]), p)
+                rows_steps += (r1 - r0) * max(1, opt["n_iters"])
+            t_all += time.perf_counter() - t0
+    rate = rows_steps / t_all / float(n.mean())
+    sample = (f"{nodes} nodes (n = {', '.join(str(int(n[k])) for k in pick)}) x {restarts} restarts x {iters} "
+              f"annealed steps ({t_all:.1f} s), scaled to the level's mean n = {n.mean():.0f}")
+    return rate, cores, sample, t_all
+
+
+def cpu_har_rate(d, chains=1024, steps=1000, seed=4):
+    """The oracle's batched chain transition (the reference's numba kernel
+    restated in numpy, vectorised over chains) with host normal/uniform draws,
+    on ``chains`` chains of the benchmark's polytope family for ``steps``
+    steps.  Returns chain-steps/s, cores, sample text, seconds."""
+
+    from threadpoolctl import threadpool_limits
+
+    from oracle import sampling as H
+
+    cores = len(os.sched_getaffinity(0))
+    rng = np.random.default_rng([seed, d, 1])
+    k = 8
+    c = rng.uniform(-0.5, 0.5, d)
+    Ao = rng.normal(size=(k, d))
+    Ao /= np.linalg.norm(Ao, axis=1, keepdims=True)
+    bo = Ao @ c + rng.uniform(0.05, 0.5, k)
+    Ab, bb = H.box_rows(-np.ones(d), np.ones(d))
+    A, b = np.vstack([Ab, Ao]), np.concatenate([bb, bo])
+    with threadpool_limits(limits=cores):
+        t0 = time.perf_counter()
+        dirs = rng.normal(size=(chains, steps, d))
+        unif = rng.random(size=(chains, steps))
+        H.chains_batched(A, b, np.repeat(c[None], chains, 0), dirs, unif, 0, 10, steps // 10)
+        secs = time.perf_counter() - t0
+    return chains * steps / secs, cores, (f"{chains} chains x {steps} steps in one polytope of the family "
+                                          f"(box cut by {k} halfspaces), draws included ({secs:.1f} s)"), secs
+
+
+def cpu_tree_rate(f, builds=1, **kw):
+    """The oracle's depth-first build (pinned to the reference's trees) of the
+    tree configuration, with the same refinement driver.  Returns builds/s,
+    cores, sample text, seconds."""
+
+    from threadpoolctl import threadpool_limits
+
+    from oracle import builder as B
+    from oracle import ridge as O
+    from oracle import split as S
+
+    cores = len(os.sched_getaffinity(0))
+    with threadpool_limits(limits=cores):
+        t0 = time.perf_counter()
+        for _ in range(builds):
+            b = B.Builder(-np.ones(2), np.ones(2), f, O.AFFINE, 1e-6, 0.05, 0.02, 6, 4096,
+                          S.Params(max_iters=100, n_restarts=1, min_side_points=32, min_side_fraction=0.0),
+                          burn_in=0, thinning=5, random_state=1, **kw)
+            root = b.build()
+        secs = time.perf_counter() - t0
+    nodes = sum(1 for _ in B.iter_nodes(root))
+    return builds / secs, cores, f"{builds} build(s), {nodes} nodes, depth-first ({secs:.1f} s)", secs
 
 
 def algorithmic(wl, idx=None):
@@ -229,15 +326,21 @@ def run_reference(args):
     if rank != 0:
         return
     wl, mix = _cpu_workload(args.systems, args.cpu_per_class)
-    times = []
+    times, walls = [], []
     for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
         rate, cores, sample, _ = cpu_solve_rate(wl, None, mix=mix)
         if i >= args.warmup:
             times.append(rate)
+            walls.append(time.perf_counter() - t0)
     value = float(np.median(times))
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * args.systems / value,
+        "steps": args.steps, "warmup": args.warmup,
+        # one step = the timed sample; the full 65,536-system workload would take
+        # ms_per_full_workload (extrapolated from the sample's per-class times)
+        "ms_per_step": 1000.0 * float(np.mean(walls)),
+        "ms_per_full_workload": 1000.0 * args.systems / value,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": {"workload": WORKLOAD, "systems": args.systems, "solver": "normal"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
@@ -396,6 +499,26 @@ def leg_split(args, stream):
                      "failures": int((res.failure != 0).sum().item()),
                      "achieved_fp64_tflops": flops / (ms / 1000.0) / 1e12, "kernel": top[0],
                      "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()}}
+    hbm, bf16, peak_kind = peaks()
+    for prec in ("fp64", "mixed"):
+        kern = out[prec]["kernels"].get("split_level")
+        if kern:
+            kms = kern["ms"] / max(kern["launches"], 1)
+            bytes_alg = float(n.sum()) * (d + 1) * 8 * 60          # x and y once per node-step, shared by restarts
+            out[prec]["roofline"] = {
+                "bound": "fp64", "kernel": "split_level", "achieved": flops / (kms / 1000.0) / 1e12,
+                "peak": FP64_SPEC_TFLOPS, "unit": "TFLOP/s",
+                "frac": flops / (kms / 1000.0) / 1e12 / FP64_SPEC_TFLOPS,
+                "peak_source": "B200 FP64 spec sheet (no measured FP64 peak on this pool)",
+                "algorithmic_bytes": bytes_alg, "achieved_gbs": bytes_alg / (kms / 1000.0) / 1e9,
+                "hbm_frac": bytes_alg / (kms / 1000.0) / 1e9 / hbm, "hbm_peak_source": peak_kind,
+                "launch_ms": kms}
+    if not args.no_cpu:
+        rate, cores, sample, secs = cpu_split_rate(wl)
+        out["cpu_baseline"] = {"value": rate, "unit": "restart-steps/s", "cores": cores, "kind": "port",
+                               "sample": sample}
+        out["speedup_vs_cpu_fp64"] = out["fp64"]["value"] / rate
+        out["speedup_vs_cpu_mixed"] = out["mixed"]["value"] / rate
     la, lb = thetas["fp64"][0], thetas["mixed"][0]
     ok = np.isfinite(la) & np.isfinite(lb)
     out["value"] = out["fp64"]["value"]
@@ -426,10 +549,23 @@ def leg_har(args, stream):
         steps = args.har_chains * 2000
         k_mean = float((wl.row_offsets[1:] - wl.row_offsets[:-1]).double().mean().item())
         flops = steps * (2 * k_mean * d + 7 * d + 6 * (2 * d + k_mean))
+        hbm, _, peak_kind = peaks()
+        bytes_alg = args.har_chains * 200 * d * 8 + int(wl.A.numel() + wl.b.numel() + 2 * wl.lo.numel()) * 8
         out[f"d{d}"] = {"value": steps / (ms / 1000.0), "unit": "chain-steps/s", "ms": ms,
                         "samples_per_s": args.har_chains * 200 / (ms / 1000.0),
                         "achieved_fp64_gflops": flops / (ms / 1000.0) / 1e9,
-                        "status_ok": bool((status == 0).all().item())}
+                        "status_ok": bool((status == 0).all().item()),
+                        "roofline": {"bound": "fp64", "achieved": flops / (ms / 1000.0) / 1e12,
+                                     "peak": FP64_SPEC_TFLOPS, "unit": "TFLOP/s",
+                                     "frac": flops / (ms / 1000.0) / 1e12 / FP64_SPEC_TFLOPS,
+                                     "peak_source": "B200 FP64 spec sheet (no measured FP64 peak on this pool)",
+                                     "algorithmic_bytes": bytes_alg,
+                                     "hbm_frac": bytes_alg / (ms / 1000.0) / 1e9 / hbm, "hbm_peak_source": peak_kind}}
+        if not args.no_cpu:
+            rate, cores, sample, _ = cpu_har_rate(d)
+            out[f"d{d}"]["cpu_baseline"] = {"value": rate, "unit": "chain-steps/s", "cores": cores, "kind": "port",
+                                            "sample": sample}
+            out[f"d{d}"]["speedup_vs_cpu"] = out[f"d{d}"]["value"] / rate
     return {"metric": "hit-and-run chain-steps/s", "chains": args.har_chains, "steps": 2000, "thinning": 10,
             "by_dim": out}
 
@@ -460,13 +596,19 @@ def leg_serving(args, stream):
 
 
 def leg_tree(args, stream):
-    """Tree builds/s on the 2-d configuration: N = 4096 uniform points, depth
-    <= 6, min 32 points per side, soft oblique splits (T = 0.05, 100
+    """Tree builds/s on the 2-d configuration: N = 4096 points per node,
+    depth <= 6, min 32 points per side, soft oblique splits (T = 0.05, 100
     iterations), affine leaves (lambda = 1e-6), children topped up by
-    hit-and-run with device Philox draws; the level-batched BFS build
-    against the per-node DFS build, both through RegressionTreeBuilder, with
-    the held-out RMSE of each tree on 20,000 uniform points."""
+    hit-and-run with device Philox draws, then 2 refinement rounds of 1024
+    new points in the 4 leaves of largest fit error.  Two GPU forms with the
+    same random stream (so the same tree): the level-batched build (one split
+    launch, one top-up launch and one mixed-form fit with FP64 refinement per
+    cohort, CUDA graphs) against the plain FP64 per-node build (one split
+    call, one top-up and one FP64 fit per node); held-out RMSE of each on
+    20,000 uniform points.  The CPU baseline is the oracle's depth-first
+    build (the reference's trees) with the same refinement driver."""
 
+    from art import _native as N
     from art import (AffineRidgeModel, BoxDomain, HitAndRunSampler, RegressionTreeBuilder, SoftObliqueSplitter,
                      TemperatureConfig)
     from art.workloads import bumps_ridge_2d
@@ -475,33 +617,65 @@ def leg_tree(args, stream):
     X_test = np.random.default_rng(99).uniform(-1.0, 1.0, (20000, 2))
     y_test = f(X_test)
 
-    def build(traversal, dispatch):
+    def build(batched):
         model = AffineRidgeModel(ridge=1e-6, solver="normal")
         sp = SoftObliqueSplitter(model, 0.05, max_iters=100, min_side_points=32, min_side_fraction=0.0)
         b = RegressionTreeBuilder(domain=BoxDomain.hypercube(2, -1.0, 1.0), oracle=f, model_template=model,
                                   splitter=sp, error_threshold=0.01, max_depth=6, sample_count=4096,
                                   temperature_config=TemperatureConfig(strategy="splitter"), random_state=1,
-                                  oracle_vectorized=True, traversal=traversal, level_dispatch=dispatch,
-                                  isotropic_sampling=False,
+                                  oracle_vectorized=True, traversal="bfs", level_dispatch=batched,
+                                  batched_fits=batched, cohort_top_up=batched, cuda_graphs=batched,
+                                  fit_precision="mixed" if batched else "fp64", isotropic_sampling=False,
+                                  refinement_rounds=2, refinement_points=1024, refinement_leaves=4,
                                   sampler=HitAndRunSampler(burn_in=0, thinning=5, rng_mode="device"))
         return b.build()
 
     out = {}
-    for name, trav, disp in (("bfs_level_batched", "bfs", True), ("dfs_per_node", "dfs", False)):
-        build(trav, disp)  # warm-up
+    trees = {}
+    for name, batched in (("level_batched_mixed", True), ("plain_fp64_per_node", False)):
+        build(batched)  # warm-up (graph capture, autotune tables)
+        torch_sync()
+        N.profile_reset()
+        N.profile_enable(True)
         t0 = time.perf_counter()
         reps = args.tree_builds
         for _ in range(reps):
-            res = build(trav, disp)
+            res = build(batched)
+        torch_sync()
         wall = time.perf_counter() - t0
+        N.profile_enable(False)
+        prof = N.profile_report()
+        kern_ms = sum(v[1] for v in prof.values())
+        top = max(prof.items(), key=lambda kv: kv[1][1]) if prof else ("none", (0, 0.0))
         rmse = float(np.sqrt(np.mean((res.tree.predict(X_test) - y_test) ** 2)))
+        trees[name] = res
         out[name] = {"builds_per_s": reps / wall, "ms_per_build": 1000 * wall / reps,
                      "nodes": len(list(res.tree.iter_nodes())), "oracle_queries": res.oracle_queries,
-                     "heldout_rmse": rmse}
-    out["speedup"] = out["bfs_level_batched"]["builds_per_s"] / out["dfs_per_node"]["builds_per_s"]
-    a, b = out["bfs_level_batched"]["heldout_rmse"], out["dfs_per_node"]["heldout_rmse"]
+                     "heldout_rmse": rmse, "gpu_kernel_ms_per_build": kern_ms / reps,
+                     "gpu_busy_fraction": kern_ms / (1000 * wall),
+                     "top_kernel": {"name": top[0], "launches_per_build": top[1][0] / reps,
+                                    "ms_per_build": top[1][1] / reps}}
+    out["speedup"] = out["level_batched_mixed"]["builds_per_s"] / out["plain_fp64_per_node"]["builds_per_s"]
+    a, b = out["level_batched_mixed"]["heldout_rmse"], out["plain_fp64_per_node"]["heldout_rmse"]
     out["heldout_rmse_rel_diff"] = abs(a - b) / max(abs(b), 1e-300)
+    ids = [[n.node_id for n in trees[k].tree.iter_nodes()] for k in trees]
+    out["same_tree"] = ids[0] == ids[1]
+    out["roofline"] = {"bound": "latency", "kernel": out["level_batched_mixed"]["top_kernel"]["name"],
+                       "gpu_busy_fraction": out["level_batched_mixed"]["gpu_busy_fraction"],
+                       "note": "a 2-d tree of ~100 nodes of 4,096 rows: kernel time is a small part of the "
+                               "wall time; host policy, oracle calls and launches dominate"}
+    if not args.no_cpu:
+        rate, cores, sample, _ = cpu_tree_rate(f, refinement_rounds=2, refinement_points=1024,
+                                               refinement_leaves=4)
+        out["cpu_baseline"] = {"value": rate, "unit": "builds/s", "cores": cores, "kind": "port", "sample": sample}
+        out["speedup_vs_cpu"] = out["level_batched_mixed"]["builds_per_s"] / rate
     return {"metric": "tree builds/s", "sampler": "hit-and-run, device Philox draws", **out}
+
+
+def torch_sync():
+    import torch
+
+    torch.cuda.synchronize()
 
 
 def run_b200(args):

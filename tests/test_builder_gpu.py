@@ -144,3 +144,80 @@ def test_c1_configuration_build_matches_reference_tree():
     np.testing.assert_allclose(pred, G["pred"], rtol=1e-8, atol=1e-10)
     rmse = lambda p: float(np.sqrt(np.mean((p - G["ytest"]) ** 2)))
     assert abs(rmse(pred) - rmse(G["pred"])) <= 1e-6 * rmse(G["pred"])
+
+
+def _c1_builder(f, **kw):
+    from art import AffineRidgeModel, BoxDomain, HitAndRunSampler, RegressionTreeBuilder, SoftObliqueSplitter, \
+        TemperatureConfig
+
+    model = AffineRidgeModel(ridge=1e-6, solver="normal")
+    splitter = SoftObliqueSplitter(model, 0.05, max_iters=kw.pop("max_iters", 100), min_side_points=kw.pop("min_side", 32),
+                                   min_side_fraction=0.0)
+    rng_mode = kw.pop("rng_mode", "device")
+    return RegressionTreeBuilder(
+        domain=BoxDomain.hypercube(2, -1.0, 1.0), oracle=f, model_template=model, splitter=splitter,
+        error_threshold=0.02, temperature_config=TemperatureConfig(strategy="splitter"), oracle_vectorized=True,
+        isotropic_sampling=False, sampler=HitAndRunSampler(burn_in=0, thinning=5, rng_mode=rng_mode), **kw)
+
+
+def test_refinement_rounds_equal_the_oracle_builder():
+    """Two refinement rounds (the 4 leaves of largest fit error get 120 new
+    hit-and-run points between them and are rebuilt through the node policy),
+    depth-first with the reference's random stream: the tree equals the
+    oracle builder's with the same driver (node ids, statuses, query counts,
+    planes and leaf coefficients within 1e-8)."""
+    from art import SplitNode
+    from oracle import builder as B
+    from oracle import ridge as O
+    from oracle import split as S
+
+    f = target_from(TG["t0_target"])
+    b = _c1_builder(f, max_iters=40, min_side=8, max_depth=3, sample_count=300, random_state=404,
+                    traversal="dfs", rng_mode="reference", refinement_rounds=2, refinement_points=120,
+                    refinement_leaves=4)
+    res = b.build()
+    ob = B.Builder(-np.ones(2), np.ones(2), f, O.AFFINE, 1e-6, 0.05, 0.02, 3, 300,
+                   S.Params(max_iters=40, n_restarts=1, min_side_points=8, min_side_fraction=0.0), burn_in=0,
+                   thinning=5, random_state=404, refinement_rounds=2, refinement_points=120, refinement_leaves=4)
+    root = ob.build()
+    mine, ref = list(res.tree.iter_nodes()), list(B.iter_nodes(root))
+    assert [n.node_id for n in mine] == [n.node_id for n in ref]
+    assert [n.status for n in mine] == [n.status for n in ref]
+    assert res.oracle_queries == ob.queries > 300
+    for a, r in zip(mine, ref):
+        if isinstance(a, SplitNode):
+            np.testing.assert_allclose(np.r_[a.w, a.z], np.r_[r.w, r.z], rtol=1e-8, atol=1e-10)
+        else:
+            np.testing.assert_allclose(a.model.coef_, r.coef, rtol=1e-8, atol=1e-10)
+
+
+def test_level_batched_mixed_build_equals_plain_per_node_build():
+    """The level-batched build (one split launch per cohort, cohort top-ups,
+    one batched fit per cohort in the mixed form with FP64 refinement, CUDA
+    graphs) and the plain per-node build (FP64 fits, one split call, one
+    top-up and one fit per node), with the same random stream and device
+    draws and two refinement rounds: the same tree, and held-out RMSE within
+    1e-6 relative."""
+    from art import SplitNode
+
+    f = target_from(TG["t1_target"])
+    common = dict(max_iters=60, min_side=16, max_depth=4, sample_count=1024, random_state=5, traversal="bfs",
+                  refinement_rounds=2, refinement_points=256, refinement_leaves=4)
+    fast = _c1_builder(f, level_dispatch=True, batched_fits=True, cohort_top_up=True, cuda_graphs=True,
+                       fit_precision="mixed", **dict(common)).build()
+    plain = _c1_builder(f, level_dispatch=False, batched_fits=False, cohort_top_up=False, cuda_graphs=False,
+                        fit_precision="fp64", **dict(common)).build()
+    na, nb = list(fast.tree.iter_nodes()), list(plain.tree.iter_nodes())
+    assert [n.node_id for n in na] == [n.node_id for n in nb] and len(na) > 5
+    assert [n.status for n in na] == [n.status for n in nb]
+    assert fast.oracle_queries == plain.oracle_queries
+    for a, b in zip(na, nb):
+        if isinstance(a, SplitNode):
+            np.testing.assert_allclose(np.r_[a.w, a.z], np.r_[b.w, b.z], rtol=1e-8, atol=1e-10)
+        else:
+            np.testing.assert_allclose(a.model.coef_, b.model.coef_, rtol=1e-8, atol=1e-10)
+    X = np.random.default_rng(3).uniform(-1, 1, (4000, 2))
+    y = f(X)
+    ra = np.sqrt(np.mean((fast.tree.predict(X) - y) ** 2))
+    rb = np.sqrt(np.mean((plain.tree.predict(X) - y) ** 2))
+    assert abs(ra - rb) <= 1e-6 * rb

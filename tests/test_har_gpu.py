@@ -242,7 +242,8 @@ def test_c4_polytope_chains_are_uniform_ks_and_decorrelate(d, k, seed):
     from the ball's centre, the last state of each after the burn-in is one
     independent draw; each coordinate passes a two-sample KS test against an
     exactly uniform rejection sample (p > 1e-4 for every coordinate), and the
-    thinned series decorrelate (median lag-20 autocorrelation below 0.2).
+    thinned series decorrelate (median autocorrelation below 0.2 at a lag of
+    200 steps for d = 8 and 2,000 steps for d = 64).
     The burn-in is 2,000 steps at d = 8 and 20,000 at d = 64 (hit-and-run
     mixes in O(d^2) steps)."""
     from scipy.stats import ks_2samp
@@ -269,11 +270,13 @@ def test_c4_polytope_chains_are_uniform_ks_and_decorrelate(d, k, seed):
     exact = _rejection_in_chunks(Ao, bo, d, 4000, rng)
     pvals = [ks_2samp(draws[:, j], exact[:, j]).pvalue for j in range(d)]
     assert min(pvals) > 1e-4, min(pvals)
-    # autocorrelation of thinned series (continue 256 chains for 200 thinned rounds)
+    # autocorrelation of the thinned series of 256 continued chains: it
+    # decays, and is below 0.2 after 200 steps at d = 8 and 2,000 at d = 64
+    rounds, lag = (200, 20) if d <= 8 else (1000, 200)
     series, _, status = hit_and_run_device(polys, np.zeros(256, np.int32), draws[:256], burn_in=0, thinning=10,
-                                           n_rounds=200, mode="batched",
+                                           n_rounds=rounds, mode="batched",
                                            seeds=np.arange(256, dtype=np.uint64) + 10_000 * seed)
     S = series.cpu().numpy()
     proj = S @ (np.ones(d) / np.sqrt(d))
-    acf = H.autocorrelation_by_lag(proj, [1, 20])
-    assert np.median(acf[1]) < 0.2
+    acf = H.autocorrelation_by_lag(proj, [1, lag])
+    assert np.median(acf[1]) < 0.2 and np.median(acf[1]) < np.median(acf[0])
