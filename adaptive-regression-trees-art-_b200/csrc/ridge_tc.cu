@@ -33,6 +33,7 @@
 #include <algorithm>
 
 #include "ridge.cuh"
+#include "tcgen05.cuh"
 
 namespace art {
 namespace {
@@ -53,69 +54,9 @@ constexpr int kMaxRefine = 14;
 // partial Grams are summed in shared memory with round-to-nearest adds.
 constexpr int kDrainChunks = 4;
 
-// ------------------------------------------------------------- PTX wrappers
-__device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t ncols) {
-  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                   smem_u32(dst)),
-               "r"(ncols)
-               : "memory");
-}
-__device__ __forceinline__ void tmem_relinquish() {
-  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
-  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
-               : "memory");
-}
-__device__ __forceinline__ void tc_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
-                                         uint32_t idesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
-      : "memory");
-}
-__device__ __forceinline__ void mma_commit(uint64_t* bar) {
-  asm volatile(
-      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-          smem_u32(bar))
-      : "memory");
-}
-// 32 lanes x 16 consecutive 32-bit columns; waits for completion.
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
 // Shared-memory matrix descriptor: K-major, no swizzle (layout type 0),
 // LBO = K-direction core-matrix stride, SBO = 8-row group stride, version 1.
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
-  return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)(kLBO >> 4) << 16) |
-         ((uint64_t)(kSBO >> 4) << 32) | (1ull << 46);
-}
-// Instruction descriptor, kind::tf32: D = F32 (bits 4-5 = 1), A = B = TF32
-// (format 2 at bits 7-9 and 10-12), both K-major, N >> 3 at bit 17, M >> 4 at 24.
-__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
-  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) |
-         ((uint32_t)(M >> 4) << 24);
-}
-
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) { return smem_desc_kmajor(addr, kLBO, kSBO); }
 // ------------------------------------------------------------- smem layout
 struct TcLayout {
   size_t x[2], y[2], w[2], q, sq, op, bars, tmem, gram, vec, fidx, total;
@@ -142,12 +83,6 @@ __host__ __device__ inline TcLayout tc_layout(int pmax, int dmax, int factor_byt
   return L;
 }
 
-// FP32 -> TF32 bit pattern, round to nearest (ties away), low 13 bits zero.
-__device__ __forceinline__ uint32_t to_tf32(float v) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
-  return r;
-}
 
 struct TcState {
   uint32_t load_issued[2];

@@ -28,6 +28,7 @@
 #include "bulk.cuh"
 #include "common.cuh"
 #include "linalg.cuh"
+#include "tcgen05.cuh"
 
 namespace art {
 namespace {
@@ -54,6 +55,21 @@ constexpr int kGangMax = 16;
 // work items to finish: that wait is bounded by a longer limit than the
 // in-pass barriers (members then run side by side).
 constexpr uint64_t kGangFormNs = 60ull * 1000000000ull;
+// Mixed form, soft passes: the side Grams on the tensor cores.  Chunks of
+// kTcRows rows; operand A = the entries P_e = psi_i psi_j of vech([phi; y]
+// [phi; y]^T) as 256 M-rows (two M = 128 tiles, entries >= E zero), operand
+// B = the weights q_L, q_R of every restart as N = 16 or 32 rows, both TF32
+// hi + lo in the K-major core-matrix layout (8 rows x 16 bytes per core
+// matrix, no swizzle); D[e][c] = sum_k P_e q_c accumulates in TMEM for
+// kTcDrain chunks, then is added into the FP64 Gram in shared memory.
+constexpr int kTcRows = 32;
+constexpr int kTcEntries = 256;
+constexpr int kTcLBO = 128;                          // bytes between K-adjacent core matrices
+constexpr int kTcSBO = (kTcRows / 4) * 128;          // bytes between 8-row groups
+constexpr int kTcAOp = (kTcEntries / 8) * kTcSBO;    // one A array (hi or lo): 32 KB
+constexpr int kTcBOp = (32 / 8) * kTcSBO;            // one B array: 4 KB
+constexpr int kTcDrain = 4;
+constexpr uint32_t kTcCols = 64;                     // TMEM columns: two tiles x N <= 32
 
 struct SplitArgs {
   int64_t K;
@@ -74,6 +90,7 @@ struct SplitArgs {
   ArtSplitParams prm;
   int R, Rg, groups, dmax, pmax, H, TC, S, CH;
   int mixed;  // ART_PRECISION_MIXED: gates in single precision
+  int tc;     // mixed form with the soft-pass Grams on the tensor cores
   // per (node, restart) results, index k * R + r
   double* r_theta;   // [.. ][dmax + 1]
   double* r_loss;
@@ -105,10 +122,10 @@ struct SplitArgs {
 // mbarriers.
 struct SLayout {
   size_t ring, rx, rstage, bars, xp, phi, q, G, cache, theta, dirn, grad, lastf, bl, br, trial, red, chol, eidx, rs,
-      total;
+      tcop, tcbar, total;
 };
 __host__ __device__ inline size_t al(size_t v) { return (v + 15) & ~(size_t)15; }
-__host__ __device__ inline SLayout split_layout(int dmax, int pmax, int Rg, int H, int S, int CH) {
+__host__ __device__ inline SLayout split_layout(int dmax, int pmax, int Rg, int H, int S, int CH, int tc = 0) {
   SLayout L;
   const int pa = pmax + 1, E = pa * (pa + 1) / 2, dt = dmax + 1;
   size_t o = 0;
@@ -134,6 +151,12 @@ __host__ __device__ inline SLayout split_layout(int dmax, int pmax, int Rg, int 
   L.chol = o; o = al(o + (size_t)kWarps * (E + 2 * pa) * 8);
   L.eidx = o; o = al(o + (size_t)E * 2 * 2);
   L.rs = o; o = al(o + (size_t)Rg * 32 * 8);  // per-restart scalar state
+  L.tcop = L.tcbar = 0;
+  if (tc) {  // operands (A hi, A lo, B hi, B lo), 1 KB aligned, then the MMA barrier and TMEM slot
+    o = (o + 1023) & ~(size_t)1023;
+    L.tcop = o; o += 2 * (size_t)kTcAOp + 2 * (size_t)kTcBOp;
+    L.tcbar = o; o = al(o + 16);
+  }
   L.total = o;
   return L;
 }
@@ -246,8 +269,11 @@ struct SplitCta {
   int16_t* eidx;
   int tid, lane, warp;
 
+  // tensor-core Gram state: MMA commits issued / waited on the barrier, TMEM base
+  uint32_t tc_commits = 0, tc_waits = 0, tmem = 0;
+
   __device__ SplitCta(const SplitArgs& a_, unsigned char* sm_) : a(a_), sm(sm_) {
-    L = split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S, a.CH);
+    L = split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S, a.CH, a.tc);
     rbar = (uint64_t*)(sm + L.bars);
     xs = (const double*)(sm + L.ring); ys = xs; phi = (double*)(sm + L.phi);
     xp = (double*)(sm + L.xp);
@@ -510,16 +536,168 @@ struct SplitCta {
     }
   }
 
+  // Bounded wait for every MMA committed so far.
+  __device__ bool tc_wait_all() {
+    uint64_t* bar = (uint64_t*)(sm + L.tcbar);
+    bool ok = true;
+    while (ok && tc_waits < tc_commits) {
+      ok = mbar_wait(bar, tc_waits & 1u);
+      if (ok) ++tc_waits;
+    }
+    return ok;
+  }
+
+  // ---- soft Gram pass on the tensor cores (mixed form).  Same sums as
+  // gram_pass(false): for every (restart, side) column c, G[c][e] =
+  // sum_k q_c(k) P_e(k), stored column-major (G + c * E) for solve_all.
+  // Gates: FP64 scores, single-precision logistic pair q_R = sigma(s),
+  // q_L = sigma(-s) (each accurate relative to itself, so a side with small
+  // weights keeps its precision), floored as in the FP64 form.  Products
+  // P_e = psi_i psi_j in FP64, split into TF32 hi + lo; three tensor-core
+  // products hi hi + hi lo + lo hi per K-step, FP32 accumulation in TMEM over
+  // kTcDrain chunks (128 rows), FP64 accumulation across drains.
+  __device__ void gram_pass_tc() {
+    const int E = it.E, C2 = 2 * a.Rg, N = C2 <= 16 ? 16 : 32;
+    unsigned char* Ahi = sm + L.tcop;
+    unsigned char* Alo = Ahi + kTcAOp;
+    unsigned char* Bhi = Alo + kTcAOp;
+    unsigned char* Blo = Bhi + kTcBOp;
+    uint64_t* bar = (uint64_t*)(sm + L.tcbar);
+    for (int i = tid; i < E * C2; i += kSplitThreads) G[i] = 0.0;
+    const uint32_t idesc = idesc_tf32(128, N);
+    const int nB = a.Rg * (kTcRows / 8), nA = E * (kTcRows / 8);
+    int64_t chunk = 0;
+    begin_pass();
+    for (int64_t c0 = (int64_t)grank * a.CH; c0 < it.n; c0 += (int64_t)gsize * a.CH, ++chunk) {
+      const int rows = load_chunk(c0);
+      // the operand buffers are free once every earlier MMA has completed
+      const bool okw = tc_wait_all();
+      if (!__syncthreads_and(okw)) {
+        rabort = true;
+        if (tid == 0) atomicExch(&a.counts[kErrSlot], 1);
+      }
+      // items: (restart, octet of rows) -> gates; (entry, octet) -> products
+      for (int j = tid; j < nB + nA; j += kSplitThreads) {
+        if (j < nB) {
+          const int r = j / (kTcRows / 8), oct = j - r * (kTcRows / 8);
+          uint32_t lh[8], ll[8], rh[8], rl[8];
+          const bool on = r < it.rn && S(r, RS_ACTIVE) != 0.0;
+          const double invt = S(r, RS_INVT), z = th[r * dt() + it.d];
+#pragma unroll
+          for (int e8 = 0; e8 < 8; ++e8) {
+            const int row = oct * 8 + e8;
+            float qL = 0.0f, qR = 0.0f;
+            if (on && row < rows) {
+              const float sf = fminf(fmaxf((float)((score(r, row) - z) * invt), -50.0f), 50.0f);
+              const float en = __expf(-sf);
+              qR = __frcp_rn(1.0f + en);
+              qL = en * qR;
+              qR = fmaxf(qR, (float)a.prm.weight_floor);
+              qL = fmaxf(qL, (float)a.prm.weight_floor);
+            }
+            lh[e8] = to_tf32(qL);
+            ll[e8] = to_tf32(qL - __uint_as_float(lh[e8]));
+            rh[e8] = to_tf32(qR);
+            rl[e8] = to_tf32(qR - __uint_as_float(rh[e8]));
+          }
+          const int cl = 2 * r, cr = 2 * r + 1;
+          const size_t ol = (size_t)(cl >> 3) * kTcSBO + (size_t)(2 * oct) * 128 + (size_t)(cl & 7) * 16;
+          const size_t orr = (size_t)(cr >> 3) * kTcSBO + (size_t)(2 * oct) * 128 + (size_t)(cr & 7) * 16;
+          *(uint4*)(Bhi + ol) = make_uint4(lh[0], lh[1], lh[2], lh[3]);
+          *(uint4*)(Bhi + ol + 128) = make_uint4(lh[4], lh[5], lh[6], lh[7]);
+          *(uint4*)(Blo + ol) = make_uint4(ll[0], ll[1], ll[2], ll[3]);
+          *(uint4*)(Blo + ol + 128) = make_uint4(ll[4], ll[5], ll[6], ll[7]);
+          *(uint4*)(Bhi + orr) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+          *(uint4*)(Bhi + orr + 128) = make_uint4(rh[4], rh[5], rh[6], rh[7]);
+          *(uint4*)(Blo + orr) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+          *(uint4*)(Blo + orr + 128) = make_uint4(rl[4], rl[5], rl[6], rl[7]);
+        } else {
+          const int jj = j - nB;
+          const int e = jj % E, oct = jj / E;
+          const int fi = eidx[2 * e], fj = eidx[2 * e + 1];
+          uint32_t ph[8], pl[8];
+#pragma unroll
+          for (int e8 = 0; e8 < 8; ++e8) {
+            const int row = oct * 8 + e8;
+            float v = 0.0f;
+            if (row < rows) {
+              const double* pr = phi + row * phs;
+              v = (float)(pr[fi] * pr[fj]);
+            }
+            ph[e8] = to_tf32(v);
+            pl[e8] = to_tf32(v - __uint_as_float(ph[e8]));
+          }
+          const size_t off = (size_t)(e >> 3) * kTcSBO + (size_t)(2 * oct) * 128 + (size_t)(e & 7) * 16;
+          *(uint4*)(Ahi + off) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
+          *(uint4*)(Ahi + off + 128) = make_uint4(ph[4], ph[5], ph[6], ph[7]);
+          *(uint4*)(Alo + off) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+          *(uint4*)(Alo + off + 128) = make_uint4(pl[4], pl[5], pl[6], pl[7]);
+        }
+      }
+      fence_proxy_async();  // operand writes -> visible to the tensor core
+      __syncthreads();
+      const bool fresh = (chunk % kTcDrain) == 0;
+      if (tid == 0 && !rabort) {
+        tc_fence_after();
+        const uint32_t ah = smem_u32(Ahi), alo = smem_u32(Alo), bh = smem_u32(Bhi), blo = smem_u32(Blo);
+#pragma unroll
+        for (int ks = 0; ks < kTcRows / 8; ++ks) {
+          const uint32_t ko = (uint32_t)ks * 2u * kTcLBO;  // 8 rows = two K-adjacent core matrices
+#pragma unroll
+          for (int prod = 0; prod < 3; ++prod) {
+            const uint32_t A = (prod == 2) ? alo : ah;
+            const uint32_t B = (prod == 1) ? blo : bh;
+            const uint32_t acc = (fresh && ks == 0 && prod == 0) ? 0u : 1u;
+#pragma unroll
+            for (int t = 0; t < 2; ++t)
+              mma_tf32(tmem + (uint32_t)(t * N), smem_desc_kmajor(A + (uint32_t)t * 16u * kTcSBO + ko, kTcLBO, kTcSBO),
+                       smem_desc_kmajor(B + ko, kTcLBO, kTcSBO), idesc, acc);
+          }
+        }
+        mma_commit(bar);
+      }
+      if (!rabort) ++tc_commits;
+      const bool seg_end = ((chunk + 1) % kTcDrain) == 0 || c0 + (int64_t)gsize * a.CH >= it.n;
+      if (seg_end && !rabort) {
+        const bool ok = tc_wait_all();
+        if (!__syncthreads_and(ok)) {
+          rabort = true;
+          if (tid == 0) atomicExch(&a.counts[kErrSlot], 1);
+        } else {
+          tc_fence_after();
+          // warps 0-3: tile 0 (entries 0..127); warps 4-7: tile 1 (128..255)
+          const int quarter = warp & 3, t = warp >> 2;
+          const int e = t * 128 + quarter * 32 + lane;
+          const uint32_t lane_base = tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(t * N);
+          for (int cb = 0; cb < N; cb += 16) {
+            float v[16];
+            tmem_ld16(lane_base + (uint32_t)cb, v);
+            if (e < E) {
+#pragma unroll
+              for (int q = 0; q < 16; ++q)
+                if (cb + q < C2) G[(size_t)(cb + q) * E + e] += (double)v[q];
+            }
+          }
+          tc_fence_before();
+        }
+      }
+      __syncthreads();
+    }
+    if (gsize > 1) gang_reduce(G, E * C2);
+  }
+
   // ---- trace-scaled ridge + Cholesky + solve for every (restart, side).
   // One warp per system; a failed factorisation marks the restart.
-  __device__ void solve_all() {
+  // `colmajor`: the Grams are stored G[c * E + e] (tensor-core pass) instead
+  // of G[e * C2 + c].
+  __device__ void solve_all(bool colmajor = false) {
     const int p = it.p, pa = it.pa, E = it.E, C2 = 2 * a.Rg;
     double* A = chol + (size_t)warp * (E + 2 * pa);
     double* z = A + E;
     for (int c = warp; c < 2 * it.rn; c += kWarps) {
       const int r = c >> 1, side = c & 1;
       if (S(r, RS_ACTIVE) == 0.0) continue;
-      for (int e = lane; e < E; e += 32) A[e] = G[(size_t)e * C2 + c];
+      for (int e = lane; e < E; e += 32) A[e] = colmajor ? G[(size_t)c * E + e] : G[(size_t)e * C2 + c];
       __syncwarp();
       double tr = 0.0;
       if (lane == 0)
@@ -904,8 +1082,13 @@ __device__ void SplitCta<TC>::run(int item_id, int rank, int members) {
   }
   // ---------------------------------------------------------- evaluate(theta)
   auto evaluate = [&]() {
-    gram_pass(false);
-    solve_all();
+    if (a.tc) {
+      gram_pass_tc();
+      solve_all(true);
+    } else {
+      gram_pass(false);
+      solve_all();
+    }
     if (tid < it.rn && S(tid, RS_ACTIVE) != 0.0 && S(tid, RS_CHOLBAD) != 0.0) {
       S(tid, RS_ACTIVE) = 0.0;
       S(tid, RS_FAIL) = ART_SPLIT_CHOLESKY_FAILURE;
@@ -1206,11 +1389,28 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) split_kernel(SplitArgs a)
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_item;
   SplitCta<TC> cta(a, smem);
+  __shared__ uint32_t s_tmem;
   if (threadIdx.x == 0) {
     for (int i = 0; i < a.S; ++i) mbar_init(&cta.rbar[i], 1);
+    if (a.tc) mbar_init((uint64_t*)(smem + cta.L.tcbar), 1);
     fence_mbar_init();
   }
+  if (a.tc) {
+    // operand rows that no item writes (entries >= E, columns >= 2 Rg) stay zero
+    uint4* op = (uint4*)(smem + cta.L.tcop);
+    for (int i = threadIdx.x; i < (2 * kTcAOp + 2 * kTcBOp) / 16; i += kSplitThreads) op[i] = make_uint4(0, 0, 0, 0);
+    fence_proxy_async();
+    if ((threadIdx.x >> 5) == 0) {
+      tmem_alloc(&s_tmem, kTcCols);
+      tmem_relinquish();
+    }
+    tc_fence_before();
+  }
   __syncthreads();
+  if (a.tc) {
+    tc_fence_after();
+    cta.tmem = s_tmem;
+  }
   const int count = a.counts[0];
   for (;;) {
     if (threadIdx.x == 0) s_item = atomicAdd(&a.counts[1], 1);
@@ -1222,6 +1422,13 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) split_kernel(SplitArgs a)
     cta.run(e.x, e.y, e.z);
   }
   cta.ring_drain();
+  if (a.tc) {  // release TMEM after a bounded wait for this CTA's MMAs
+    cta.tc_wait_all();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if ((threadIdx.x >> 5) == 0) tmem_dealloc(cta.tmem, kTcCols);
+  }
 }
 
 // Per node: best non-fallback restart by hard loss, else best fallback,
@@ -1436,8 +1643,27 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
   }
   const int R = prm->n_restarts;
   int TC = 2;
-  const int Rg = choose_rg(R, pr->max_features + 1, prm->group_restarts, TC);
+  int Rg = choose_rg(R, pr->max_features + 1, prm->group_restarts, TC);
   if (Rg < 1) { set_error("art_split_level: model too large for the split kernel"); return ART_E_UNSUPPORTED; }
+  // Mixed form: the soft-pass Grams go to the tensor cores when the entries
+  // fit two M = 128 tiles and the operands fit shared memory next to the
+  // rest; all restarts of a node (up to 16) then share one CTA and one
+  // operand generation per chunk.
+  int use_tc = 0;
+  {
+    const int pa = pr->max_features + 1, E = pa * (pa + 1) / 2;
+    if (prm->precision == ART_PRECISION_MIXED && E <= kTcEntries) {
+      int tc_cols = 2;
+      const int rg = choose_rg(R, pa, 0, tc_cols);
+      const int H = std::min(std::min(prm->trial_steps > 0 ? prm->trial_steps : 4, std::max(1, kSplitThreads / std::max(rg, 1))),
+                             prm->max_backtracks + 1);
+      if (rg >= 1 && split_layout(pr->max_dim, pr->max_features, rg, H, 2, kTcRows, 1).total <= 227 * 1024) {
+        use_tc = 1;
+        Rg = rg;
+        TC = tc_cols;
+      }
+    }
+  }
   const SplitWs wl = split_ws(K, R, pr->max_dim, pr->max_features);
   if (!workspace || ws_bytes < wl.total) {
     set_error("art_split_level: workspace %zu bytes < required %zu", ws_bytes, wl.total);
@@ -1457,6 +1683,7 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
   a.R = R; a.Rg = Rg; a.groups = (R + Rg - 1) / Rg;
   a.dmax = pr->max_dim; a.pmax = pr->max_features; a.TC = TC;
   a.mixed = prm->precision == ART_PRECISION_MIXED ? 1 : 0;
+  a.tc = use_tc;
   // default: four speculative Armijo steps per trial pass (adaptive step
   // sizes are usually accepted within the first two; longer backtracks take
   // further passes), spare threads share the rows instead
@@ -1507,15 +1734,23 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
   // ring for that chunk; two CTAs per SM fall back to one when even the
   // shortest chunk does not fit half the SM's shared memory
   int minb = prm->ctas_per_sm == 2 ? 2 : 1;
-  if (minb == 2 && split_layout(a.dmax, a.pmax, a.Rg, a.H, 1, 32).total > kHalfSmem) minb = 1;
-  const size_t chunk_budget = minb == 2 ? 100 * 1024 : 200 * 1024;
-  const size_t smem_budget = minb == 2 ? kHalfSmem : 227 * 1024;
-  const int min_stages = minb == 2 ? 2 : 4;
-  a.CH = kMaxCH;
-  while (a.CH > 32 && split_layout(a.dmax, a.pmax, a.Rg, a.H, min_stages, a.CH).total > chunk_budget) a.CH >>= 1;
-  a.S = kMaxStages;
-  while (a.S > 1 && split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S, a.CH).total > smem_budget) --a.S;
-  const size_t smem = split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S, a.CH).total;
+  if (a.tc) {
+    // one CTA per SM: chunks of kTcRows rows and the deepest ring that fits
+    minb = 1;
+    a.CH = kTcRows;
+    a.S = kMaxStages;
+    while (a.S > 2 && split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S, a.CH, 1).total > 227 * 1024) --a.S;
+  } else {
+    if (minb == 2 && split_layout(a.dmax, a.pmax, a.Rg, a.H, 1, 32).total > kHalfSmem) minb = 1;
+    const size_t chunk_budget = minb == 2 ? 100 * 1024 : 200 * 1024;
+    const size_t smem_budget = minb == 2 ? kHalfSmem : 227 * 1024;
+    const int min_stages = minb == 2 ? 2 : 4;
+    a.CH = kMaxCH;
+    while (a.CH > 32 && split_layout(a.dmax, a.pmax, a.Rg, a.H, min_stages, a.CH).total > chunk_budget) a.CH >>= 1;
+    a.S = kMaxStages;
+    while (a.S > 1 && split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S, a.CH).total > smem_budget) --a.S;
+  }
+  const size_t smem = split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S, a.CH, a.tc).total;
   if (smem > 227 * 1024) { set_error("art_split_level: shared memory %zu too large", smem); return ART_E_UNSUPPORTED; }
   auto launch = [&](auto kern) -> int {
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
