@@ -291,10 +291,13 @@ class ServingEngine:
         # distinct value); the minimum side count goes per node, so nodes of
         # every dimension share a launch.  A node's split never depends on the
         # jobs it is batched with.
-        groups: dict[int, list[int]] = {}
+        # the mixed form's tensor-core split Gram takes models of at most 21
+        # features; nodes of larger models go to a launch of their own
+        groups: dict[tuple, list[int]] = {}
         for k in split_idx:
-            groups.setdefault(work[k][0].job.max_iters, []).append(k)
-        for iters, ks in sorted(groups.items()):
+            job = work[k][0].job
+            groups.setdefault((job.max_iters, job.n_features <= 21), []).append(k)
+        for (iters, _), ks in sorted(groups.items()):
             self._split([work[k] for k in ks], x, y, ro, xo, d, kinds, ks, iters)
 
     def _split(self, sub, x, y, ro, xo, d, kinds, idx, iters) -> None:
@@ -313,7 +316,7 @@ class ServingEngine:
         min_side = np.array([st.min_side for st, _ in sub], dtype=np.int32)
         sp = SoftObliqueSplitter(AffineRidgeModel(ridge=1e-6), 1.0, max_iters=iters, grad_atol=1e-8,
                                  grad_rtol=1e-5, min_side_points=int(min_side.min()), min_side_fraction=0.0,
-                                 n_restarts=1)
+                                 n_restarts=1, precision=self.precision)
         res = split_level(sp, xs, ys, sro, dd, kinds[idx], temps, ridge, x_offsets=sxo, hard_refit=False,
                           node_keys=keys, max_dim=int(dd.max()), max_features=int(max(st.job.n_features for st, _ in sub)),
                           min_side_points=min_side, group_restarts=0, trial_steps=0, ctas_per_sm=0,
@@ -351,7 +354,9 @@ class ServingEngine:
             st.frontier.append(_Node(nd.path + "R", nd.depth + 1, nd.r0 + nl, nd.r1, nd.rows + [(-w, -z)]))
 
     # ------------------------------------------------------------ rounds
-    _CHAINS = 8
+    _CHAINS = 8            # fewest chains per refined leaf
+    _MAX_CHAINS = 256      # most chains per refined leaf
+    _PER_CHAIN = 128       # target samples per chain
 
     def _refine_all(self, states: list[_JobState]) -> None:
         """One adaptive round for every given job: grow_fraction * n0 new
@@ -374,9 +379,13 @@ class ServingEngine:
         by_dim: dict[int, list] = {}
         for plan in plans:
             by_dim.setdefault(plan[0].job.dim, []).append(plan)
-        ch = self._CHAINS
         for dim, group in sorted(by_dim.items()):
             leaves_all = [(st, nd, per[i]) for st, leaves, per in group for i, nd in enumerate(leaves)]
+            # a leaf's samples come from several short chains (one long chain
+            # is a sequential walk of n * thinning steps); each chain starts at
+            # the leaf's sample mean and burns in 20 + 2 d steps
+            chains = [int(min(self._MAX_CHAINS, max(self._CHAINS, -(-n // self._PER_CHAIN))))
+                      for _, _, n in leaves_all]
             dev = group[0][0].X.device
             m = len(leaves_all)
             A = [np.asarray(w, float) for _, nd, _ in leaves_all for w, _ in nd.rows]
@@ -388,15 +397,18 @@ class ServingEngine:
                 t.as_tensor(np.array(A).reshape(-1, dim) if A else np.zeros((1, dim)), device=dev),
                 t.as_tensor(np.array(bb) if bb else np.zeros(1), device=dev), max(1, int(np.diff(rof).max())))
             # start every chain at its leaf's sample mean (inside the convex leaf)
-            x0 = t.stack([st.X[nd.r0:nd.r1].mean(0) for st, nd, _ in leaves_all]).repeat_interleave(ch, 0)
-            cpoly = np.repeat(np.arange(m, dtype=np.int32), ch)
-            seeds = np.array([_key(st.job.seed, "har", st.round, nd.path, c) for st, nd, _ in leaves_all
-                              for c in range(ch)], dtype=np.uint64)
-            n_rounds = max(1, -(-max(n for _, _, n in leaves_all) // ch))
-            samples, _, status = hit_and_run_device(polys, cpoly, x0, burn_in=20, thinning=10, n_rounds=n_rounds,
-                                                    seeds=seeds, stream=self.stream)
+            means = t.stack([st.X[nd.r0:nd.r1].mean(0) for st, nd, _ in leaves_all])
+            cnt = t.as_tensor(np.asarray(chains), device=dev)
+            x0 = means.repeat_interleave(cnt, 0)
+            cpoly = np.repeat(np.arange(m, dtype=np.int32), chains)
+            seeds = np.array([_key(st.job.seed, "har", st.round, nd.path, c) for (st, nd, _), ch in
+                              zip(leaves_all, chains) for c in range(ch)], dtype=np.uint64)
+            n_rounds = max(1, max(-(-n // ch) for (_, _, n), ch in zip(leaves_all, chains)))
+            samples, _, status = hit_and_run_device(polys, cpoly, x0, burn_in=20 + 2 * dim, thinning=10,
+                                                    n_rounds=n_rounds, seeds=seeds, stream=self.stream)
+            first = np.concatenate([[0], np.cumsum(chains)])
             for i, (st, nd, n) in enumerate(leaves_all):
-                nd._new = samples[:, i * ch:(i + 1) * ch, :].reshape(-1, dim)[:n]
+                nd._new = samples[:, first[i]:first[i + 1], :].reshape(-1, dim)[:n]
         for st, leaves, _ in plans:
             self._reopen(st, {nd.path for nd in leaves})
 

@@ -1505,41 +1505,100 @@ __global__ void split_init_theta(SplitArgs a, double* theta0, int64_t stride) {
     for (int i = 0; i < d; ++i) w[i] /= nrm;
   }
   __syncthreads();
-  // median of u = X w: order statistics by bisection on the ordered 64-bit
-  // keys of the doubles (count(key(u) <= t) is monotone; <= 64 passes)
-  __shared__ long long red_c[32];
-  // monotone map of doubles to int64: +x -> bits, -x (magnitude bits m) -> -m - 1
-  auto key = [](double v) -> long long {
-    const long long b = __double_as_longlong(v);
-    return b >= 0 ? b : -(b & 0x7FFFFFFFFFFFFFFFll) - 1;
+  // median of u = X w by a radix select on the order-preserving 64-bit image
+  // of the doubles (sign bit flipped for positives, all bits flipped for
+  // negatives): six digit passes of up to 11 bits narrow a prefix to the
+  // exact key of the m-th smallest u, each pass recomputing u and counting
+  // the rows that share the prefix into a shared histogram.
+  constexpr int kBins = 2048;
+  __shared__ unsigned int hist[kBins];
+  __shared__ unsigned long long s_pre;
+  __shared__ long long s_m;
+  auto ukey = [](double v) -> unsigned long long {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
   };
-  auto kth = [&](long long m) {
-    long long lo = key(-INFINITY), hi = key(INFINITY);
-    for (int it = 0; it < 70 && lo < hi; ++it) {
-      const long long mid = lo + (long long)(((unsigned long long)hi - (unsigned long long)lo) >> 1);
-      long long c = 0;
+  auto from_ukey = [](unsigned long long k) -> double {
+    return __longlong_as_double((long long)((k >> 63) ? (k & 0x7FFFFFFFFFFFFFFFull) : ~k));
+  };
+  auto u_of = [&](int64_t i) {
+    double u = 0.0;
+    for (int cc = 0; cc < d; ++cc) u = fma(a.x[xoff + i * d + cc], w[cc], u);
+    return u;
+  };
+  auto kth = [&](long long m) -> unsigned long long {
+    unsigned long long prefix = 0ull, mask = 0ull;
+    // digits (shift, width): bits 53..63, 42..52, 31..41, 20..30, 9..19, 0..8
+    for (int pass = 0; pass < 6; ++pass) {
+      const int sh = pass < 5 ? 53 - 11 * pass : 0;
+      const int width = pass < 5 ? 11 : 9;
+      const unsigned long long dmask = (1ull << width) - 1ull;
+      for (int b = threadIdx.x; b < kBins; b += blockDim.x) hist[b] = 0u;
+      __syncthreads();
       for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
-        double u = 0.0;
-        for (int cc = 0; cc < d; ++cc) u = fma(a.x[xoff + i * d + cc], w[cc], u);
-        c += (key(u) <= mid);
+        const unsigned long long k = ukey(u_of(i));
+        if ((k & mask) == prefix) atomicAdd(&hist[(k >> sh) & dmask], 1u);
       }
-      for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-      if ((threadIdx.x & 31) == 0) red_c[threadIdx.x >> 5] = c;
       __syncthreads();
-      long long tot = 0;
-      for (int i = 0; i < (int)(blockDim.x >> 5); ++i) tot += red_c[i];
+      if (threadIdx.x < 32) {
+        // warp 0: lane l sums bins [64 l, 64 l + 64); an exclusive scan over
+        // the lanes finds the lane holding rank m, which scans its own bins
+        const int l = threadIdx.x;
+        long long part = 0;
+        for (int b = 64 * l; b < 64 * l + 64; ++b) part += hist[b];
+        long long incl = part;
+        for (int o = 1; o < 32; o <<= 1) {
+          const long long t = __shfl_up_sync(0xffffffffu, incl, o);
+          if (l >= o) incl += t;
+        }
+        const long long excl = incl - part;
+        const unsigned hit = __ballot_sync(0xffffffffu, m >= excl && m < incl);
+        const int owner = hit ? __ffs(hit) - 1 : 31;
+        if (l == owner) {
+          long long mm = m - excl;
+          int b = 64 * l;
+          for (; b < 64 * l + 63; ++b) {
+            if (mm < (long long)hist[b]) break;
+            mm -= hist[b];
+          }
+          s_pre = prefix | ((unsigned long long)b << sh);
+          s_m = mm;
+        }
+      }
       __syncthreads();
-      if (tot > m) hi = mid; else lo = mid + 1;
+      prefix = s_pre;
+      m = s_m;
+      mask |= dmask << sh;
+      __syncthreads();
     }
-    const long long b = lo;
-    return __longlong_as_double(b >= 0 ? b : ((-(b + 1)) | (long long)0x8000000000000000ull));
+    return prefix;
   };
   if (n == 0) {
     if (threadIdx.x == 0) { for (int i = 0; i < d; ++i) theta0[kr * stride + i] = w[i]; theta0[kr * stride + d] = 0.0; }
     return;
   }
-  const double v1 = kth((n - 1) / 2);
-  const double v2 = (n % 2 == 0) ? kth(n / 2) : v1;
+  const unsigned long long k1 = kth((n - 1) / 2);
+  const double v1 = from_ukey(k1);
+  double v2 = v1;
+  if (n % 2 == 0) {
+    // the next order statistic: v1 again if more than n/2 keys are <= k1,
+    // else the smallest u above v1
+    __shared__ unsigned long long s_min;
+    __shared__ long long s_cnt;
+    if (threadIdx.x == 0) { s_min = ~0ull; s_cnt = 0; }
+    __syncthreads();
+    long long cnt = 0;
+    unsigned long long mn = ~0ull;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+      const unsigned long long k = ukey(u_of(i));
+      if (k <= k1) ++cnt;
+      else if (k < mn) mn = k;
+    }
+    atomicAdd((unsigned long long*)&s_cnt, (unsigned long long)cnt);
+    atomicMin(&s_min, mn);
+    __syncthreads();
+    v2 = s_cnt > n / 2 ? v1 : from_ukey(s_min);
+  }
   if (threadIdx.x == 0) {
     for (int i = 0; i < d; ++i) theta0[kr * stride + i] = w[i];
     theta0[kr * stride + d] = (n % 2 == 0) ? 0.5 * (v1 + v2) : v1;

