@@ -291,13 +291,10 @@ class ServingEngine:
         # distinct value); the minimum side count goes per node, so nodes of
         # every dimension share a launch.  A node's split never depends on the
         # jobs it is batched with.
-        # the mixed form's tensor-core split Gram takes models of at most 21
-        # features; nodes of larger models go to a launch of their own
-        groups: dict[tuple, list[int]] = {}
+        groups: dict[int, list[int]] = {}
         for k in split_idx:
-            job = work[k][0].job
-            groups.setdefault((job.max_iters, job.n_features <= 21), []).append(k)
-        for (iters, _), ks in sorted(groups.items()):
+            groups.setdefault(work[k][0].job.max_iters, []).append(k)
+        for iters, ks in sorted(groups.items()):
             self._split([work[k] for k in ks], x, y, ro, xo, d, kinds, ks, iters)
 
     def _split(self, sub, x, y, ro, xo, d, kinds, idx, iters) -> None:
@@ -316,7 +313,7 @@ class ServingEngine:
         min_side = np.array([st.min_side for st, _ in sub], dtype=np.int32)
         sp = SoftObliqueSplitter(AffineRidgeModel(ridge=1e-6), 1.0, max_iters=iters, grad_atol=1e-8,
                                  grad_rtol=1e-5, min_side_points=int(min_side.min()), min_side_fraction=0.0,
-                                 n_restarts=1, precision=self.precision)
+                                 n_restarts=1)
         res = split_level(sp, xs, ys, sro, dd, kinds[idx], temps, ridge, x_offsets=sxo, hard_refit=False,
                           node_keys=keys, max_dim=int(dd.max()), max_features=int(max(st.job.n_features for st, _ in sub)),
                           min_side_points=min_side, group_restarts=0, trial_steps=0, ctas_per_sm=0,

@@ -165,7 +165,9 @@ def split_params(s: "SoftObliqueSplitter", hard_refit: bool, anneal_ratio: float
                  group_restarts: int = 0, trial_steps: int = 0, ctas_per_sm: int = 0):
     """ArtSplitParams of a splitter.  ``precision="mixed"`` evaluates the
     sigmoid gates in single precision (objective within 1e-5 relative of the
-    FP64 form); sums, solves and the side decisions stay FP64."""
+    FP64 form); solves and the side decisions stay FP64, and the soft-pass
+    side Grams are FP64 sums, or tensor-core TF32 hi/lo products with
+    ``tensor_gram=True``."""
 
     if getattr(s, "precision", "fp64") not in ("fp64", "mixed"):
         raise ValueError("precision must be 'fp64' or 'mixed'.")
@@ -177,7 +179,7 @@ def split_params(s: "SoftObliqueSplitter", hard_refit: bool, anneal_ratio: float
         int(s.max_line_search_failures), float(s.weight_floor), int(bool(hard_refit)),
         N.PRECISION_MIXED if getattr(s, "precision", "fp64") == "mixed" else N.PRECISION_FP64,
         float(anneal_ratio), int(seed) & ((1 << 64) - 1), int(group_restarts), int(trial_steps),
-        int(ctas_per_sm))
+        int(ctas_per_sm), int(bool(getattr(s, "tensor_gram", False)) and getattr(s, "precision", "fp64") == "mixed"))
 
 
 def split_level(splitter: "SoftObliqueSplitter", x, y, row_offsets, dims, features, temperature, ridge,
@@ -327,6 +329,7 @@ class SoftObliqueSplitter:
     qr_parallel: bool = True
     Xw_refresh: int = 32
     precision: Literal["fp64", "mixed"] = "fp64"
+    tensor_gram: bool = False
 
     def _validate_inputs(self, X: np.ndarray, y: np.ndarray) -> None:
         """splitters.py:732-750"""

@@ -137,9 +137,21 @@ __host__ __device__ inline SLayout split_layout(int dmax, int pmax, int Rg, int 
   // reading different rows of a chunk fall in different banks
   L.xp = o; o = al(o + (size_t)CH * (dmax | 1) * 8);
   L.phi = o; o = al(o + (size_t)CH * (pa | 1) * 8);
-  L.q = o; o = al(o + (size_t)CH * (2 * Rg + 1) * 8);
+  L.tcop = 0;
+  if (tc) {
+    // the weights Q (hard Gram pass), the row cache (residual and trial
+    // passes) and the tensor-core operands (soft Gram pass) are never live
+    // together: one region, 1 KB aligned for the operand descriptors
+    o = (o + 1023) & ~(size_t)1023;
+    const size_t qb = (size_t)CH * (2 * Rg + 1) * 8, cb = (size_t)CH * (4 * Rg + 4) * 8;
+    const size_t tb = 2 * (size_t)kTcAOp + 2 * (size_t)kTcBOp;
+    L.q = L.cache = L.tcop = o;
+    o = al(o + (qb > cb ? (qb > tb ? qb : tb) : (cb > tb ? cb : tb)));
+  } else {
+    L.q = o; o = al(o + (size_t)CH * (2 * Rg + 1) * 8);
+  }
   L.G = o; o = al(o + (size_t)E * 2 * Rg * 8);
-  L.cache = o; o = al(o + (size_t)CH * (4 * Rg + 4) * 8);
+  if (!tc) { L.cache = o; o = al(o + (size_t)CH * (4 * Rg + 4) * 8); }
   L.theta = o; o = al(o + (size_t)Rg * dt * 8);
   L.dirn = o; o = al(o + (size_t)Rg * dt * 8);
   L.grad = o; o = al(o + (size_t)Rg * dt * 8);
@@ -151,12 +163,8 @@ __host__ __device__ inline SLayout split_layout(int dmax, int pmax, int Rg, int 
   L.chol = o; o = al(o + (size_t)kWarps * (E + 2 * pa) * 8);
   L.eidx = o; o = al(o + (size_t)E * 2 * 2);
   L.rs = o; o = al(o + (size_t)Rg * 32 * 8);  // per-restart scalar state
-  L.tcop = L.tcbar = 0;
-  if (tc) {  // operands (A hi, A lo, B hi, B lo), 1 KB aligned, then the MMA barrier and TMEM slot
-    o = (o + 1023) & ~(size_t)1023;
-    L.tcop = o; o += 2 * (size_t)kTcAOp + 2 * (size_t)kTcBOp;
-    L.tcbar = o; o = al(o + 16);
-  }
+  L.tcbar = 0;
+  if (tc) { L.tcbar = o; o = al(o + 16); }  // the MMA completion barrier
   L.total = o;
   return L;
 }
@@ -564,12 +572,31 @@ struct SplitCta {
     unsigned char* Blo = Bhi + kTcBOp;
     uint64_t* bar = (uint64_t*)(sm + L.tcbar);
     for (int i = tid; i < E * C2; i += kSplitThreads) G[i] = 0.0;
+    // the operand region is shared with the other passes' buffers: the rows
+    // no item writes (entries >= E of A, columns >= 2 Rg of B) are cleared
+    // here, in both hi and lo, for all 8 K-adjacent core matrices
+    for (int i = tid; i < (kTcEntries - E) * 8; i += kSplitThreads) {
+      const int e = E + i / 8, kc = i % 8;
+      const size_t off = (size_t)(e >> 3) * kTcSBO + (size_t)kc * 128 + (size_t)(e & 7) * 16;
+      *(uint4*)(Ahi + off) = make_uint4(0, 0, 0, 0);
+      *(uint4*)(Alo + off) = make_uint4(0, 0, 0, 0);
+    }
+    for (int i = tid; i < (N - C2) * 8; i += kSplitThreads) {
+      const int c = C2 + i / 8, kc = i % 8;
+      const size_t off = (size_t)(c >> 3) * kTcSBO + (size_t)kc * 128 + (size_t)(c & 7) * 16;
+      *(uint4*)(Bhi + off) = make_uint4(0, 0, 0, 0);
+      *(uint4*)(Blo + off) = make_uint4(0, 0, 0, 0);
+    }
     const uint32_t idesc = idesc_tf32(128, N);
     const int nB = a.Rg * (kTcRows / 8), nA = E * (kTcRows / 8);
-    int64_t chunk = 0;
+    int64_t chunk = 0;  // sub-chunks of kTcRows rows issued in this pass
     begin_pass();
-    for (int64_t c0 = (int64_t)grank * a.CH; c0 < it.n; c0 += (int64_t)gsize * a.CH, ++chunk) {
-      const int rows = load_chunk(c0);
+    for (int64_t c0 = (int64_t)grank * a.CH; c0 < it.n; c0 += (int64_t)gsize * a.CH) {
+     const int crows = load_chunk(c0);
+     for (int sub = 0; sub * kTcRows < crows; ++sub, ++chunk) {
+      const int r0 = sub * kTcRows;
+      const int rows = min(kTcRows, crows - r0);
+      const bool last = c0 + (int64_t)gsize * a.CH >= it.n && r0 + kTcRows >= crows;
       // the operand buffers are free once every earlier MMA has completed
       const bool okw = tc_wait_all();
       if (!__syncthreads_and(okw)) {
@@ -588,7 +615,7 @@ struct SplitCta {
             const int row = oct * 8 + e8;
             float qL = 0.0f, qR = 0.0f;
             if (on && row < rows) {
-              const float sf = fminf(fmaxf((float)((score(r, row) - z) * invt), -50.0f), 50.0f);
+              const float sf = fminf(fmaxf((float)((score(r, r0 + row) - z) * invt), -50.0f), 50.0f);
               const float en = __expf(-sf);
               qR = __frcp_rn(1.0f + en);
               qL = en * qR;
@@ -621,7 +648,7 @@ struct SplitCta {
             const int row = oct * 8 + e8;
             float v = 0.0f;
             if (row < rows) {
-              const double* pr = phi + row * phs;
+              const double* pr = phi + (r0 + row) * phs;
               v = (float)(pr[fi] * pr[fj]);
             }
             ph[e8] = to_tf32(v);
@@ -657,7 +684,7 @@ struct SplitCta {
         mma_commit(bar);
       }
       if (!rabort) ++tc_commits;
-      const bool seg_end = ((chunk + 1) % kTcDrain) == 0 || c0 + (int64_t)gsize * a.CH >= it.n;
+      const bool seg_end = ((chunk + 1) % kTcDrain) == 0 || last;
       if (seg_end && !rabort) {
         const bool ok = tc_wait_all();
         if (!__syncthreads_and(ok)) {
@@ -682,7 +709,10 @@ struct SplitCta {
         }
       }
       __syncthreads();
+     }
     }
+    // every MMA of the pass has been drained: the operand region is free for
+    // the row cache of the next passes
     if (gsize > 1) gang_reduce(G, E * C2);
   }
 
@@ -1396,10 +1426,6 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) split_kernel(SplitArgs a)
     fence_mbar_init();
   }
   if (a.tc) {
-    // operand rows that no item writes (entries >= E, columns >= 2 Rg) stay zero
-    uint4* op = (uint4*)(smem + cta.L.tcop);
-    for (int i = threadIdx.x; i < (2 * kTcAOp + 2 * kTcBOp) / 16; i += kSplitThreads) op[i] = make_uint4(0, 0, 0, 0);
-    fence_proxy_async();
     if ((threadIdx.x >> 5) == 0) {
       tmem_alloc(&s_tmem, kTcCols);
       tmem_relinquish();
@@ -1688,7 +1714,8 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
       !(prm->armijo_c > 0.0 && prm->armijo_c < 1.0) || !(prm->alpha0 > 0.0) ||
       !(prm->alpha_min > 0.0) || prm->alpha_max < prm->alpha_min || prm->min_side_points < 1 ||
       !(prm->min_side_fraction >= 0.0 && prm->min_side_fraction < 0.5) || !(prm->anneal_ratio > 0.0) ||
-      prm->group_restarts < 0 || prm->trial_steps < 0 || prm->ctas_per_sm < 0 || prm->ctas_per_sm > 2) {
+      prm->group_restarts < 0 || prm->trial_steps < 0 || prm->ctas_per_sm < 0 || prm->ctas_per_sm > 2 ||
+      prm->tensor_gram < 0 || prm->tensor_gram > 1) {
     set_error("art_split_level: invalid splitter parameters");
     return ART_E_INVALID;
   }
@@ -1711,7 +1738,7 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
   int use_tc = 0;
   {
     const int pa = pr->max_features + 1, E = pa * (pa + 1) / 2;
-    if (prm->precision == ART_PRECISION_MIXED && E <= kTcEntries) {
+    if (prm->precision == ART_PRECISION_MIXED && prm->tensor_gram && E <= kTcEntries) {
       int tc_cols = 2;
       const int rg = choose_rg(R, pa, 0, tc_cols);
       const int H = std::min(std::min(prm->trial_steps > 0 ? prm->trial_steps : 4, std::max(1, kSplitThreads / std::max(rg, 1))),
@@ -1796,7 +1823,8 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
   if (a.tc) {
     // one CTA per SM: chunks of kTcRows rows and the deepest ring that fits
     minb = 1;
-    a.CH = kTcRows;
+    a.CH = 128;
+    while (a.CH > kTcRows && split_layout(a.dmax, a.pmax, a.Rg, a.H, 2, a.CH, 1).total > 227 * 1024) a.CH >>= 1;
     a.S = kMaxStages;
     while (a.S > 2 && split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S, a.CH, 1).total > 227 * 1024) --a.S;
   } else {

@@ -479,8 +479,9 @@ def leg_split(args, stream):
     out = {"metric": "split restart-steps/s", "unit": "restart-steps/s", "nodes": wl.count, "rows": wl.n_rows,
            "restarts": 16, "iterations": 60, "autotune": tuned}
     thetas = {}
-    for prec in ("fp64", "mixed"):
-        sp.precision = prec
+    for prec in ("fp64", "mixed", "mixed_tc"):
+        sp.precision = "mixed" if prec == "mixed_tc" else prec
+        sp.tensor_gram = prec == "mixed_tc"
 
         def step():
             return split_level(sp, wl.x, wl.y, wl.row_offsets, wl.dims, wl.kinds, wl.temperature, wl.ridge,
@@ -500,7 +501,7 @@ def leg_split(args, stream):
                      "achieved_fp64_tflops": flops / (ms / 1000.0) / 1e12, "kernel": top[0],
                      "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()}}
     hbm, bf16, peak_kind = peaks()
-    for prec in ("fp64", "mixed"):
+    for prec in ("fp64", "mixed", "mixed_tc"):
         kern = out[prec]["kernels"].get("split_level")
         if kern:
             kms = kern["ms"] / max(kern["launches"], 1)
@@ -523,6 +524,7 @@ def leg_split(args, stream):
     ok = np.isfinite(la) & np.isfinite(lb)
     out["value"] = out["fp64"]["value"]
     out["mixed_speedup"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    out["mixed_tc_speedup"] = out["fp64"]["ms_per_step"] / out["mixed_tc"]["ms_per_step"]
     out["mixed_vs_fp64_hard_loss_rel_diff_median"] = float(np.median(np.abs(lb[ok] - la[ok]) / np.abs(la[ok])))
     out["mixed_same_partition_fraction"] = float(np.mean(thetas["fp64"][1] == thetas["mixed"][1]))
     return out

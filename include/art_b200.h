@@ -211,7 +211,8 @@ typedef struct ArtSplitParams {
   double weight_floor;          /* soft fits                               */
   int32_t hard_refit;           /* bool: fit hard children + hard loss      */
   int32_t precision;            /* ART_PRECISION_FP64, or _MIXED: sigmoid gates
-                                   in single precision, sums/solves FP64     */
+                                   in single precision, sums/solves FP64
+                                   (see tensor_gram)                         */
   double anneal_ratio;          /* T_k = T * anneal_ratio^(k/(max_iters-1)); 1 = off */
   uint64_t seed;                /* Philox key for device initialisation     */
   int32_t group_restarts;       /* restarts sharing one CTA's row passes
@@ -223,6 +224,12 @@ typedef struct ArtSplitParams {
                                    110 KB of shared memory and 128 registers a
                                    thread (falls back to 1 when the level's
                                    layout does not fit)                      */
+  int32_t tensor_gram;          /* mixed form only: 1 = the soft-pass side Grams
+                                   on the tensor cores (tcgen05 kind::tf32,
+                                   TF32 hi/lo products of vech([phi;y][phi;y]^T)
+                                   and the gate weights, FP32 accumulation over
+                                   128 rows, FP64 across) when the augmented
+                                   model has at most 21 features; 0 = FP64 sums */
 } ArtSplitParams;
 
 typedef struct ArtSplitProblem {
