@@ -125,6 +125,26 @@ class _Target:
         return (self.a * t.exp(-r2 / (2.0 * self.w ** 2))).sum(1) + t.tanh(8.0 * (X @ self.u - self.b))
 
 
+def _target_numpy(job: SurrogateJob):
+    """The job's target as a host function (the same parameters as _Target)."""
+
+    rng = np.random.default_rng([job.seed, 7])
+    d = job.dim
+    c = rng.uniform(-1, 1, (8, d))
+    w = rng.uniform(0.1, 0.6, 8) * np.sqrt(d / 2.0)
+    a = rng.normal(size=8)
+    u = rng.normal(size=d)
+    u = u / np.linalg.norm(u)
+    b = float(rng.uniform(-0.3, 0.3))
+
+    def f(X):
+        X = np.atleast_2d(X)
+        r2 = ((X[:, None, :] - c[None]) ** 2).sum(-1)
+        return (a * np.exp(-r2 / (2.0 * w ** 2))).sum(1) + np.tanh(8.0 * (X @ u - b))
+
+    return f
+
+
 @dataclass
 class _Node:
     path: str
@@ -200,7 +220,11 @@ class ServingEngine:
         self.peak_active = 0
 
     # ------------------------------------------------------------ public
-    def run(self, jobs: list[SurrogateJob], clock=None) -> list[JobResult]:
+    def run(self, jobs: list[SurrogateJob], clock=None, admit_until: float | None = None) -> list[JobResult]:
+        """Serve ``jobs`` against the clock.  With ``admit_until`` (seconds),
+        no job is admitted after that time: the admitted ones finish, and the
+        rest are left unserved (``self.backlog`` counts those that had
+        arrived by the end, ``self.unserved`` all of them)."""
         t = torch()
         dev = require_cuda()
         N.load_library()
@@ -213,15 +237,24 @@ class ServingEngine:
         results: list[JobResult] = []
         start = clock()
         used = 0
+        self.backlog = self.unserved = 0
         while pending or active:
             now = clock() - start
-            while (pending and pending[0].arrival <= now and len(active) < self.max_active
+            if admit_until is not None and now > admit_until and pending:
+                if not active:
+                    break
+                pending_closed = True
+            else:
+                pending_closed = False
+            while (not pending_closed and pending and pending[0].arrival <= now and len(active) < self.max_active
                    and used + job_footprint(pending[0]) <= self.hbm_budget):
                 j = pending.pop(0)
                 active.append(_JobState(j, dev, now))
                 used += job_footprint(j)
             self.peak_active = max(self.peak_active, len(active))
             if not active:
+                if pending_closed:
+                    break
                 time.sleep(max(0.0, min(pending[0].arrival - now, 0.01)))
                 continue
             self.tick(active)
@@ -231,6 +264,9 @@ class ServingEngine:
                 used -= job_footprint(st.job)
                 results.append(self._result(st, now))
         t.cuda.synchronize()
+        end = clock() - start
+        self.unserved = len(pending)
+        self.backlog = sum(1 for j in pending if j.arrival <= end)
         return sorted(results, key=lambda r: r.job_id)
 
     def build_alone(self, job: SurrogateJob) -> JobResult:

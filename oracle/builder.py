@@ -100,6 +100,7 @@ class Builder:
     refinement_rounds: int = 0
     refinement_points: int = 1024
     refinement_leaves: int = 4
+    top_up: bool = True                # False: children keep only their inherited samples
     queries: int = field(default=0, init=False)
 
     def next_seed(self):
@@ -159,7 +160,7 @@ class Builder:
                     or res["fallback"])
 
     def _node(self, A, b, X, y, depth, node_id, parent=True) -> Node:
-        if parent:                                                      # _top_up_child (builder.py:502-551)
+        if parent and self.top_up:                                      # _top_up_child (builder.py:502-551)
             if X.shape[0] > self.sample_count:
                 keep = self.rng.choice(X.shape[0], size=self.sample_count, replace=False)
                 X, y = X[keep], y[keep]
