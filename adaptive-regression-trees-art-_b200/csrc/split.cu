@@ -258,7 +258,7 @@ __global__ void split_plan_scatter(SplitArgs a) {
 }
 
 // ================================================================ kernel
-template <int TC>
+template <int TC, int TCG>
 struct SplitCta {
   static constexpr int TE = 32 / TC;
   const SplitArgs& a;
@@ -565,6 +565,7 @@ struct SplitCta {
   // products hi hi + hi lo + lo hi per K-step, FP32 accumulation in TMEM over
   // kTcDrain chunks (128 rows), FP64 accumulation across drains.
   __device__ void gram_pass_tc() {
+    static_assert(TCG, "the tensor-core pass is compiled into the TCG kernels only");
     const int E = it.E, C2 = 2 * a.Rg, N = C2 <= 16 ? 16 : 32;
     unsigned char* Ahi = sm + L.tcop;
     unsigned char* Alo = Ahi + kTcAOp;
@@ -967,8 +968,8 @@ struct SplitCta {
   __device__ void gang_end();
 };
 
-template <int TC>
-__device__ bool SplitCta<TC>::gang_begin(int item_id, int rank, int members) {
+template <int TC, int TCG>
+__device__ bool SplitCta<TC, TCG>::gang_begin(int item_id, int rank, int members) {
   // rank 0 takes a free scratch slot and publishes it; the other members
   // wait (bounded) for it.  At most one gang is being popped at a time and
   // every other active gang holds >= 2 CTAs, so the slots (one per SM plus
@@ -1032,8 +1033,8 @@ __device__ bool SplitCta<TC>::gang_begin(int item_id, int rank, int members) {
   return gslot >= 0;
 }
 
-template <int TC>
-__device__ void SplitCta<TC>::gang_end() {
+template <int TC, int TCG>
+__device__ void SplitCta<TC, TCG>::gang_end() {
   if (gsize == 1) return;
   __syncthreads();
   if (tid == 0 && gslot >= 0) {
@@ -1046,8 +1047,8 @@ __device__ void SplitCta<TC>::gang_end() {
   gslot = -1;
 }
 
-template <int TC>
-__device__ void SplitCta<TC>::run(int item_id, int rank, int members) {
+template <int TC, int TCG>
+__device__ void SplitCta<TC, TCG>::run(int item_id, int rank, int members) {
   const ArtSplitParams& P = a.prm;
   if (!gang_begin(item_id, rank, members)) {  // no slot: the level is reported lost
     gang_end();
@@ -1112,7 +1113,7 @@ __device__ void SplitCta<TC>::run(int item_id, int rank, int members) {
   }
   // ---------------------------------------------------------- evaluate(theta)
   auto evaluate = [&]() {
-    if (a.tc) {
+    if constexpr (TCG) {
       gram_pass_tc();
       solve_all(true);
     } else {
@@ -1414,18 +1415,18 @@ __device__ void SplitCta<TC>::run(int item_id, int rank, int members) {
 // MINB resident CTAs per SM: 1 keeps every register a thread wants and the
 // deepest row ring; 2 doubles the warps that hide the per-row latency of the
 // passes at the cost of a 128-register cap and half the shared memory
-template <int TC, int MINB>
+template <int TC, int MINB, int TCG = 0>
 __global__ void __launch_bounds__(kSplitThreads, MINB) split_kernel(SplitArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_item;
-  SplitCta<TC> cta(a, smem);
+  SplitCta<TC, TCG> cta(a, smem);
   __shared__ uint32_t s_tmem;
   if (threadIdx.x == 0) {
     for (int i = 0; i < a.S; ++i) mbar_init(&cta.rbar[i], 1);
-    if (a.tc) mbar_init((uint64_t*)(smem + cta.L.tcbar), 1);
+    if constexpr (TCG) mbar_init((uint64_t*)(smem + cta.L.tcbar), 1);
     fence_mbar_init();
   }
-  if (a.tc) {
+  if constexpr (TCG) {
     if ((threadIdx.x >> 5) == 0) {
       tmem_alloc(&s_tmem, kTcCols);
       tmem_relinquish();
@@ -1433,7 +1434,7 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) split_kernel(SplitArgs a)
     tc_fence_before();
   }
   __syncthreads();
-  if (a.tc) {
+  if constexpr (TCG) {
     tc_fence_after();
     cta.tmem = s_tmem;
   }
@@ -1448,7 +1449,7 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) split_kernel(SplitArgs a)
     cta.run(e.x, e.y, e.z);
   }
   cta.ring_drain();
-  if (a.tc) {  // release TMEM after a bounded wait for this CTA's MMAs
+  if constexpr (TCG) {  // release TMEM after a bounded wait for this CTA's MMAs
     cta.tc_wait_all();
     tc_fence_before();
     __syncthreads();
@@ -1731,16 +1732,16 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
   int TC = 2;
   int Rg = choose_rg(R, pr->max_features + 1, prm->group_restarts, TC);
   if (Rg < 1) { set_error("art_split_level: model too large for the split kernel"); return ART_E_UNSUPPORTED; }
-  // Mixed form: the soft-pass Grams go to the tensor cores when the entries
-  // fit two M = 128 tiles and the operands fit shared memory next to the
-  // rest; all restarts of a node (up to 16) then share one CTA and one
-  // operand generation per chunk.
+  // Mixed form with tensor_gram: the soft-pass Grams go to the tensor cores
+  // when the entries fit two M = 128 tiles and the operands fit shared
+  // memory next to the rest (one CTA per SM); the restarts of a work item
+  // share one operand generation per chunk.
   int use_tc = 0;
   {
     const int pa = pr->max_features + 1, E = pa * (pa + 1) / 2;
     if (prm->precision == ART_PRECISION_MIXED && prm->tensor_gram && E <= kTcEntries) {
       int tc_cols = 2;
-      const int rg = choose_rg(R, pa, 0, tc_cols);
+      const int rg = choose_rg(R, pa, prm->group_restarts, tc_cols);
       const int H = std::min(std::min(prm->trial_steps > 0 ? prm->trial_steps : 4, std::max(1, kSplitThreads / std::max(rg, 1))),
                              prm->max_backtracks + 1);
       if (rg >= 1 && split_layout(pr->max_dim, pr->max_features, rg, H, 2, kTcRows, 1).total <= 227 * 1024) {
@@ -1857,7 +1858,11 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
     return check_launch("split_level");
   };
   int rc;
-  if (minb == 2) {
+  if (a.tc) {
+    if (TC == 8) rc = launch(split_kernel<8, 1, 1>);
+    else if (TC == 4) rc = launch(split_kernel<4, 1, 1>);
+    else rc = launch(split_kernel<2, 1, 1>);
+  } else if (minb == 2) {
     if (TC == 8) rc = launch(split_kernel<8, 2>);
     else if (TC == 4) rc = launch(split_kernel<4, 2>);
     else rc = launch(split_kernel<2, 2>);
