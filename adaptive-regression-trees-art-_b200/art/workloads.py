@@ -360,3 +360,26 @@ def bumps_ridge_2d(seed: int = 1):
         return (amps * np.exp(-r2 / (2 * widths ** 2))).sum(1) + np.tanh(8 * (X @ a - b))
 
     return f
+
+
+def random_tree(depth: int = 8, d: int = 4, seed: int = 6):
+    """A full regression tree of the given depth on [-1,1]^d for prediction
+    benchmarks: random unit split normals with thresholds in (-0.2, 0.2),
+    affine leaves with N(0,1) coefficients."""
+
+    from .models import AffineRidgeModel
+    from .tree import LeafNode, RegressionTree, SplitNode
+
+    rng = np.random.default_rng(seed)
+
+    def grow(level, node_id):
+        if level == depth:
+            m = AffineRidgeModel()
+            m.coef_ = rng.normal(size=d + 1)
+            return LeafNode(m, depth=level, node_id=node_id)
+        w = rng.normal(size=d)
+        w /= np.linalg.norm(w)
+        return SplitNode(w, float(rng.uniform(-0.2, 0.2)), grow(level + 1, node_id + "/L"),
+                         grow(level + 1, node_id + "/R"), depth=level, node_id=node_id)
+
+    return RegressionTree(grow(0, "root"))
