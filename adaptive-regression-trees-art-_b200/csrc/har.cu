@@ -158,49 +158,35 @@ __global__ void __launch_bounds__(kHarThreads, har_min_ctas(L, MAXK)) har_kernel
   // step of each thinning block after burn_in
   int keep_step = scalar ? a.burn_in : a.burn_in + a.thinning - 1;
   int keep_idx = 0;
-  // Device draws of a step (direction pair of this lane and the chord
-  // uniform) depend on the step counter only, so each iteration draws the
-  // next step's while the current chord is computed (the two dependency
-  // chains interleave instead of adding up).
-  const bool device_draws = !a.dirs && !a.unif;
-  auto draw = [&](int step, double& u0, double& u1, double& U) {
-    const uint64_t ctr = a.counter_base + (uint64_t)step;
-    Philox4 r = philox4x32_10((uint32_t)ctr, (uint32_t)(ctr >> 32), (uint32_t)lane, 0u, key0, key1);
-    normal_pair_f32(r, u0, u1);
-    if (!h0) u0 = 0.0;
-    if (!h1) u1 = 0.0;
-    if (a.maps) {  // covariance-shaped direction u = M z, z gathered across the team
-      const double* M = a.maps + (int64_t)pj * d * d;
-      double m0 = 0.0, m1 = 0.0;
-      for (int j = 0; j < d; ++j) {
-        const double za = __shfl_sync(0xffffffffu, u0, j >> 1, L);
-        const double zb = __shfl_sync(0xffffffffu, u1, j >> 1, L);
-        const double zj = (j & 1) ? zb : za;
-        if (h0) m0 = fma(M[(int64_t)i0 * d + j], zj, m0);
-        if (h1) m1 = fma(M[(int64_t)i1 * d + j], zj, m1);
-      }
-      u0 = m0;
-      u1 = m1;
-    }
-    Philox4 ru = philox4x32_10((uint32_t)ctr, (uint32_t)(ctr >> 32), 0xFFFFFFFFu, 1u, key0, key1);
-    U = u01_closed_open(ru.v[0], ru.v[1]);
-  };
-  double nu0 = 0.0, nu1 = 0.0, nU = 0.0;
-  if (device_draws && total > 0) draw(0, nu0, nu1, nU);
   // one step per iteration: the body is long, and unrolling it only grows the
   // code the warps fetch
 #pragma unroll 1
   for (int step = 0; step < total; ++step) {
-    double u0, u1, Ud = 0.0;
-    if (device_draws) {
-      u0 = nu0;
-      u1 = nu1;
-      Ud = nU;
-      if (step + 1 < total) draw(step + 1, nu0, nu1, nU);
-    } else {
+    double u0, u1;
+    if (a.dirs) {
       const double* dp = a.dirs + (chain * total + step) * (int64_t)d;
       u0 = h0 ? dp[i0] : 0.0;
       u1 = h1 ? dp[i1] : 0.0;
+    } else {
+      const uint64_t ctr = a.counter_base + (uint64_t)step;
+      Philox4 r = philox4x32_10((uint32_t)ctr, (uint32_t)(ctr >> 32), (uint32_t)lane, 0u, key0,
+                                key1);
+      normal_pair_f32(r, u0, u1);
+      if (!h0) u0 = 0.0;
+      if (!h1) u1 = 0.0;
+      if (a.maps) {  // covariance-shaped direction u = M z, z gathered across the team
+        const double* M = a.maps + (int64_t)pj * d * d;
+        double m0 = 0.0, m1 = 0.0;
+        for (int j = 0; j < d; ++j) {
+          const double za = __shfl_sync(0xffffffffu, u0, j >> 1, L);
+          const double zb = __shfl_sync(0xffffffffu, u1, j >> 1, L);
+          const double zj = (j & 1) ? zb : za;
+          if (h0) m0 = fma(M[(int64_t)i0 * d + j], zj, m0);
+          if (h1) m1 = fma(M[(int64_t)i1 * d + j], zj, m1);
+        }
+        u0 = m0;
+        u1 = m1;
+      }
     }
     bool skip = false;
     if (scalar) {
@@ -248,7 +234,15 @@ __global__ void __launch_bounds__(kHarThreads, har_min_ctas(L, MAXK)) har_kernel
       thi = team_min<L>(thi);
       infeasible = team_or<L>(infeasible);
       if (status == 0 && (tlo > thi || infeasible)) status = 1;
-      const double U = device_draws ? Ud : a.unif[chain * total + (scalar ? ucur : step)];
+      double U;
+      if (a.unif) {
+        U = a.unif[chain * total + (scalar ? ucur : step)];
+      } else {
+        const uint64_t ctr = a.counter_base + (uint64_t)step;
+        Philox4 r = philox4x32_10((uint32_t)ctr, (uint32_t)(ctr >> 32), 0xFFFFFFFFu, 1u, key0,
+                                  key1);
+        U = u01_closed_open(r.v[0], r.v[1]);
+      }
       ++ucur;
       // Separate roundings (no FMA contraction), as numpy/numba evaluate them.
       const double t = __dadd_rn(tlo, __dmul_rn(U, __dsub_rn(thi, tlo)));
