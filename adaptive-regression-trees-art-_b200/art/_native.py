@@ -99,7 +99,7 @@ class ArtSplitParams(C.Structure):
         ("heavy_backtrack_threshold", I32), ("max_line_search_failures", I32),
         ("weight_floor", F64), ("hard_refit", I32), ("precision", I32),
         ("anneal_ratio", F64), ("seed", U64), ("group_restarts", I32), ("trial_steps", I32),
-        ("ctas_per_sm", I32), ("tensor_gram", I32),
+        ("ctas_per_sm", I32), ("tensor_gram", I32), ("restart_warps", I32),
     ]
 
 

@@ -10,12 +10,13 @@ caller's own batch, with CUDA events on the launching stream:
   factorisation; the threshold is the smallest p from which the tensor-core
   kernel wins for every larger class, and the factorisation is the one with
   the lower total time over the tensor classes.
-* ``split_shape`` for a (d, p, R) split level -- the restarts that share one
-  CTA's row passes (``group_restarts``), the Armijo step sizes evaluated
-  per trial pass (``trial_steps``) and the resident CTAs per SM
-  (``ctas_per_sm``: one with the deepest row ring, or two with half the
-  shared memory and a 128-register cap); each candidate runs the sample
-  level and the fastest is kept.
+* ``split_shape`` for a (d, p, R) split level -- either the CTA form, with
+  the restarts that share one CTA's row passes (``group_restarts``), the
+  Armijo step sizes evaluated per trial pass (``trial_steps``) and the
+  resident CTAs per SM (``ctas_per_sm``: one with the deepest row ring, or
+  two with half the shared memory and a 128-register cap), or the
+  warp-per-restart form (``restart_warps``) with its trial steps; each
+  candidate runs the sample level and the fastest is kept.
 
 Results live in an in-process table keyed by the device (name, SM count,
 compute capability), persisted as JSON at ``$ART_AUTOTUNE_CACHE`` when that
@@ -117,17 +118,19 @@ def cached_ridge_threshold(dims=None, features=None, row_offsets=None, fp64_fact
     return cached_ridge_choice()[0]
 
 
-def cached_split_shape(d: int, p: int, R: int) -> tuple[int, int, int]:
-    """Tuned (group_restarts, trial_steps, ctas_per_sm) for a (d, p, R) level, or (0, 0, 0)."""
+def cached_split_shape(d: int, p: int, R: int) -> tuple[int, int, int, int]:
+    """Tuned (group_restarts, trial_steps, ctas_per_sm, restart_warps) for a
+    (d, p, R) level, or (0, 0, 0, 0)."""
 
     _load()
     try:
         entry = _TABLE.get(_split_key(d, p, R))
     except RuntimeError:
-        return 0, 0, 0
+        return 0, 0, 0, 0
     if not entry:
-        return 0, 0, 0
-    return int(entry["group_restarts"]), int(entry["trial_steps"]), int(entry.get("ctas_per_sm", 0))
+        return 0, 0, 0, 0
+    return (int(entry["group_restarts"]), int(entry["trial_steps"]), int(entry.get("ctas_per_sm", 0)),
+            int(entry.get("restart_warps", 0)))
 
 
 def _event_time(fn, repeats: int, stream) -> float:
@@ -230,11 +233,20 @@ def tune_ridge_threshold(x, y, w, row_offsets, dims, kinds, ridge, *, x_offsets=
     return entry
 
 
-def split_candidates(R: int, max_backtracks: int) -> list[tuple[int, int, int]]:
-    """(group_restarts, trial_steps, ctas_per_sm) shapes tried for R restarts.
+WARP_MAX_DIM = 23       # warp-per-restart form: inputs, features and trial steps it takes
+WARP_MAX_FEATURES = 23
+WARP_MAX_TRIALS = 8
+
+
+def split_candidates(R: int, max_backtracks: int, d: int = 0, p: int = 0,
+                     tensor_gram: bool = False) -> list[tuple[int, int, int, int]]:
+    """(group_restarts, trial_steps, ctas_per_sm, restart_warps) shapes tried
+    for R restarts.
 
     Two CTAs per SM are tried for groups of at most 8 restarts: a group of 16
-    keeps 16 restarts' state per thread, which the 128-register cap spills."""
+    keeps 16 restarts' state per thread, which the 128-register cap spills.
+    The warp-per-restart form is tried when the level fits it (d and p at
+    most 23, no tensor-core Gram)."""
 
     groups = sorted({g for g in (R, 16, 8, 4, 2, 1) if 1 <= g <= min(R, 16)}, reverse=True)
     out = []
@@ -242,7 +254,11 @@ def split_candidates(R: int, max_backtracks: int) -> list[tuple[int, int, int]]:
         hmax = min(32, max(1, 256 // g), max_backtracks + 1)
         for h in sorted({min(hmax, v) for v in (2, 4, 8, 16)}, reverse=True):
             for c in ((1, 2) if g <= 8 else (1,)):
-                out.append((g, h, c))
+                out.append((g, h, c, 0))
+    if not tensor_gram and 1 <= d <= WARP_MAX_DIM and 1 <= p <= WARP_MAX_FEATURES:
+        hmax = min(WARP_MAX_TRIALS, max_backtracks + 1)
+        for h in sorted({min(hmax, v) for v in (1, 2, 4)}, reverse=True):
+            out.append((0, h, 0, 1))
     return out
 
 
@@ -256,17 +272,19 @@ def tune_split_shape(splitter, x, y, row_offsets, dims, features, temperature, r
     t = torch()
     stream = t.cuda.current_stream() if stream is None else stream
     R = int(max(1, splitter.n_restarts))
+    tc = bool(getattr(splitter, "tensor_gram", False)) and getattr(splitter, "precision", "fp64") == "mixed"
     timings = {}
-    for g, h, c in split_candidates(R, int(splitter.max_backtracks)):
-        def run(g=g, h=h, c=c):
+    for g, h, c, w in split_candidates(R, int(splitter.max_backtracks), int(max_dim), int(max_features), tc):
+        def run(g=g, h=h, c=c, w=w):
             return split_level(splitter, x, y, row_offsets, dims, features, temperature, ridge, theta0=theta0,
                                anneal_ratio=anneal_ratio, hard_refit=hard_refit, max_dim=max_dim,
                                max_features=max_features, group_restarts=g, trial_steps=h, ctas_per_sm=c,
-                               stream=stream)
+                               restart_warps=w, stream=stream)
 
-        timings[f"{g}x{h}x{c}"] = _event_time(run, repeats, stream)
+        timings[f"{g}x{h}x{c}x{w}"] = _event_time(run, repeats, stream)
     best = min(timings, key=timings.get)
-    g, h, c = (int(v) for v in best.split("x"))
-    entry = {"group_restarts": g, "trial_steps": h, "ctas_per_sm": c, "candidates_ms": timings}
+    g, h, c, w = (int(v) for v in best.split("x"))
+    entry = {"group_restarts": g, "trial_steps": h, "ctas_per_sm": c, "restart_warps": w,
+             "candidates_ms": timings}
     _store(_split_key(max_dim, max_features, R), entry)
     return entry

@@ -162,7 +162,7 @@ class LevelResult:
 
 
 def split_params(s: "SoftObliqueSplitter", hard_refit: bool, anneal_ratio: float = 1.0, seed: int = 0,
-                 group_restarts: int = 0, trial_steps: int = 0, ctas_per_sm: int = 0):
+                 group_restarts: int = 0, trial_steps: int = 0, ctas_per_sm: int = 0, restart_warps: int = 0):
     """ArtSplitParams of a splitter.  ``precision="mixed"`` evaluates the
     sigmoid gates in single precision (objective within 1e-5 relative of the
     FP64 form); solves and the side decisions stay FP64, and the soft-pass
@@ -179,7 +179,8 @@ def split_params(s: "SoftObliqueSplitter", hard_refit: bool, anneal_ratio: float
         int(s.max_line_search_failures), float(s.weight_floor), int(bool(hard_refit)),
         N.PRECISION_MIXED if getattr(s, "precision", "fp64") == "mixed" else N.PRECISION_FP64,
         float(anneal_ratio), int(seed) & ((1 << 64) - 1), int(group_restarts), int(trial_steps),
-        int(ctas_per_sm), int(bool(getattr(s, "tensor_gram", False)) and getattr(s, "precision", "fp64") == "mixed"))
+        int(ctas_per_sm), int(bool(getattr(s, "tensor_gram", False)) and getattr(s, "precision", "fp64") == "mixed"),
+        int(bool(restart_warps)))
 
 
 def split_level(splitter: "SoftObliqueSplitter", x, y, row_offsets, dims, features, temperature, ridge,
@@ -187,18 +188,18 @@ def split_level(splitter: "SoftObliqueSplitter", x, y, row_offsets, dims, featur
                 hard_refit: bool = True, anneal_ratio: float = 1.0, seed: int = 0, traces: bool = False,
                 max_dim: int | None = None, max_features: int | None = None, node_keys=None,
                 group_restarts: int | None = None, trial_steps: int | None = None,
-                ctas_per_sm: int | None = None, min_side_points=None, out: LevelResult | None = None, workspace=None,
-                stream=None) -> LevelResult:
+                ctas_per_sm: int | None = None, restart_warps: int | None = None, min_side_points=None,
+                out: LevelResult | None = None, workspace=None, stream=None) -> LevelResult:
     """Split K nodes in one launch sequence; arrays are numpy or torch (moved to the device).
 
     theta0, when given, is (K, R, d_max + 1); otherwise restarts start from
     device draws keyed by ``seed`` and the node's position k (unit Gaussian w,
     z = median(X w)), or by ``node_keys[k]`` (uint64 per node) when given, so
     that a node's draws do not depend on the batch it is solved in.
-    ``group_restarts`` / ``trial_steps`` / ``ctas_per_sm`` fix the kernel's
-    launch shape (restarts per CTA, Armijo steps per trial pass, resident
-    CTAs per SM); None takes the autotuned choice for (d, p, R) on this
-    device, else the library's.
+    ``group_restarts`` / ``trial_steps`` / ``ctas_per_sm`` / ``restart_warps``
+    fix the kernel's launch shape (restarts per CTA, Armijo steps per trial
+    pass, resident CTAs per SM, or one warp per restart); None takes the
+    autotuned choice for (d, p, R) on this device, else the library's.
     ``min_side_points`` (K ints) overrides the splitter's minimum side count
     per node, so nodes with different limits share one launch.
     ``out`` (a LevelResult of K rows) and ``workspace`` (a uint8 device
@@ -252,14 +253,16 @@ def split_level(splitter: "SoftObliqueSplitter", x, y, row_offsets, dims, featur
                        else min_side_points, t.int32, dev)
     prob = N.ArtSplitProblem(seg, ptr(x), ptr(y), ptr(temp), ptr(rid), ptr(pl), ptr(fb), ptr(th0), stride,
                              int(max_dim), int(max_features), ptr(nk), ptr(ms))
-    if group_restarts is None or trial_steps is None or ctas_per_sm is None:
+    if group_restarts is None or trial_steps is None or ctas_per_sm is None or restart_warps is None:
         from . import autotune
 
-        g_auto, h_auto, c_auto = autotune.cached_split_shape(int(max_dim), int(max_features), R)
+        g_auto, h_auto, c_auto, w_auto = autotune.cached_split_shape(int(max_dim), int(max_features), R)
         group_restarts = g_auto if group_restarts is None else group_restarts
         trial_steps = h_auto if trial_steps is None else trial_steps
         ctas_per_sm = c_auto if ctas_per_sm is None else ctas_per_sm
-    prm = split_params(splitter, hard_refit, anneal_ratio, seed, group_restarts, trial_steps, ctas_per_sm)
+        restart_warps = w_auto if restart_warps is None else restart_warps
+    prm = split_params(splitter, hard_refit, anneal_ratio, seed, group_restarts, trial_steps, ctas_per_sm,
+                       restart_warps)
     res = N.ArtSplitResult(ptr(out.theta), int(out.theta.shape[1]), ptr(out.beta), int(out.beta.shape[2]),
                            ptr(out.loss), ptr(out.child_loss), ptr(out.ridge_effective), ptr(out.n_right),
                            ptr(out.n_iters), ptr(out.stop_reason), ptr(out.failure), ptr(out.flags),

@@ -221,6 +221,50 @@ __device__ __forceinline__ void entry_ij(int e, int& i, int& j) {
   j = e - i * (i + 1) / 2;
 }
 
+// Trace-scaled ridge + left-looking Cholesky + solve of one augmented
+// system by a warp: A is the packed lower triangle of [G h; h^T y'Wy]
+// (p + 1 rows) in shared memory, overwritten by the factor; the solution
+// goes to z[0..p).  lambda = ridge * trace(G) / p (models.py:271).  Returns
+// 0, or the 1-based failing pivot.
+__device__ __noinline__ int warp_ridge_solve(double* A, double* z, int p, double ridge, double& lam_out) {
+  const int lane = threadIdx.x & 31;
+  double tr = 0.0;
+  if (lane == 0)
+    for (int i = 0; i < p; ++i) tr += A[pk(i, i)];
+  tr = __shfl_sync(0xffffffffu, tr, 0);
+  const double lam = ridge * tr / p;
+  lam_out = lam;
+  for (int i = lane; i < p; i += 32) A[pk(i, i)] += lam;
+  __syncwarp();
+  int fail = 0;
+  for (int j = 0; j < p && !fail; ++j) {
+    double s = 0.0;
+    for (int k2 = lane; k2 < j; k2 += 32) s += A[pk(j, k2)] * A[pk(j, k2)];
+    s = warp_sum(s);
+    const double djj = A[pk(j, j)] - s;
+    if (!(djj > 0.0) || !isfinite(djj)) { fail = j + 1; break; }
+    const double ljj = sqrt(djj);
+    __syncwarp();
+    if (lane == 0) A[pk(j, j)] = ljj;
+    for (int i = j + 1 + lane; i < p; i += 32) {
+      double t2 = A[pk(i, j)];
+      for (int k2 = 0; k2 < j; ++k2) t2 -= A[pk(i, k2)] * A[pk(j, k2)];
+      A[pk(i, j)] = t2 / ljj;
+    }
+    __syncwarp();
+  }
+  if (fail) {
+    __syncwarp();
+    return fail;
+  }
+  for (int i = lane; i < p; i += 32) z[i] = A[pk(p, i)];  // h
+  __syncwarp();
+  warp_forward<double, double>(A, z, p);
+  warp_backward<double, double>(A, z, p);
+  __syncwarp();
+  return 0;
+}
+
 // =========================================================== plan (LPT order)
 __device__ __forceinline__ int gang_size(const SplitArgs& a, int64_t n) {
   if (!a.gang_on) return 1;
@@ -730,40 +774,13 @@ struct SplitCta {
       if (S(r, RS_ACTIVE) == 0.0) continue;
       for (int e = lane; e < E; e += 32) A[e] = colmajor ? G[(size_t)c * E + e] : G[(size_t)e * C2 + c];
       __syncwarp();
-      double tr = 0.0;
-      if (lane == 0)
-        for (int i = 0; i < p; ++i) tr += A[pk(i, i)];
-      tr = __shfl_sync(0xffffffffu, tr, 0);
-      const double lam = it.ridge * tr / p;  // models.py:271
-      for (int i = lane; i < p; i += 32) A[pk(i, i)] += lam;
-      __syncwarp();
-      // left-looking Cholesky, lanes over rows
-      int fail = 0;
-      for (int j = 0; j < p && !fail; ++j) {
-        double s = 0.0;
-        for (int k2 = lane; k2 < j; k2 += 32) s += A[pk(j, k2)] * A[pk(j, k2)];
-        s = warp_sum(s);
-        const double djj = A[pk(j, j)] - s;
-        if (!(djj > 0.0) || !isfinite(djj)) { fail = j + 1; break; }
-        const double ljj = sqrt(djj);
-        __syncwarp();
-        if (lane == 0) A[pk(j, j)] = ljj;
-        for (int i = j + 1 + lane; i < p; i += 32) {
-          double t2 = A[pk(i, j)];
-          for (int k2 = 0; k2 < j; ++k2) t2 -= A[pk(i, k2)] * A[pk(j, k2)];
-          A[pk(i, j)] = t2 / ljj;
-        }
-        __syncwarp();
-      }
+      double lam;
+      const int fail = warp_ridge_solve(A, z, p, it.ridge, lam);
       if (fail) {
         if (lane == 0) S(r, RS_CHOLBAD) = 1.0;
         __syncwarp();
         continue;
       }
-      for (int i = lane; i < p; i += 32) z[i] = A[pk(p, i)];  // h
-      __syncwarp();
-      warp_forward<double, double>(A, z, p);
-      warp_backward<double, double>(A, z, p);
       double* beta = (side ? br : bl) + r * a.pmax;
       for (int i = lane; i < p; i += 32) beta[i] = z[i];
       if (lane == 0) S(r, side ? RS_LAMR : RS_LAML) = lam;
@@ -1412,6 +1429,667 @@ __device__ void SplitCta<TC, TCG>::run(int item_id, int rank, int members) {
   gang_end();
 }
 
+// ============================================ warp-per-restart split kernel
+// One warp per (node, restart) work item, no block barriers: each warp
+// streams its node's rows in tiles of 32, keeps its restart's state in
+// registers (uniform across the warp) and a few shared-memory vectors, and
+// runs its own projected-gradient loop.  The row products run on the FP64
+// tensor path (mma.sync m8n8k4 f64, IEEE FP64 products and sums):
+//   * scores and fitted values: [u, f_L, f_R] = psi [w; beta_L; beta_R]
+//     (x sits in a contiguous block of psi's columns for every feature kind);
+//   * side Grams: G_side += (q_side psi)^T psi, lower-triangular 8 x 8 blocks;
+//   * gradient: g = psi^T c over the x columns.
+// Gates, losses and Armijo tests are per-row lane work added across the warp.
+// The trial step and the next Gram share one pass: the candidate theta_c =
+// project(theta + alpha d) is scored as x . w_c - z_c (the frozen-model
+// evaluation of objectives.py:131-160), its frozen loss taken at the current
+// temperature, and the side Grams at theta_c (at the temperature that
+// follows an accepted step) accumulated on the way, so an accepted step
+// needs no separate Gram pass.  Same objective, stop rules, Armijo steps,
+// AdaptiveAlpha, feasibility tracking, hard partition and refits as the CTA
+// kernel above; the summation order differs.
+
+// D = A B + D for one 8 x 8 x 4 FP64 tile (warp-wide): lane l holds
+// A[l / 4][l % 4], B[l % 4][l / 4] and D[l / 4][2 (l % 4) + {0, 1}].
+__device__ __forceinline__ void dmma_884(double (&c)[2], double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+      : "+d"(c[0]), "+d"(c[1])
+      : "d"(a), "d"(b));
+}
+
+constexpr int kWTile = 32;                                   // rows per tile
+constexpr int kWMaxPa = 24;                                  // p + 1 (augmented with y)
+constexpr int kWMaxD = 23;                                   // inputs
+constexpr int kWMaxK = 6;                                    // 4-feature steps of the score MMAs
+constexpr int kWThreads = 256;
+constexpr int kWWarps = kWThreads / 32;
+
+struct WLayout {
+  size_t xt, psi, cf, sc, tc, A, th, dn, gr, lf, bl, br, fidx, per_warp, total;
+  int xs, ps;
+};
+__host__ __device__ inline WLayout warp_layout(int dmax, int pmax) {
+  WLayout L;
+  const int pa = pmax + 1, E = pa * (pa + 1) / 2, dt = dmax + 1;
+  L.xs = dmax | 1;
+  L.ps = (8 * ((pa + 7) / 8)) | 1;                  // whole 8-column blocks for the MMAs
+  size_t o = 0;
+  L.xt = o; o += (size_t)kWTile * L.xs;             // doubles from here on
+  L.psi = o; o += (size_t)kWTile * L.ps;
+  L.cf = o; o += 2 * kWTile;                        // per-row Gram weights / gradient coefficients
+  L.sc = o; o += 3 * kWTile;                        // per-row u, f_L, f_R
+  L.tc = o; o += dt;                                // trial candidate theta
+  L.A = o; o += (size_t)E + 2 * pa;
+  L.th = o; o += dt;
+  L.dn = o; o += dt;
+  L.gr = o; o += dt;
+  L.lf = o; o += dt;
+  L.bl = o; o += pmax;
+  L.br = o; o += pmax;
+  L.fidx = o; o += pa;                              // two int16 per feature, in a double
+  L.per_warp = o;                                   // doubles per warp
+  L.total = (size_t)kWWarps * o * 8;
+  return L;
+}
+
+__device__ __forceinline__ double wbcast_sum(double v) {
+  // butterfly sum, then lane 0's value: every lane holds the same bits
+  return __shfl_sync(0xffffffffu, warp_sum(v), 0);
+}
+
+// first psi column holding x_1 for each feature kind (x is contiguous there)
+__device__ __forceinline__ int x_column(int kind) {
+  return (kind == ART_FEATURES_POLY1 || kind == ART_FEATURES_POLY2) ? 1 : 0;
+}
+
+struct SplitWarp {
+  const SplitArgs& a;
+  int xs, ps;  // padded row strides of xt and psi (odd, in doubles)
+  // the x tile: its own buffer, or for affine features the first d columns
+  // of psi = [x, 1, y] (no second copy)
+  double *xt, *xt0;
+  int xs0;
+  bool aff = false;
+  double *psi, *cf, *sc, *tc, *A, *th, *dn, *gr, *lf, *bl, *br;
+  int16_t* fidx;
+  int lane, kq, mq;  // lane, and its (k, m) coordinates in the MMA fragments
+  // item
+  int64_t k, r0, n, xoff, kr;
+  int d, kind, p, pa, E, xcol, nb, nk;
+  double ridge, T0;
+  // restart state (uniform)
+  double loss = 0, dd = 0, tol = 0, gnorm = 0, T = 0, invT = 0, alpha = 0, lamL = 0, lamR = 0;
+  double hlossL = 0, hlossR = 0;
+  int nright = 0, iters = 0, stop = 0, fail = 0, feasit = -1;
+  bool active = false, hasfeas = false, conv = false, fbk = false;
+
+  __device__ SplitWarp(const SplitArgs& a_, unsigned char* sm, int warp) : a(a_) {
+    const WLayout L = warp_layout(a.dmax, a.pmax);
+    xs = xs0 = L.xs;
+    ps = L.ps;
+    double* base = (double*)sm + (size_t)warp * L.per_warp;
+    xt = xt0 = base + L.xt; psi = base + L.psi; cf = base + L.cf; sc = base + L.sc; tc = base + L.tc;
+    A = base + L.A; th = base + L.th; dn = base + L.dn; gr = base + L.gr; lf = base + L.lf;
+    bl = base + L.bl; br = base + L.br;
+    fidx = (int16_t*)(base + L.fidx);
+    lane = threadIdx.x & 31;
+    kq = lane & 3;
+    mq = lane >> 2;
+  }
+
+  // Tile rows [t0, t0 + rows): x (coalesced copy) and psi = [phi(x); y],
+  // rows past the end zero.  Returns the row count; ends with __syncwarp.
+  __device__ int load_tile(int64_t t0, double& yv) {
+    const int rows = (int)min((int64_t)kWTile, n - t0);
+    const double* src = a.x + xoff + t0 * d;
+    const int tot = rows * d;
+    const uint32_t inv = 65536u / (uint32_t)d + 1u;  // e / d by a multiply (e < 32 * 23)
+    __syncwarp();
+    for (int e = lane; e < tot; e += 32) {
+      const int rr = (int)(((uint32_t)e * inv) >> 16), i = e - rr * d;
+      xt[rr * xs + i] = __ldg(src + e);
+    }
+    yv = lane < rows ? __ldg(a.y + r0 + t0 + lane) : 0.0;
+    __syncwarp();
+    double* pr = psi + lane * ps;
+    const double* xr = xt + lane * xs;
+    if (aff && lane < rows) {
+      pr[d] = 1.0;
+      pr[p] = yv;
+    } else if (lane < rows) {
+      for (int f = 0; f < p; ++f) {
+        const int ia = fidx[2 * f], ib = fidx[2 * f + 1];
+        pr[f] = (ia < 0 ? 1.0 : xr[ia]) * (ib < 0 ? 1.0 : xr[ib]);
+      }
+      pr[p] = yv;
+    } else {
+      for (int f = 0; f <= p; ++f) pr[f] = 0.0;
+    }
+    __syncwarp();
+    return rows;
+  }
+
+  // B fragments of [w; beta_L; beta_R] (columns 0, 1, 2; rows = psi columns)
+  // for the score MMAs: lane (k, m) holds B[4 s + k][m] of step s.
+  __device__ void score_operand(const double* w, double (&b)[kWMaxK]) const {
+#pragma unroll
+    for (int s = 0; s < kWMaxK; ++s) {
+      const int f = 4 * s + kq;
+      double v = 0.0;
+      if (mq == 0) v = (f >= xcol && f < xcol + d) ? w[f - xcol] : 0.0;
+      else if (mq == 1) v = f < p ? bl[f] : 0.0;
+      else if (mq == 2) v = f < p ? br[f] : 0.0;
+      b[s] = s < nk ? v : 0.0;
+    }
+  }
+
+  // u, f_L, f_R of this lane's row: psi [w; beta_L; beta_R] by MMAs over
+  // 8-row blocks, staged through shared memory.  Call after load_tile.
+  __device__ void scores(int rows, const double (&b)[kWMaxK], double& u, double& fl, double& fr) {
+#pragma unroll
+    for (int rb = 0; rb < 4; ++rb) {
+      if (8 * rb < rows) {  // warp-uniform
+        double c[2] = {0.0, 0.0};
+        const double* pr = psi + (8 * rb + mq) * ps + kq;
+#pragma unroll
+        for (int s = 0; s < kWMaxK; ++s)
+          if (s < nk) dmma_884(c, pr[4 * s], b[s]);
+        if (kq == 0) { sc[8 * rb + mq] = c[0]; sc[kWTile + 8 * rb + mq] = c[1]; }
+        else if (kq == 1) sc[2 * kWTile + 8 * rb + mq] = c[0];
+      }
+    }
+    __syncwarp();
+    u = sc[lane];
+    fl = sc[kWTile + lane];
+    fr = sc[2 * kWTile + lane];
+    __syncwarp();
+  }
+
+  // G_side += (q_side psi)^T psi over the tile (lower 8 x 8 blocks), the
+  // weights staged in cf.  Rows past the tile's end are zero rows.
+  __device__ void gram_tile(int rows, double qL, double qR, double (&cL)[6][2], double (&cR)[6][2]) {
+    cf[lane] = qL;
+    cf[kWTile + lane] = qR;
+    __syncwarp();
+    for (int k0 = 0; k0 < rows; k0 += 4) {
+      const int row = k0 + kq;
+      const double* pr = psi + row * ps + mq;
+      const double ql = cf[row], qr = cf[kWTile + row];
+      double v[3];
+#pragma unroll
+      for (int I = 0; I < 3; ++I) v[I] = I < nb ? pr[8 * I] : 0.0;
+#pragma unroll
+      for (int I = 0; I < 3; ++I) {
+        if (I < nb) {  // warp-uniform
+          const double aL = ql * v[I], aR = qr * v[I];
+#pragma unroll
+          for (int J = 0; J <= I; ++J) {
+            dmma_884(cL[I * (I + 1) / 2 + J], aL, v[J]);
+            dmma_884(cR[I * (I + 1) / 2 + J], aR, v[J]);
+          }
+        }
+      }
+    }
+    __syncwarp();
+  }
+
+  // g += psi^T c over the tile (column 0 of the MMA output; c staged in cf).
+  __device__ void grad_tile(int rows, double c, double (&g)[3][2]) {
+    cf[lane] = c;
+    __syncwarp();
+    for (int k0 = 0; k0 < rows; k0 += 4) {
+      const int row = k0 + kq;
+      const double* pr = psi + row * ps + mq;
+      const double b = mq == 0 ? cf[row] : 0.0;
+#pragma unroll
+      for (int I = 0; I < 3; ++I)
+        if (I < nb) dmma_884(g[I], pr[8 * I], b);
+    }
+    __syncwarp();
+  }
+
+  __device__ double gate(double s) const { return a.mixed ? sigm32(s) : sigm(s); }
+
+  __device__ void run(int item);
+  __device__ bool solve_sides(const double (&cL)[6][2], const double (&cR)[6][2]);
+  __device__ void gram_pass(const double* w, bool hard, int req, bool accumulate, double (&cL)[6][2],
+                            double (&cR)[6][2]);
+  __device__ void resid_pass();
+  __device__ double trial_gram_pass(double invT_next, double (&cL)[6][2], double (&cR)[6][2]);
+  __device__ void hard_losses();
+};
+
+// Both sides' ridge solves from the accumulated Gram blocks; false (restart
+// failed) when either factorisation fails.
+__device__ bool SplitWarp::solve_sides(const double (&cL)[6][2], const double (&cR)[6][2]) {
+  double* z_ = A + E;
+  bool ok = true;
+  for (int side = 0; side < 2; ++side) {
+    __syncwarp();
+#pragma unroll
+    for (int I = 0; I < 3; ++I)
+#pragma unroll
+      for (int J = 0; J <= I; ++J)
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+          const int i = 8 * I + mq, j = 8 * J + 2 * kq + t;
+          if (I < nb && i < pa && j <= i)
+            A[i * (i + 1) / 2 + j] = side ? cR[I * (I + 1) / 2 + J][t] : cL[I * (I + 1) / 2 + J][t];
+        }
+    __syncwarp();
+    double lam;
+    if (warp_ridge_solve(A, z_, p, ridge, lam)) {
+      ok = false;
+      continue;
+    }
+    double* beta = side ? br : bl;
+    for (int i = lane; i < p; i += 32) beta[i] = z_[i];
+    if (side) lamR = lam; else lamL = lam;
+  }
+  __syncwarp();
+  return ok;
+}
+
+// Side Grams at theta = (w, w[d]) over all rows.  Soft: gates with the
+// weight floor; hard: exact sides (weights 1 / 0) and the right-side count,
+// the Gram skipped when a side is below req or `accumulate` is off.
+__device__ void SplitWarp::gram_pass(const double* w, bool hard, int req, bool accumulate, double (&cL)[6][2],
+                                     double (&cR)[6][2]) {
+  const double z = w[d];
+  double b[kWMaxK];
+  score_operand(w, b);
+#pragma unroll
+  for (int q = 0; q < 6; ++q) cL[q][0] = cL[q][1] = cR[q][0] = cR[q][1] = 0.0;
+  int cnt = 0;
+  if (hard) {  // count first: the Grams are needed only when both sides are large enough
+    for (int64_t t0 = 0; t0 < n; t0 += kWTile) {
+      double yv;
+      const int rows = load_tile(t0, yv);
+      if (lane < rows) cnt += right_side(psi + lane * ps + xcol, w, d, z) ? 1 : 0;
+    }
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    nright = cnt;
+    if (nright < req || (int)n - nright < req || !accumulate) return;
+  }
+  for (int64_t t0 = 0; t0 < n; t0 += kWTile) {
+    double yv;
+    const int rows = load_tile(t0, yv);
+    double qL = 0.0, qR = 0.0;
+    if (hard) {
+      if (lane < rows) {
+        const bool right = right_side(psi + lane * ps + xcol, w, d, z);
+        qL = right ? 0.0 : 1.0;
+        qR = right ? 1.0 : 0.0;
+      }
+    } else {
+      double u, fl, fr;
+      scores(rows, b, u, fl, fr);
+      if (lane < rows) {
+        const double pi = gate((u - z) * invT);
+        qL = fmax(1.0 - pi, a.prm.weight_floor);
+        qR = fmax(pi, a.prm.weight_floor);
+      }
+    }
+    gram_tile(rows, qL, qR, cL, cR);
+  }
+}
+
+// Soft residual pass at theta with the current child models: loss,
+// gradient, n_right (pi >= 0.5), then the projected gradient, its norm and
+// the directional derivative.
+__device__ void SplitWarp::resid_pass() {
+  const double z = th[d];
+  const double inv_n = 1.0 / (double)n;
+  double b[kWMaxK];
+  score_operand(th, b);
+  double g[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+  double sl = 0.0, sa = 0.0, snr = 0.0;
+  for (int64_t t0 = 0; t0 < n; t0 += kWTile) {
+    double yv;
+    const int rows = load_tile(t0, yv);
+    double u, fl, fr;
+    scores(rows, b, u, fl, fr);
+    double c = 0.0;
+    if (lane < rows) {
+      const double pi = gate((u - z) * invT);
+      const double eL = yv - fl, eR = yv - fr;
+      const double eL2 = eL * eL, eR2 = eR * eR;
+      c = (eR2 - eL2) * pi * (1.0 - pi) * inv_n;
+      sl += (1.0 - pi) * eL2 + pi * eR2;
+      sa += c;
+      snr += pi >= 0.5 ? 1.0 : 0.0;
+    }
+    grad_tile(rows, c, g);
+  }
+  // psi column 8 I + m of the gradient sits in lane (k = 0, m), block I
+  __syncwarp();
+  if (kq == 0) {
+#pragma unroll
+    for (int I = 0; I < 3; ++I) {
+      const int col = 8 * I + mq - xcol;
+      if (I < nb && col >= 0 && col < d) gr[col] = g[I][0] / T;
+    }
+  }
+  const double tot_l = wbcast_sum(sl), tot_a = wbcast_sum(sa), tot_nr = wbcast_sum(snr);
+  if (lane == 0) gr[d] = -tot_a / T;
+  __syncwarp();
+  loss = tot_l / (double)n;
+  nright = (int)tot_nr;
+  // projected gradient and its norm (splitters.py:86-98), evaluated by every
+  // lane in the same order
+  const double* w = th;
+  double gw = 0.0, nrm2 = 0.0;
+  for (int i = 0; i < d; ++i) gw += gr[i] * w[i];
+  for (int i = 0; i < d; ++i) {
+    const double pg = gr[i] - gw * w[i];
+    nrm2 += pg * pg;
+  }
+  nrm2 += gr[d] * gr[d];
+  __syncwarp();
+  if (lane == 0) {
+    for (int i = 0; i < d; ++i) dn[i] = -(gr[i] - gw * w[i]);
+    dn[d] = -gr[d];
+  }
+  __syncwarp();
+  gnorm = sqrt(nrm2);
+  double s = 0.0;
+  for (int i = 0; i <= d; ++i) s += gr[i] * dn[i];
+  dd = s;
+}
+
+// One Armijo candidate theta_c (in tc): its frozen-model loss at the current
+// temperature (objectives.py:145-156), and the side Grams at theta_c with the
+// gates at invT_next, the temperature that follows an accepted step.
+__device__ double SplitWarp::trial_gram_pass(double invT_next, double (&cL)[6][2], double (&cR)[6][2]) {
+  const double z = tc[d];
+  double b[kWMaxK];
+  score_operand(tc, b);
+#pragma unroll
+  for (int q = 0; q < 6; ++q) cL[q][0] = cL[q][1] = cR[q][0] = cR[q][1] = 0.0;
+  const bool same_t = invT_next == invT;
+  double sl = 0.0;
+  for (int64_t t0 = 0; t0 < n; t0 += kWTile) {
+    double yv;
+    const int rows = load_tile(t0, yv);
+    double u, fl, fr;
+    scores(rows, b, u, fl, fr);
+    double qL = 0.0, qR = 0.0;
+    if (lane < rows) {
+      const double pi = gate((u - z) * invT);
+      const double eL = yv - fl, eR = yv - fr;
+      sl += (1.0 - pi) * (eL * eL) + pi * (eR * eR);
+      const double pn = same_t ? pi : gate((u - z) * invT_next);
+      qL = fmax(1.0 - pn, a.prm.weight_floor);
+      qR = fmax(pn, a.prm.weight_floor);
+    }
+    gram_tile(rows, qL, qR, cL, cR);
+  }
+  return wbcast_sum(sl) / (double)n;
+}
+
+// Hard losses: mean squared residual of each side's hard model.
+__device__ void SplitWarp::hard_losses() {
+  const double z = th[d];
+  double b[kWMaxK];
+  score_operand(th, b);
+  double sL = 0.0, sR = 0.0;
+  for (int64_t t0 = 0; t0 < n; t0 += kWTile) {
+    double yv;
+    const int rows = load_tile(t0, yv);
+    double u, fl, fr;
+    scores(rows, b, u, fl, fr);
+    if (lane < rows) {
+      const bool right = right_side(psi + lane * ps + xcol, th, d, z);
+      const double e = yv - (right ? fr : fl);
+      (right ? sR : sL) += e * e;
+    }
+  }
+  const double tl = wbcast_sum(sL), trr = wbcast_sum(sR);
+  const int nl = (int)n - nright;
+  hlossL = tl / nl;
+  hlossR = trr / nright;
+  loss = (double)nl / n * hlossL + (double)nright / n * hlossR;
+}
+
+__device__ void SplitWarp::run(int item) {
+  const ArtSplitParams& P = a.prm;
+  k = item / a.R;
+  kr = (int64_t)item;  // items are k * R + restart
+  r0 = a.row_offsets[k];
+  n = a.row_offsets[k + 1] - r0;
+  xoff = a.x_offsets[k];
+  d = a.dims[k];
+  kind = a.features[k];
+  p = feature_count(d, kind);
+  pa = p + 1;
+  E = pa * (pa + 1) / 2;
+  xcol = x_column(kind);
+  nb = (pa + 7) >> 3;
+  nk = (p + 3) >> 2;
+  T0 = a.temperature[k];
+  ridge = a.ridge[k];
+  const int req = max(a.min_side ? max(1, a.min_side[k]) : P.min_side_points,
+                      (int)ceil(P.min_side_fraction * (double)n));
+  const bool fb_allowed = a.fallback ? a.fallback[k] != 0 : false;
+  const int M = P.max_iters;
+  aff = kind == ART_FEATURES_AFFINE;
+  xt = aff ? psi : xt0;
+  xs = aff ? ps : xs0;
+  __syncwarp();
+  for (int i = lane; i < kWTile * ps; i += 32) psi[i] = 0.0;  // columns past pa stay zero
+  for (int f = lane; f < p; f += 32) {
+    int ia, ib;
+    feature_factors(d, kind, f, ia, ib);
+    fidx[2 * f] = (int16_t)ia;
+    fidx[2 * f + 1] = (int16_t)ib;
+  }
+  // initial theta: projected theta0 (splitters.py:379)
+  const double* t0 = a.theta0 + kr * a.theta0_stride;
+  double nrm2 = 0.0;
+  for (int i = 0; i < d; ++i) nrm2 += t0[i] * t0[i];
+  const double nrm = sqrt(nrm2);
+  active = true;
+  fail = 0;
+  if (!(nrm > 1e-12) || !isfinite(nrm)) { active = false; fail = ART_SPLIT_INVALID; }
+  for (int i = lane; i < d; i += 32) th[i] = t0[i] / nrm;
+  if (lane == 0) th[d] = t0[d];
+  __syncwarp();
+  T = T0;
+  invT = 1.0 / T0;
+  alpha = fmin(fmax(P.alpha0, P.alpha_min), P.alpha_max);
+  stop = ART_STOP_MAX_ITERS;
+  feasit = -1;
+  hasfeas = conv = fbk = false;
+  iters = 0;
+  nright = 0;
+  loss = gnorm = dd = 0.0;
+  lamL = lamR = 0.0;
+  if (n == 0) { active = false; fail = ART_SPLIT_MIN_SIDE_POINTS; }
+  auto record_trace = [&](int iter) {
+    if (lane != 0) return;
+    if (a.tr_loss) a.tr_loss[kr * (M + 1) + iter] = loss;
+    if (a.tr_gnorm) a.tr_gnorm[kr * (M + 1) + iter] = gnorm;
+  };
+  auto save_feasible = [&](int it_) {
+    if (min(nright, (int)n - nright) >= req) {
+      hasfeas = true;
+      feasit = it_;
+      __syncwarp();
+      for (int i = lane; i <= d; i += 32) lf[i] = th[i];
+      __syncwarp();
+    }
+  };
+  double cL[6][2], cR[6][2];
+  // evaluate(theta): child fits from the Grams, then the residual pass
+  auto fit_and_resid = [&]() {
+    if (!solve_sides(cL, cR)) {
+      active = false;
+      fail = ART_SPLIT_CHOLESKY_FAILURE;
+      return;
+    }
+    resid_pass();
+  };
+  if (active) {
+    gram_pass(th, false, 0, true, cL, cR);
+    fit_and_resid();
+    if (active) {
+      tol = P.grad_atol + P.grad_rtol * gnorm;
+      save_feasible(0);
+      record_trace(0);
+    }
+  }
+  for (int iter = 0; iter < M && active; ++iter) {
+    // stop checks (splitters.py:424-437)
+    if (gnorm <= tol) { conv = true; stop = ART_STOP_GRADIENT_TOLERANCE; active = false; break; }
+    if (dd >= 0.0) { stop = ART_STOP_NON_DESCENT; active = false; break; }
+    // temperature after an accepted step (the candidate Grams are taken at it)
+    double T_next = T, invT_next = invT;
+    if (P.anneal_ratio != 1.0 && P.max_iters > 1) {
+      T_next = T0 * pow(P.anneal_ratio, (double)(iter + 1) / (double)(P.max_iters - 1));
+      invT_next = 1.0 / T_next;
+    }
+    // Armijo backtracking, one candidate per pass (optimizers.py:72-121),
+    // restarted from the adapted step after a failed attempt
+    bool accept = false;
+    int failures = 0, nb_ = 0;
+    double a_ = P.adaptive_alpha ? alpha : P.alpha0, step = 0.0;
+    const int max_trials = (P.max_backtracks + 1) * P.max_line_search_failures;
+    for (int trial = 0; trial < max_trials; ++trial) {
+      // candidate theta_c = project(theta + alpha d) (splitters.py:451, 497)
+      __syncwarp();
+      if (lane == 0) {
+        double s2 = 0.0;
+        for (int i = 0; i < d; ++i) {
+          const double v = th[i] + a_ * dn[i];
+          s2 += v * v;
+        }
+        const double nw = sqrt(s2);
+        for (int i = 0; i < d; ++i) tc[i] = (th[i] + a_ * dn[i]) / nw;
+        tc[d] = th[d] + a_ * dn[d];
+      }
+      __syncwarp();
+      const double fv = trial_gram_pass(invT_next, cL, cR);
+      const double rhs = __dadd_rn(loss, __dmul_rn(__dmul_rn(P.armijo_c, a_), dd));
+      if (fv <= rhs) {
+        accept = true;
+        step = a_;
+        if (P.adaptive_alpha) {  // AdaptiveAlpha.update (optimizers.py:49-66)
+          double na;
+          if (nb_ == 0) na = step * P.alpha_grow;
+          else if (nb_ >= P.heavy_backtrack_threshold) na = step * P.alpha_recovery;
+          else na = step / P.rho;
+          alpha = fmin(fmax(na, P.alpha_min), P.alpha_max);
+        }
+        break;
+      }
+      if (nb_ < P.max_backtracks) {  // next backtrack
+        ++nb_;
+        a_ *= P.rho;
+        continue;
+      }
+      // attempt failed: the last step tried
+      if (P.adaptive_alpha) alpha = fmin(fmax(a_ * P.rho, P.alpha_min), P.alpha_max);
+      ++failures;
+      int st = -1;
+      if (!P.adaptive_alpha) st = ART_STOP_LINE_SEARCH_FAILED;
+      else if (failures >= P.max_line_search_failures) st = ART_STOP_MAX_LINE_SEARCH_FAILURES;
+      else if (alpha <= P.alpha_min) st = ART_STOP_ALPHA_MIN_REACHED;
+      if (st >= 0) {
+        stop = st;
+        break;
+      }
+      nb_ = 0;
+      a_ = alpha;
+    }
+    if (!accept) {
+      if (stop == ART_STOP_MAX_ITERS) stop = ART_STOP_MAX_LINE_SEARCH_FAILURES;
+      active = false;
+      break;
+    }
+    // commit theta <- theta_c, then the new temperature
+    __syncwarp();
+    for (int i = lane; i <= d; i += 32) th[i] = tc[i];
+    __syncwarp();
+    T = T_next;
+    invT = invT_next;
+    iters = iter + 1;
+    if (lane == 0) {
+      if (a.tr_step) a.tr_step[kr * P.max_iters + iter] = step;
+      if (a.tr_back) a.tr_back[kr * P.max_iters + iter] = nb_;
+    }
+    fit_and_resid();
+    if (active) {
+      save_feasible(iter + 1);
+      record_trace(iter + 1);
+    }
+  }
+  // ------------------------------------------------ finish (splitters.py:584-601)
+  if (fail == 0) {
+    const bool final_ok = min(nright, (int)n - nright) >= req;
+    __syncwarp();
+    if (!final_ok && fb_allowed && hasfeas) {
+      for (int i = lane; i <= d; i += 32) th[i] = lf[i];
+      fbk = true;
+    }
+    __syncwarp();
+    double s2 = 0.0;
+    for (int i = 0; i < d; ++i) s2 += th[i] * th[i];
+    const double nw = sqrt(s2);
+    __syncwarp();
+    if (lane == 0)
+      for (int i = 0; i < d; ++i) th[i] = th[i] / nw;
+    __syncwarp();
+    // hard partition: exact sides and right count; hard child fits when asked
+    gram_pass(th, true, req, P.hard_refit != 0, cL, cR);
+    if (nright < req || (int)n - nright < req) {
+      fail = ART_SPLIT_MIN_SIDE_POINTS;
+    } else if (P.hard_refit) {
+      if (!solve_sides(cL, cR)) fail = ART_SPLIT_CHOLESKY_FAILURE;
+      else hard_losses();
+    }
+  }
+  // ----------------------------------------------------------- write results
+  __syncwarp();
+  if (lane == 0) {
+    const int dts = a.dmax + 1;
+    for (int i = 0; i <= d; ++i) a.r_theta[kr * dts + i] = th[i];
+    a.r_fail[kr] = fail;
+    a.r_stop[kr] = stop;
+    a.r_iters[kr] = iters;
+    a.r_nright[kr] = nright;
+    a.r_flags[kr] = (conv ? 1 : 0) | (fbk ? 2 : 0);
+    a.r_fbiter[kr] = feasit;
+    a.r_alpha[kr] = P.adaptive_alpha ? alpha : P.alpha0;
+    const double nan = __longlong_as_double(0x7ff8000000000000ll);
+    const bool have = P.hard_refit && fail == 0;
+    a.r_loss[kr] = have ? loss : nan;
+    a.r_child[kr * 2] = P.hard_refit ? hlossL : nan;
+    a.r_child[kr * 2 + 1] = P.hard_refit ? hlossR : nan;
+    a.r_ridge[kr * 2] = lamL;
+    a.r_ridge[kr * 2 + 1] = lamR;
+    for (int f = 0; f < p; ++f) {
+      a.r_beta[(kr * 2) * a.pmax + f] = have ? bl[f] : nan;
+      a.r_beta[(kr * 2 + 1) * a.pmax + f] = have ? br[f] : nan;
+    }
+  }
+  __syncwarp();
+}
+
+// MINB = 2: two 8-warp CTAs per SM (a 128-register cap)
+__global__ void __launch_bounds__(kWThreads, 2) split_warp_kernel(SplitArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  SplitWarp W(a, smem, warp);
+  const int count = a.counts[0];
+  for (;;) {
+    int q = 0;
+    if (lane == 0) q = atomicAdd(&a.counts[1], 1);
+    q = __shfl_sync(0xffffffffu, q, 0);
+    if (q >= count) break;
+    W.run(a.items[q].x);
+  }
+}
+
 // MINB resident CTAs per SM: 1 keeps every register a thread wants and the
 // deepest row ring; 2 doubles the warps that hide the per-row latency of the
 // passes at the cost of a 128-register cap and half the shared memory
@@ -1716,7 +2394,7 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
       !(prm->alpha_min > 0.0) || prm->alpha_max < prm->alpha_min || prm->min_side_points < 1 ||
       !(prm->min_side_fraction >= 0.0 && prm->min_side_fraction < 0.5) || !(prm->anneal_ratio > 0.0) ||
       prm->group_restarts < 0 || prm->trial_steps < 0 || prm->ctas_per_sm < 0 || prm->ctas_per_sm > 2 ||
-      prm->tensor_gram < 0 || prm->tensor_gram > 1) {
+      prm->tensor_gram < 0 || prm->tensor_gram > 1 || prm->restart_warps < 0 || prm->restart_warps > 1) {
     set_error("art_split_level: invalid splitter parameters");
     return ART_E_INVALID;
   }
@@ -1751,6 +2429,10 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
       }
     }
   }
+  // Warp-per-restart form: asked for, the level fits its register tiles and
+  // no tensor-core Gram is in use
+  const bool use_warp = prm->restart_warps == 1 && !use_tc && pr->max_dim <= kWMaxD &&
+                        pr->max_features + 1 <= kWMaxPa;
   const SplitWs wl = split_ws(K, R, pr->max_dim, pr->max_features);
   if (!workspace || ws_bytes < wl.total) {
     set_error("art_split_level: workspace %zu bytes < required %zu", ws_bytes, wl.total);
@@ -1804,6 +2486,14 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
     prof_end(s);
     count_launch();
   }
+  if (use_warp) {
+    // one work item per (node, restart), largest nodes first
+    a.Rg = 1;
+    a.groups = R;
+    a.TC = 2;
+    a.H = 1;
+    a.gang_on = 0;
+  }
   if (cudaMemsetAsync(a.counts, 0, 4 * (kErrSlot + 1), s) != cudaSuccess) return check_launch("memset");
   if (a.gang_on &&
       (cudaMemsetAsync(a.gang_rec, 0, 16 * (size_t)K * a.groups, s) != cudaSuccess ||
@@ -1816,6 +2506,28 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
   split_plan_scatter<<<pg, 256, 0, s>>>(a);
   prof_end(s);
   count_launch(); count_launch(); count_launch();
+  if (use_warp) {
+    const size_t wsm = warp_layout(a.dmax, a.pmax).total;
+    if (cudaFuncSetAttribute(split_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      set_error("art_split_level: cannot reserve %zu bytes of shared memory", wsm);
+      return ART_E_UNSUPPORTED;
+    }
+    const int occ = resident_ctas((const void*)split_warp_kernel, kWThreads, wsm);
+    const int64_t resident = (int64_t)device_sm_count() * std::max(occ, 1);
+    const int64_t grid = std::min<int64_t>(resident, (K * R + kWWarps - 1) / kWWarps);
+    prof_begin("split_level", s);
+    split_warp_kernel<<<(unsigned)std::max<int64_t>(grid, 1), kWThreads, wsm, s>>>(a);
+    prof_end(s);
+    count_launch();
+    if (int rc = check_launch("split_level")) return rc;
+    prof_begin("split_select", s);
+    split_select<<<(unsigned)((K + 127) / 128), 128, 0, s>>>(a, *out);
+    prof_end(s);
+    count_launch();
+    return check_launch("split_select");
+  }
   // longest chunk (fewer block barriers per row) with a ring of at least 4
   // stages (2 at two CTAs per SM) that fits shared memory, then the deepest
   // ring for that chunk; two CTAs per SM fall back to one when even the

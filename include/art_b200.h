@@ -230,6 +230,14 @@ typedef struct ArtSplitParams {
                                    and the gate weights, FP32 accumulation over
                                    128 rows, FP64 across) when the augmented
                                    model has at most 21 features; 0 = FP64 sums */
+  int32_t restart_warps;        /* 1 = one warp per (node, restart): each warp
+                                   streams its node's rows in 32-row tiles and
+                                   runs its restart's loop with no block
+                                   barriers (d <= 23, p <= 23, at most 8 trial
+                                   steps, not with tensor_gram; group_restarts
+                                   and ctas_per_sm are then unused); 0 = the
+                                   restarts of a group share one CTA's row
+                                   passes                                   */
 } ArtSplitParams;
 
 typedef struct ArtSplitProblem {

@@ -52,7 +52,7 @@ def test_autotune_table_persists_and_is_keyed_by_device(tmp_path, monkeypatch):
     monkeypatch.setattr(autotune, "_LOADED", False)
     autotune.clear()
     try:
-        assert autotune.cached_split_shape(16, 17, 16) == (0, 0, 0)
+        assert autotune.cached_split_shape(16, 17, 16) == (0, 0, 0, 0)
         assert autotune.cached_ridge_choice() == (0, None)
         autotune._store(autotune._split_key(16, 17, 16), {"group_restarts": 8, "trial_steps": 2,
                                                                   "ctas_per_sm": 2})
@@ -61,10 +61,10 @@ def test_autotune_table_persists_and_is_keyed_by_device(tmp_path, monkeypatch):
         assert len(saved) == 2
         autotune.clear()
         monkeypatch.setattr(autotune, "_LOADED", False)
-        assert autotune.cached_split_shape(16, 17, 16) == (8, 2, 2)    # reloaded from the file
+        assert autotune.cached_split_shape(16, 17, 16) == (8, 2, 2, 0)    # reloaded from the file
         assert autotune.cached_ridge_choice() == (153, False)
         monkeypatch.setattr(autotune, "device_key", lambda: "other-device|sm132|cc9.0")
-        assert autotune.cached_split_shape(16, 17, 16) == (0, 0, 0)    # another device: untuned
+        assert autotune.cached_split_shape(16, 17, 16) == (0, 0, 0, 0)    # another device: untuned
     finally:
         autotune.clear()
 
@@ -74,13 +74,20 @@ def test_split_candidates_respect_thread_and_backtrack_limits(R, backtracks):
     sys.path.insert(0, str(ROOT / "adaptive-regression-trees-art-_b200"))
     from art import autotune
 
-    cands = autotune.split_candidates(R, backtracks)
+    cands = autotune.split_candidates(R, backtracks, 16, 17)
     assert cands and len(set(cands)) == len(cands)
-    for g, h, c in cands:
+    for g, h, c, w in cands:
+        if w:
+            assert g == 0 and c == 0 and 1 <= h <= min(8, backtracks + 1)
+            continue
         assert 1 <= g <= min(R, 16)
         assert 1 <= h <= min(32, 256 // g, backtracks + 1)
         assert c in (1, 2) and (c == 1 or g <= 8)
-    assert {c for _, _, c in cands} == {1, 2}
+    assert {c for _, _, c, w in cands if not w} == {1, 2}
+    assert any(w for *_, w in cands)
+    # too wide for the warp form, or with the tensor-core Gram: CTA shapes only
+    assert not any(w for *_, w in autotune.split_candidates(R, backtracks, 24, 25))
+    assert not any(w for *_, w in autotune.split_candidates(R, backtracks, 16, 17, tensor_gram=True))
 
 
 def test_graph_shape_classes_round_up_to_powers_of_two():

@@ -27,8 +27,13 @@ def splitter_for(kind, T, lam, R, iters, extra):
     return SoftObliqueSplitter(model, T, max_iters=int(iters), n_restarts=int(R), **extra)
 
 
+# 0: the restarts of a group share one CTA's row passes; 1: one warp per restart
+FORMS = [0, 1]
+
+
+@pytest.mark.parametrize("warps", FORMS)
 @pytest.mark.parametrize("i", range(int(SG["count"])))
-def test_split_matches_reference_golden(i):
+def test_split_matches_reference_golden(i, warps):
     from art.splitters import level_result_to_split, split_level
 
     kind, T, lam, R, iters, parent_loss = SG[f"s{i}_meta"]
@@ -36,7 +41,7 @@ def test_split_matches_reference_golden(i):
     s = splitter_for(int(kind), T, lam, R, iters, extra)
     X, y = SG[f"s{i}_X"], SG[f"s{i}_y"]
     res = split_level(s, X.reshape(-1), y, [0, len(y)], [X.shape[1]], [int(kind)], T, lam,
-                      parent_loss=[parent_loss], theta0=SG[f"s{i}_theta0"][None], traces=True)
+                      parent_loss=[parent_loss], theta0=SG[f"s{i}_theta0"][None], traces=True, restart_warps=warps)
     out = level_result_to_split(s, res, 0, len(y), parent_loss, True)
     ref_theta = SG[f"s{i}_theta"]
     if not np.allclose(np.r_[out.w, out.z], ref_theta, rtol=1e-9, atol=1e-11):
@@ -88,8 +93,9 @@ def random_level(seed, K=10, R=3, d=4, kinds=(O.AFFINE, O.POLY2)):
     return ns, Xs, ys, np.array(th0), np.array(kd)
 
 
+@pytest.mark.parametrize("warps", FORMS)
 @pytest.mark.parametrize("anneal", [1.0, 0.1])
-def test_level_matches_oracle_per_node(anneal):
+def test_level_matches_oracle_per_node(anneal, warps):
     """Many nodes of uneven size and mixed feature kinds in one launch == per-node oracle."""
 
     from art.splitters import level_result_to_split, split_level
@@ -105,7 +111,7 @@ def test_level_matches_oracle_per_node(anneal):
         parent.append(float(np.mean((y - phi @ b) ** 2)))
     ro = np.concatenate([[0], np.cumsum(ns)])
     res = split_level(s, np.concatenate([X.reshape(-1) for X in Xs]), np.concatenate(ys), ro, [4] * K, kd, T, lam,
-                      parent_loss=parent, theta0=th0, anneal_ratio=anneal, traces=True)
+                      parent_loss=parent, theta0=th0, anneal_ratio=anneal, traces=True, restart_warps=warps)
     p = S.Params(max_iters=iters, n_restarts=R, min_side_points=5, anneal_ratio=anneal)
     picks = (res.flags.cpu().numpy() >> 8) & 255
     for k in range(K):
@@ -129,7 +135,8 @@ def test_level_matches_oracle_per_node(anneal):
         np.testing.assert_allclose(out.loss, ref["loss"], rtol=1e-9)
 
 
-def test_partition_only_mode_and_failures():
+@pytest.mark.parametrize("warps", FORMS)
+def test_partition_only_mode_and_failures(warps):
     from art.splitters import SplitNotFoundError, level_result_to_split, split_level
 
     rng = np.random.default_rng(8)
@@ -138,13 +145,13 @@ def test_partition_only_mode_and_failures():
     s = splitter_for(O.AFFINE, 0.1, 1e-6, 1, 10, {"min_side_points": 40, "min_side_fraction": 0.0})
     th0 = np.array([[[1.0, 0.0, 0.0]]])
     res = split_level(s, X.reshape(-1), y, [0, 60], [2], [O.AFFINE], 0.1, 1e-6, parent_loss=[0.25], theta0=th0,
-                      hard_refit=False)
+                      hard_refit=False, restart_warps=warps)
     with pytest.raises(SplitNotFoundError) as err:
         level_result_to_split(s, res, 0, 60, 0.25, False)
     assert err.value.reason == "min_side_points"
     s.min_side_points = 5
     res = split_level(s, X.reshape(-1), y, [0, 60], [2], [O.AFFINE], 0.1, 1e-6, parent_loss=[0.25], theta0=th0,
-                      hard_refit=False)
+                      hard_refit=False, restart_warps=warps)
     out = level_result_to_split(s, res, 0, 60, 0.25, False)
     assert out.loss is None and out.left_model is None and out.n_left + out.n_right == 60
     right = (X @ out.w - out.z) >= 0
@@ -185,11 +192,12 @@ def test_public_split_api_matches_oracle():
                                rtol=1e-8, atol=1e-10)
 
 
-@pytest.mark.parametrize("shape", [(1, 1, 1), (2, 4, 2), (3, 32, 1), (8, 2, 1), (8, 2, 2)])
+@pytest.mark.parametrize("shape", [(1, 1, 1, 0), (2, 4, 2, 0), (3, 32, 1, 0), (8, 2, 1, 0), (8, 2, 2, 0),
+                                   (0, 1, 0, 1), (0, 2, 0, 1), (0, 4, 0, 1), (0, 16, 0, 1)])
 def test_every_launch_shape_matches_oracle(shape):
-    """Restarts per CTA, trial steps per pass and CTAs per SM regroup the work
-    (and the summation order of row sums): each shape meets the per-node oracle check
-    of the default shape."""
+    """Restarts per CTA, trial steps per pass, CTAs per SM, or one warp per
+    restart regroup the work (and the summation order of row sums): each
+    shape meets the per-node oracle check of the default shape."""
 
     from art.splitters import level_result_to_split, split_level
 
@@ -205,7 +213,7 @@ def test_every_launch_shape_matches_oracle(shape):
     ro = np.concatenate([[0], np.cumsum(ns)])
     res = split_level(s, np.concatenate([X.reshape(-1) for X in Xs]), np.concatenate(ys), ro, [4] * K, kd, T, lam,
                       parent_loss=parent, theta0=th0, group_restarts=shape[0], trial_steps=shape[1],
-                      ctas_per_sm=shape[2])
+                      ctas_per_sm=shape[2], restart_warps=shape[3])
     p = S.Params(max_iters=iters, n_restarts=R, min_side_points=5)
     picks = (res.flags.cpu().numpy() >> 8) & 255
     for k in range(K):
@@ -224,7 +232,8 @@ def test_every_launch_shape_matches_oracle(shape):
         assert out.n_iters == ref["n_iters"] and out.n_right == ref["n_right"]
 
 
-def test_long_nodes_stream_through_the_row_ring():
+@pytest.mark.parametrize("warps", FORMS)
+def test_long_nodes_stream_through_the_row_ring(warps):
     """Nodes much longer than the row ring (many chunks per pass) match the oracle."""
 
     from art.splitters import level_result_to_split, split_level
@@ -238,7 +247,7 @@ def test_long_nodes_stream_through_the_row_ring():
     th0 = np.array([[[0.6, 0.8, 0.0, 0.05]] for _ in ns])
     ro = np.concatenate([[0], np.cumsum(ns)])
     res = split_level(s, np.concatenate([X.reshape(-1) for X in Xs]), np.concatenate(ys), ro, [3] * 4,
-                      [O.AFFINE] * 4, T, lam, parent_loss=[1.0] * 4, theta0=th0)
+                      [O.AFFINE] * 4, T, lam, parent_loss=[1.0] * 4, theta0=th0, restart_warps=warps)
     p = S.Params(max_iters=iters, n_restarts=1, min_side_points=1)
     for k in (0, 3):
         opt = S.optimize(Xs[k], ys[k], th0[k][0], T, O.AFFINE, lam, p)
@@ -362,7 +371,8 @@ def c3_nodes(seed, ns, d=16):
     return Xs, ys, rng
 
 
-def test_c3_shape_fp64_level_matches_oracle_at_1e10():
+@pytest.mark.parametrize("warps", FORMS)
+def test_c3_shape_fp64_level_matches_oracle_at_1e10(warps):
     """The C3 split configuration at full shape on a few nodes: d = 16, 16
     restarts, exactly 60 projected-gradient steps (grad_atol = grad_rtol = 0),
     temperature annealed 0.2 -> 0.02, affine child fits with lambda = 1e-6,
@@ -386,7 +396,8 @@ def test_c3_shape_fp64_level_matches_oracle_at_1e10():
         parent.append(float(np.mean((y - phi @ b) ** 2)))
     ro = np.concatenate([[0], np.cumsum(ns)])
     res = split_level(s, np.concatenate([X.reshape(-1) for X in Xs]), np.concatenate(ys), ro, [d] * K,
-                      [O.AFFINE] * K, 0.2, lam, parent_loss=parent, theta0=th0, anneal_ratio=0.1, traces=True)
+                      [O.AFFINE] * K, 0.2, lam, parent_loss=parent, theta0=th0, anneal_ratio=0.1, traces=True,
+                      restart_warps=warps)
     p = S.Params(max_iters=iters, n_restarts=R, anneal_ratio=0.1, **extra)
     picks = (res.flags.cpu().numpy() >> 8) & 255
     for k in range(K):
@@ -410,8 +421,8 @@ def test_c3_shape_fp64_level_matches_oracle_at_1e10():
         np.testing.assert_allclose(out.loss, ref["loss"], rtol=1e-10)
 
 
-@pytest.mark.parametrize("tensor_gram", [False, True])
-def test_mixed_form_objective_along_its_trajectory_within_1e5(tensor_gram):
+@pytest.mark.parametrize("tensor_gram,warps", [(False, 0), (True, 0), (False, 1)])
+def test_mixed_form_objective_along_its_trajectory_within_1e5(tensor_gram, warps):
     """The mixed form (single-precision gates, FP64 sums and solves): at every
     iterate of its own trajectory, the soft objective it reports is within
     1e-5 relative of the FP64 oracle's objective at that same theta.  The
@@ -432,7 +443,7 @@ def test_mixed_form_objective_along_its_trajectory_within_1e5(tensor_gram):
         s.precision = prec
         s.tensor_gram = tensor_gram and prec == "mixed"
         return split_level(s, x, y, ro, [d] * K, kd, T, lam, parent_loss=[1.0] * K, theta0=th0, traces=True,
-                           hard_refit=True)
+                           hard_refit=True, restart_warps=warps)
 
     full = run("mixed", M)
     trace = full.trace_loss.cpu().numpy()[:, 0, :]
