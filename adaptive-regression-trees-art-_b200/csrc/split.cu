@@ -1460,35 +1460,23 @@ __device__ __forceinline__ void dmma_884(double (&c)[2], double a, double b) {
 constexpr int kWTile = 32;                                   // rows per tile
 constexpr int kWMaxPa = 24;                                  // p + 1 (augmented with y)
 constexpr int kWMaxD = 23;                                   // inputs
-constexpr int kWMaxK = 6;                                    // 4-feature steps of the score MMAs
-constexpr int kWThreads = 256;
+constexpr int kWThreads = 128;                               // 4 warps per CTA
 constexpr int kWWarps = kWThreads / 32;
 
+// Per-warp shared memory (doubles): psi | cf | sc | tc | th | dn | gr | lf |
+// bl | br | A | fidx | xt; psi's row stride is 8 NB + 1 (NB = the kernel's
+// block count), the rest follow from (dmax, pmax).
 struct WLayout {
-  size_t xt, psi, cf, sc, tc, A, th, dn, gr, lf, bl, br, fidx, per_warp, total;
+  size_t per_warp, total;
   int xs, ps;
 };
 __host__ __device__ inline WLayout warp_layout(int dmax, int pmax) {
   WLayout L;
   const int pa = pmax + 1, E = pa * (pa + 1) / 2, dt = dmax + 1;
   L.xs = dmax | 1;
-  L.ps = (8 * ((pa + 7) / 8)) | 1;                  // whole 8-column blocks for the MMAs
-  size_t o = 0;
-  L.xt = o; o += (size_t)kWTile * L.xs;             // doubles from here on
-  L.psi = o; o += (size_t)kWTile * L.ps;
-  L.cf = o; o += 2 * kWTile;                        // per-row Gram weights / gradient coefficients
-  L.sc = o; o += 3 * kWTile;                        // per-row u, f_L, f_R
-  L.tc = o; o += dt;                                // trial candidate theta
-  L.A = o; o += (size_t)E + 2 * pa;
-  L.th = o; o += dt;
-  L.dn = o; o += dt;
-  L.gr = o; o += dt;
-  L.lf = o; o += dt;
-  L.bl = o; o += pmax;
-  L.br = o; o += pmax;
-  L.fidx = o; o += pa;                              // two int16 per feature, in a double
-  L.per_warp = o;                                   // doubles per warp
-  L.total = (size_t)kWWarps * o * 8;
+  L.ps = (8 * ((pa + 7) / 8)) | 1;
+  L.per_warp = (size_t)kWTile * L.ps + 5 * kWTile + 5 * dt + 2 * pmax + E + 2 * pa + pa + kWTile * L.xs;
+  L.total = (size_t)kWWarps * L.per_warp * 8;
   return L;
 }
 
@@ -1502,20 +1490,41 @@ __device__ __forceinline__ int x_column(int kind) {
   return (kind == ART_FEATURES_POLY1 || kind == ART_FEATURES_POLY2) ? 1 : 0;
 }
 
+// NB 8-column blocks of psi (pa <= 8 NB); the score MMAs take NK = 2 NB
+// 4-column steps.  Fixed trip counts: padding columns and rows are zeros.
+template <int NB>
 struct SplitWarp {
+  static constexpr int NK = 2 * NB;
   const SplitArgs& a;
-  int xs, ps;  // padded row strides of xt and psi (odd, in doubles)
-  // the x tile: its own buffer, or for affine features the first d columns
-  // of psi = [x, 1, y] (no second copy)
-  double *xt, *xt0;
-  int xs0;
-  bool aff = false;
-  double *psi, *cf, *sc, *tc, *A, *th, *dn, *gr, *lf, *bl, *br;
-  int16_t* fidx;
-  int lane, kq, mq;  // lane, and its (k, m) coordinates in the MMA fragments
+  static constexpr int ps = 8 * NB + 1;  // psi row stride (odd, in doubles)
+  double* base;                          // this warp's shared-memory region
+  bool aff = false;                      // affine features: x is psi's first d columns
+  int lane;
+  // region pointers, recomputed from the launch's (dmax, pmax) where used
+  __device__ double* psi() const { return base; }
+  __device__ double* cf() const { return base + kWTile * ps; }
+  __device__ double* sc() const { return base + kWTile * ps + 2 * kWTile; }
+  __device__ double* tc() const { return base + kWTile * ps + 5 * kWTile; }
+  __device__ double* th() const { return tc() + (a.dmax + 1); }
+  __device__ double* dn() const { return tc() + 2 * (a.dmax + 1); }
+  __device__ double* gr() const { return tc() + 3 * (a.dmax + 1); }
+  __device__ double* lf() const { return tc() + 4 * (a.dmax + 1); }
+  __device__ double* bl() const { return tc() + 5 * (a.dmax + 1); }
+  __device__ double* br() const { return bl() + a.pmax; }
+  __device__ double* A() const { return bl() + 2 * a.pmax; }
+  __device__ int16_t* fidx() const {
+    return (int16_t*)(A() + (a.pmax + 1) * (a.pmax + 2) / 2 + 2 * (a.pmax + 1));
+  }
+  // the x tile: its own buffer, or for affine features psi itself
+  __device__ double* xt() const {
+    return aff ? base : (double*)fidx() + (a.pmax + 1);
+  }
+  __device__ int xs() const { return aff ? ps : (a.dmax | 1); }
+  __device__ int kq() const { return lane & 3; }   // fragment coordinates of this lane
+  __device__ int mq() const { return lane >> 2; }
   // item
   int64_t k, r0, n, xoff, kr;
-  int d, kind, p, pa, E, xcol, nb, nk;
+  int d, kind, p, pa, E, xcol;
   double ridge, T0;
   // restart state (uniform)
   double loss = 0, dd = 0, tol = 0, gnorm = 0, T = 0, invT = 0, alpha = 0, lamL = 0, lamR = 0;
@@ -1524,17 +1533,8 @@ struct SplitWarp {
   bool active = false, hasfeas = false, conv = false, fbk = false;
 
   __device__ SplitWarp(const SplitArgs& a_, unsigned char* sm, int warp) : a(a_) {
-    const WLayout L = warp_layout(a.dmax, a.pmax);
-    xs = xs0 = L.xs;
-    ps = L.ps;
-    double* base = (double*)sm + (size_t)warp * L.per_warp;
-    xt = xt0 = base + L.xt; psi = base + L.psi; cf = base + L.cf; sc = base + L.sc; tc = base + L.tc;
-    A = base + L.A; th = base + L.th; dn = base + L.dn; gr = base + L.gr; lf = base + L.lf;
-    bl = base + L.bl; br = base + L.br;
-    fidx = (int16_t*)(base + L.fidx);
+    base = (double*)sm + (size_t)warp * warp_layout(a.dmax, a.pmax).per_warp;
     lane = threadIdx.x & 31;
-    kq = lane & 3;
-    mq = lane >> 2;
   }
 
   // Tile rows [t0, t0 + rows): x (coalesced copy) and psi = [phi(x); y],
@@ -1544,21 +1544,23 @@ struct SplitWarp {
     const double* src = a.x + xoff + t0 * d;
     const int tot = rows * d;
     const uint32_t inv = 65536u / (uint32_t)d + 1u;  // e / d by a multiply (e < 32 * 23)
+    double* xd = xt();
+    const int xsv = xs();
     __syncwarp();
     for (int e = lane; e < tot; e += 32) {
       const int rr = (int)(((uint32_t)e * inv) >> 16), i = e - rr * d;
-      xt[rr * xs + i] = __ldg(src + e);
+      xd[rr * xsv + i] = __ldg(src + e);
     }
     yv = lane < rows ? __ldg(a.y + r0 + t0 + lane) : 0.0;
     __syncwarp();
-    double* pr = psi + lane * ps;
-    const double* xr = xt + lane * xs;
+    double* pr = psi() + lane * ps;
+    const double* xr = xt() + lane * xs();
     if (aff && lane < rows) {
       pr[d] = 1.0;
       pr[p] = yv;
     } else if (lane < rows) {
       for (int f = 0; f < p; ++f) {
-        const int ia = fidx[2 * f], ib = fidx[2 * f + 1];
+        const int ia = fidx()[2 * f], ib = fidx()[2 * f + 1];
         pr[f] = (ia < 0 ? 1.0 : xr[ia]) * (ib < 0 ? 1.0 : xr[ib]);
       }
       pr[p] = yv;
@@ -1571,62 +1573,59 @@ struct SplitWarp {
 
   // B fragments of [w; beta_L; beta_R] (columns 0, 1, 2; rows = psi columns)
   // for the score MMAs: lane (k, m) holds B[4 s + k][m] of step s.
-  __device__ void score_operand(const double* w, double (&b)[kWMaxK]) const {
+  __device__ void score_operand(const double* w, double (&b)[NK]) const {
 #pragma unroll
-    for (int s = 0; s < kWMaxK; ++s) {
-      const int f = 4 * s + kq;
+    for (int s = 0; s < NK; ++s) {
+      const int f = 4 * s + kq();
       double v = 0.0;
-      if (mq == 0) v = (f >= xcol && f < xcol + d) ? w[f - xcol] : 0.0;
-      else if (mq == 1) v = f < p ? bl[f] : 0.0;
-      else if (mq == 2) v = f < p ? br[f] : 0.0;
-      b[s] = s < nk ? v : 0.0;
+      if (mq() == 0) v = (f >= xcol && f < xcol + d) ? w[f - xcol] : 0.0;
+      else if (mq() == 1) v = f < p ? bl()[f] : 0.0;
+      else if (mq() == 2) v = f < p ? br()[f] : 0.0;
+      b[s] = v;
     }
   }
 
   // u, f_L, f_R of this lane's row: psi [w; beta_L; beta_R] by MMAs over
   // 8-row blocks, staged through shared memory.  Call after load_tile.
-  __device__ void scores(int rows, const double (&b)[kWMaxK], double& u, double& fl, double& fr) {
+  __device__ void scores(const double (&b)[NK], double& u, double& fl, double& fr) {
 #pragma unroll
     for (int rb = 0; rb < 4; ++rb) {
-      if (8 * rb < rows) {  // warp-uniform
-        double c[2] = {0.0, 0.0};
-        const double* pr = psi + (8 * rb + mq) * ps + kq;
+      double c[2] = {0.0, 0.0};
+      const double* pr = psi() + (8 * rb + mq()) * ps + kq();
 #pragma unroll
-        for (int s = 0; s < kWMaxK; ++s)
-          if (s < nk) dmma_884(c, pr[4 * s], b[s]);
-        if (kq == 0) { sc[8 * rb + mq] = c[0]; sc[kWTile + 8 * rb + mq] = c[1]; }
-        else if (kq == 1) sc[2 * kWTile + 8 * rb + mq] = c[0];
-      }
+      for (int s = 0; s < NK; ++s) dmma_884(c, pr[4 * s], b[s]);
+      if (kq() == 0) { sc()[8 * rb + mq()] = c[0]; sc()[kWTile + 8 * rb + mq()] = c[1]; }
+      else if (kq() == 1) sc()[2 * kWTile + 8 * rb + mq()] = c[0];
     }
     __syncwarp();
-    u = sc[lane];
-    fl = sc[kWTile + lane];
-    fr = sc[2 * kWTile + lane];
+    u = sc()[lane];
+    fl = sc()[kWTile + lane];
+    fr = sc()[2 * kWTile + lane];
     __syncwarp();
   }
 
   // G_side += (q_side psi)^T psi over the tile (lower 8 x 8 blocks), the
   // weights staged in cf.  Rows past the tile's end are zero rows.
-  __device__ void gram_tile(int rows, double qL, double qR, double (&cL)[6][2], double (&cR)[6][2]) {
-    cf[lane] = qL;
-    cf[kWTile + lane] = qR;
+  static constexpr int NBLK = NB * (NB + 1) / 2;  // lower-triangular 8 x 8 blocks
+  __device__ void gram_tile(double qL, double qR, double (&cL)[NBLK][2], double (&cR)[NBLK][2]) {
+    cf()[lane] = qL;
+    cf()[kWTile + lane] = qR;
     __syncwarp();
-    for (int k0 = 0; k0 < rows; k0 += 4) {
-      const int row = k0 + kq;
-      const double* pr = psi + row * ps + mq;
-      const double ql = cf[row], qr = cf[kWTile + row];
-      double v[3];
+#pragma unroll 2
+    for (int k0 = 0; k0 < kWTile; k0 += 4) {
+      const int row = k0 + kq();
+      const double* pr = psi() + row * ps + mq();
+      const double ql = cf()[row], qr = cf()[kWTile + row];
+      double v[NB];
 #pragma unroll
-      for (int I = 0; I < 3; ++I) v[I] = I < nb ? pr[8 * I] : 0.0;
+      for (int I = 0; I < NB; ++I) v[I] = pr[8 * I];
 #pragma unroll
-      for (int I = 0; I < 3; ++I) {
-        if (I < nb) {  // warp-uniform
-          const double aL = ql * v[I], aR = qr * v[I];
+      for (int I = 0; I < NB; ++I) {
+        const double aL = ql * v[I], aR = qr * v[I];
 #pragma unroll
-          for (int J = 0; J <= I; ++J) {
-            dmma_884(cL[I * (I + 1) / 2 + J], aL, v[J]);
-            dmma_884(cR[I * (I + 1) / 2 + J], aR, v[J]);
-          }
+        for (int J = 0; J <= I; ++J) {
+          dmma_884(cL[I * (I + 1) / 2 + J], aL, v[J]);
+          dmma_884(cR[I * (I + 1) / 2 + J], aR, v[J]);
         }
       }
     }
@@ -1634,16 +1633,16 @@ struct SplitWarp {
   }
 
   // g += psi^T c over the tile (column 0 of the MMA output; c staged in cf).
-  __device__ void grad_tile(int rows, double c, double (&g)[3][2]) {
-    cf[lane] = c;
+  __device__ void grad_tile(double c, double (&g)[NB][2]) {
+    cf()[lane] = c;
     __syncwarp();
-    for (int k0 = 0; k0 < rows; k0 += 4) {
-      const int row = k0 + kq;
-      const double* pr = psi + row * ps + mq;
-      const double b = mq == 0 ? cf[row] : 0.0;
 #pragma unroll
-      for (int I = 0; I < 3; ++I)
-        if (I < nb) dmma_884(g[I], pr[8 * I], b);
+    for (int k0 = 0; k0 < kWTile; k0 += 4) {
+      const int row = k0 + kq();
+      const double* pr = psi() + row * ps + mq();
+      const double b = mq() == 0 ? cf()[row] : 0.0;
+#pragma unroll
+      for (int I = 0; I < NB; ++I) dmma_884(g[I], pr[8 * I], b);
     }
     __syncwarp();
   }
@@ -1651,38 +1650,39 @@ struct SplitWarp {
   __device__ double gate(double s) const { return a.mixed ? sigm32(s) : sigm(s); }
 
   __device__ void run(int item);
-  __device__ bool solve_sides(const double (&cL)[6][2], const double (&cR)[6][2]);
-  __device__ void gram_pass(const double* w, bool hard, int req, bool accumulate, double (&cL)[6][2],
-                            double (&cR)[6][2]);
+  __device__ bool solve_sides(const double (&cL)[NBLK][2], const double (&cR)[NBLK][2]);
+  __device__ void gram_pass(const double* w, bool hard, int req, bool accumulate, double (&cL)[NBLK][2],
+                            double (&cR)[NBLK][2]);
   __device__ void resid_pass();
-  __device__ double trial_gram_pass(double invT_next, double (&cL)[6][2], double (&cR)[6][2]);
+  __device__ double trial_gram_pass(double invT_next, double (&cL)[NBLK][2], double (&cR)[NBLK][2]);
   __device__ void hard_losses();
 };
 
 // Both sides' ridge solves from the accumulated Gram blocks; false (restart
 // failed) when either factorisation fails.
-__device__ bool SplitWarp::solve_sides(const double (&cL)[6][2], const double (&cR)[6][2]) {
-  double* z_ = A + E;
+template <int NB>
+__device__ bool SplitWarp<NB>::solve_sides(const double (&cL)[NBLK][2], const double (&cR)[NBLK][2]) {
+  double* z_ = A() + E;
   bool ok = true;
   for (int side = 0; side < 2; ++side) {
     __syncwarp();
 #pragma unroll
-    for (int I = 0; I < 3; ++I)
+    for (int I = 0; I < NB; ++I)
 #pragma unroll
       for (int J = 0; J <= I; ++J)
 #pragma unroll
         for (int t = 0; t < 2; ++t) {
-          const int i = 8 * I + mq, j = 8 * J + 2 * kq + t;
-          if (I < nb && i < pa && j <= i)
-            A[i * (i + 1) / 2 + j] = side ? cR[I * (I + 1) / 2 + J][t] : cL[I * (I + 1) / 2 + J][t];
+          const int i = 8 * I + mq(), j = 8 * J + 2 * kq() + t;
+          if (i < pa && j <= i)
+            A()[i * (i + 1) / 2 + j] = side ? cR[I * (I + 1) / 2 + J][t] : cL[I * (I + 1) / 2 + J][t];
         }
     __syncwarp();
     double lam;
-    if (warp_ridge_solve(A, z_, p, ridge, lam)) {
+    if (warp_ridge_solve(A(), z_, p, ridge, lam)) {
       ok = false;
       continue;
     }
-    double* beta = side ? br : bl;
+    double* beta = side ? br() : bl();
     for (int i = lane; i < p; i += 32) beta[i] = z_[i];
     if (side) lamR = lam; else lamL = lam;
   }
@@ -1693,19 +1693,20 @@ __device__ bool SplitWarp::solve_sides(const double (&cL)[6][2], const double (&
 // Side Grams at theta = (w, w[d]) over all rows.  Soft: gates with the
 // weight floor; hard: exact sides (weights 1 / 0) and the right-side count,
 // the Gram skipped when a side is below req or `accumulate` is off.
-__device__ void SplitWarp::gram_pass(const double* w, bool hard, int req, bool accumulate, double (&cL)[6][2],
-                                     double (&cR)[6][2]) {
+template <int NB>
+__device__ void SplitWarp<NB>::gram_pass(const double* w, bool hard, int req, bool accumulate,
+                                         double (&cL)[NBLK][2], double (&cR)[NBLK][2]) {
   const double z = w[d];
-  double b[kWMaxK];
+  double b[NK];
   score_operand(w, b);
 #pragma unroll
-  for (int q = 0; q < 6; ++q) cL[q][0] = cL[q][1] = cR[q][0] = cR[q][1] = 0.0;
+  for (int q = 0; q < NBLK; ++q) cL[q][0] = cL[q][1] = cR[q][0] = cR[q][1] = 0.0;
   int cnt = 0;
   if (hard) {  // count first: the Grams are needed only when both sides are large enough
     for (int64_t t0 = 0; t0 < n; t0 += kWTile) {
       double yv;
       const int rows = load_tile(t0, yv);
-      if (lane < rows) cnt += right_side(psi + lane * ps + xcol, w, d, z) ? 1 : 0;
+      if (lane < rows) cnt += right_side(psi() + lane * ps + xcol, w, d, z) ? 1 : 0;
     }
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
     nright = cnt;
@@ -1717,38 +1718,41 @@ __device__ void SplitWarp::gram_pass(const double* w, bool hard, int req, bool a
     double qL = 0.0, qR = 0.0;
     if (hard) {
       if (lane < rows) {
-        const bool right = right_side(psi + lane * ps + xcol, w, d, z);
+        const bool right = right_side(psi() + lane * ps + xcol, w, d, z);
         qL = right ? 0.0 : 1.0;
         qR = right ? 1.0 : 0.0;
       }
     } else {
       double u, fl, fr;
-      scores(rows, b, u, fl, fr);
+      scores(b, u, fl, fr);
       if (lane < rows) {
         const double pi = gate((u - z) * invT);
         qL = fmax(1.0 - pi, a.prm.weight_floor);
         qR = fmax(pi, a.prm.weight_floor);
       }
     }
-    gram_tile(rows, qL, qR, cL, cR);
+    gram_tile(qL, qR, cL, cR);
   }
 }
 
 // Soft residual pass at theta with the current child models: loss,
 // gradient, n_right (pi >= 0.5), then the projected gradient, its norm and
 // the directional derivative.
-__device__ void SplitWarp::resid_pass() {
-  const double z = th[d];
+template <int NB>
+__device__ void SplitWarp<NB>::resid_pass() {
+  const double z = th()[d];
   const double inv_n = 1.0 / (double)n;
-  double b[kWMaxK];
-  score_operand(th, b);
-  double g[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+  double b[NK];
+  score_operand(th(), b);
+  double g[NB][2];
+#pragma unroll
+  for (int I = 0; I < NB; ++I) g[I][0] = g[I][1] = 0.0;
   double sl = 0.0, sa = 0.0, snr = 0.0;
   for (int64_t t0 = 0; t0 < n; t0 += kWTile) {
     double yv;
     const int rows = load_tile(t0, yv);
     double u, fl, fr;
-    scores(rows, b, u, fl, fr);
+    scores(b, u, fl, fr);
     double c = 0.0;
     if (lane < rows) {
       const double pi = gate((u - z) * invT);
@@ -1759,60 +1763,61 @@ __device__ void SplitWarp::resid_pass() {
       sa += c;
       snr += pi >= 0.5 ? 1.0 : 0.0;
     }
-    grad_tile(rows, c, g);
+    grad_tile(c, g);
   }
   // psi column 8 I + m of the gradient sits in lane (k = 0, m), block I
   __syncwarp();
-  if (kq == 0) {
+  if (kq() == 0) {
 #pragma unroll
-    for (int I = 0; I < 3; ++I) {
-      const int col = 8 * I + mq - xcol;
-      if (I < nb && col >= 0 && col < d) gr[col] = g[I][0] / T;
+    for (int I = 0; I < NB; ++I) {
+      const int col = 8 * I + mq() - xcol;
+      if (col >= 0 && col < d) gr()[col] = g[I][0] / T;
     }
   }
   const double tot_l = wbcast_sum(sl), tot_a = wbcast_sum(sa), tot_nr = wbcast_sum(snr);
-  if (lane == 0) gr[d] = -tot_a / T;
+  if (lane == 0) gr()[d] = -tot_a / T;
   __syncwarp();
   loss = tot_l / (double)n;
   nright = (int)tot_nr;
   // projected gradient and its norm (splitters.py:86-98), evaluated by every
   // lane in the same order
-  const double* w = th;
+  const double* w = th();
   double gw = 0.0, nrm2 = 0.0;
-  for (int i = 0; i < d; ++i) gw += gr[i] * w[i];
+  for (int i = 0; i < d; ++i) gw += gr()[i] * w[i];
   for (int i = 0; i < d; ++i) {
-    const double pg = gr[i] - gw * w[i];
+    const double pg = gr()[i] - gw * w[i];
     nrm2 += pg * pg;
   }
-  nrm2 += gr[d] * gr[d];
+  nrm2 += gr()[d] * gr()[d];
   __syncwarp();
   if (lane == 0) {
-    for (int i = 0; i < d; ++i) dn[i] = -(gr[i] - gw * w[i]);
-    dn[d] = -gr[d];
+    for (int i = 0; i < d; ++i) dn()[i] = -(gr()[i] - gw * w[i]);
+    dn()[d] = -gr()[d];
   }
   __syncwarp();
   gnorm = sqrt(nrm2);
   double s = 0.0;
-  for (int i = 0; i <= d; ++i) s += gr[i] * dn[i];
+  for (int i = 0; i <= d; ++i) s += gr()[i] * dn()[i];
   dd = s;
 }
 
 // One Armijo candidate theta_c (in tc): its frozen-model loss at the current
 // temperature (objectives.py:145-156), and the side Grams at theta_c with the
 // gates at invT_next, the temperature that follows an accepted step.
-__device__ double SplitWarp::trial_gram_pass(double invT_next, double (&cL)[6][2], double (&cR)[6][2]) {
-  const double z = tc[d];
-  double b[kWMaxK];
-  score_operand(tc, b);
+template <int NB>
+__device__ double SplitWarp<NB>::trial_gram_pass(double invT_next, double (&cL)[NBLK][2], double (&cR)[NBLK][2]) {
+  const double z = tc()[d];
+  double b[NK];
+  score_operand(tc(), b);
 #pragma unroll
-  for (int q = 0; q < 6; ++q) cL[q][0] = cL[q][1] = cR[q][0] = cR[q][1] = 0.0;
+  for (int q = 0; q < NBLK; ++q) cL[q][0] = cL[q][1] = cR[q][0] = cR[q][1] = 0.0;
   const bool same_t = invT_next == invT;
   double sl = 0.0;
   for (int64_t t0 = 0; t0 < n; t0 += kWTile) {
     double yv;
     const int rows = load_tile(t0, yv);
     double u, fl, fr;
-    scores(rows, b, u, fl, fr);
+    scores(b, u, fl, fr);
     double qL = 0.0, qR = 0.0;
     if (lane < rows) {
       const double pi = gate((u - z) * invT);
@@ -1822,24 +1827,25 @@ __device__ double SplitWarp::trial_gram_pass(double invT_next, double (&cL)[6][2
       qL = fmax(1.0 - pn, a.prm.weight_floor);
       qR = fmax(pn, a.prm.weight_floor);
     }
-    gram_tile(rows, qL, qR, cL, cR);
+    gram_tile(qL, qR, cL, cR);
   }
   return wbcast_sum(sl) / (double)n;
 }
 
 // Hard losses: mean squared residual of each side's hard model.
-__device__ void SplitWarp::hard_losses() {
-  const double z = th[d];
-  double b[kWMaxK];
-  score_operand(th, b);
+template <int NB>
+__device__ void SplitWarp<NB>::hard_losses() {
+  const double z = th()[d];
+  double b[NK];
+  score_operand(th(), b);
   double sL = 0.0, sR = 0.0;
   for (int64_t t0 = 0; t0 < n; t0 += kWTile) {
     double yv;
     const int rows = load_tile(t0, yv);
     double u, fl, fr;
-    scores(rows, b, u, fl, fr);
+    scores(b, u, fl, fr);
     if (lane < rows) {
-      const bool right = right_side(psi + lane * ps + xcol, th, d, z);
+      const bool right = right_side(psi() + lane * ps + xcol, th(), d, z);
       const double e = yv - (right ? fr : fl);
       (right ? sR : sL) += e * e;
     }
@@ -1851,7 +1857,8 @@ __device__ void SplitWarp::hard_losses() {
   loss = (double)nl / n * hlossL + (double)nright / n * hlossR;
 }
 
-__device__ void SplitWarp::run(int item) {
+template <int NB>
+__device__ void SplitWarp<NB>::run(int item) {
   const ArtSplitParams& P = a.prm;
   k = item / a.R;
   kr = (int64_t)item;  // items are k * R + restart
@@ -1864,8 +1871,6 @@ __device__ void SplitWarp::run(int item) {
   pa = p + 1;
   E = pa * (pa + 1) / 2;
   xcol = x_column(kind);
-  nb = (pa + 7) >> 3;
-  nk = (p + 3) >> 2;
   T0 = a.temperature[k];
   ridge = a.ridge[k];
   const int req = max(a.min_side ? max(1, a.min_side[k]) : P.min_side_points,
@@ -1873,15 +1878,13 @@ __device__ void SplitWarp::run(int item) {
   const bool fb_allowed = a.fallback ? a.fallback[k] != 0 : false;
   const int M = P.max_iters;
   aff = kind == ART_FEATURES_AFFINE;
-  xt = aff ? psi : xt0;
-  xs = aff ? ps : xs0;
   __syncwarp();
-  for (int i = lane; i < kWTile * ps; i += 32) psi[i] = 0.0;  // columns past pa stay zero
+  for (int i = lane; i < kWTile * ps; i += 32) psi()[i] = 0.0;  // columns past pa stay zero
   for (int f = lane; f < p; f += 32) {
     int ia, ib;
     feature_factors(d, kind, f, ia, ib);
-    fidx[2 * f] = (int16_t)ia;
-    fidx[2 * f + 1] = (int16_t)ib;
+    fidx()[2 * f] = (int16_t)ia;
+    fidx()[2 * f + 1] = (int16_t)ib;
   }
   // initial theta: projected theta0 (splitters.py:379)
   const double* t0 = a.theta0 + kr * a.theta0_stride;
@@ -1891,8 +1894,8 @@ __device__ void SplitWarp::run(int item) {
   active = true;
   fail = 0;
   if (!(nrm > 1e-12) || !isfinite(nrm)) { active = false; fail = ART_SPLIT_INVALID; }
-  for (int i = lane; i < d; i += 32) th[i] = t0[i] / nrm;
-  if (lane == 0) th[d] = t0[d];
+  for (int i = lane; i < d; i += 32) th()[i] = t0[i] / nrm;
+  if (lane == 0) th()[d] = t0[d];
   __syncwarp();
   T = T0;
   invT = 1.0 / T0;
@@ -1915,11 +1918,11 @@ __device__ void SplitWarp::run(int item) {
       hasfeas = true;
       feasit = it_;
       __syncwarp();
-      for (int i = lane; i <= d; i += 32) lf[i] = th[i];
+      for (int i = lane; i <= d; i += 32) lf()[i] = th()[i];
       __syncwarp();
     }
   };
-  double cL[6][2], cR[6][2];
+  double cL[NBLK][2], cR[NBLK][2];
   // evaluate(theta): child fits from the Grams, then the residual pass
   auto fit_and_resid = [&]() {
     if (!solve_sides(cL, cR)) {
@@ -1930,7 +1933,7 @@ __device__ void SplitWarp::run(int item) {
     resid_pass();
   };
   if (active) {
-    gram_pass(th, false, 0, true, cL, cR);
+    gram_pass(th(), false, 0, true, cL, cR);
     fit_and_resid();
     if (active) {
       tol = P.grad_atol + P.grad_rtol * gnorm;
@@ -1960,12 +1963,12 @@ __device__ void SplitWarp::run(int item) {
       if (lane == 0) {
         double s2 = 0.0;
         for (int i = 0; i < d; ++i) {
-          const double v = th[i] + a_ * dn[i];
+          const double v = th()[i] + a_ * dn()[i];
           s2 += v * v;
         }
         const double nw = sqrt(s2);
-        for (int i = 0; i < d; ++i) tc[i] = (th[i] + a_ * dn[i]) / nw;
-        tc[d] = th[d] + a_ * dn[d];
+        for (int i = 0; i < d; ++i) tc()[i] = (th()[i] + a_ * dn()[i]) / nw;
+        tc()[d] = th()[d] + a_ * dn()[d];
       }
       __syncwarp();
       const double fv = trial_gram_pass(invT_next, cL, cR);
@@ -2008,7 +2011,7 @@ __device__ void SplitWarp::run(int item) {
     }
     // commit theta <- theta_c, then the new temperature
     __syncwarp();
-    for (int i = lane; i <= d; i += 32) th[i] = tc[i];
+    for (int i = lane; i <= d; i += 32) th()[i] = tc()[i];
     __syncwarp();
     T = T_next;
     invT = invT_next;
@@ -2028,19 +2031,19 @@ __device__ void SplitWarp::run(int item) {
     const bool final_ok = min(nright, (int)n - nright) >= req;
     __syncwarp();
     if (!final_ok && fb_allowed && hasfeas) {
-      for (int i = lane; i <= d; i += 32) th[i] = lf[i];
+      for (int i = lane; i <= d; i += 32) th()[i] = lf()[i];
       fbk = true;
     }
     __syncwarp();
     double s2 = 0.0;
-    for (int i = 0; i < d; ++i) s2 += th[i] * th[i];
+    for (int i = 0; i < d; ++i) s2 += th()[i] * th()[i];
     const double nw = sqrt(s2);
     __syncwarp();
     if (lane == 0)
-      for (int i = 0; i < d; ++i) th[i] = th[i] / nw;
+      for (int i = 0; i < d; ++i) th()[i] = th()[i] / nw;
     __syncwarp();
     // hard partition: exact sides and right count; hard child fits when asked
-    gram_pass(th, true, req, P.hard_refit != 0, cL, cR);
+    gram_pass(th(), true, req, P.hard_refit != 0, cL, cR);
     if (nright < req || (int)n - nright < req) {
       fail = ART_SPLIT_MIN_SIDE_POINTS;
     } else if (P.hard_refit) {
@@ -2052,7 +2055,7 @@ __device__ void SplitWarp::run(int item) {
   __syncwarp();
   if (lane == 0) {
     const int dts = a.dmax + 1;
-    for (int i = 0; i <= d; ++i) a.r_theta[kr * dts + i] = th[i];
+    for (int i = 0; i <= d; ++i) a.r_theta[kr * dts + i] = th()[i];
     a.r_fail[kr] = fail;
     a.r_stop[kr] = stop;
     a.r_iters[kr] = iters;
@@ -2068,18 +2071,21 @@ __device__ void SplitWarp::run(int item) {
     a.r_ridge[kr * 2] = lamL;
     a.r_ridge[kr * 2 + 1] = lamR;
     for (int f = 0; f < p; ++f) {
-      a.r_beta[(kr * 2) * a.pmax + f] = have ? bl[f] : nan;
-      a.r_beta[(kr * 2 + 1) * a.pmax + f] = have ? br[f] : nan;
+      a.r_beta[(kr * 2) * a.pmax + f] = have ? bl()[f] : nan;
+      a.r_beta[(kr * 2 + 1) * a.pmax + f] = have ? br()[f] : nan;
     }
   }
   __syncwarp();
 }
 
-// MINB = 2: two 8-warp CTAs per SM (a 128-register cap)
-__global__ void __launch_bounds__(kWThreads, 2) split_warp_kernel(SplitArgs a) {
+// Resident 4-warp CTAs per SM: 4 (16 warps, a 128-register cap) for up to
+// two blocks; 3 (12 warps, 168 registers) for three, whose six Gram blocks
+// per side would spill under the tighter cap.
+template <int NB>
+__global__ void __launch_bounds__(kWThreads, NB == 3 ? 3 : 4) split_warp_kernel(SplitArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  SplitWarp W(a, smem, warp);
+  SplitWarp<NB> W(a, smem, warp);
   const int count = a.counts[0];
   for (;;) {
     int q = 0;
@@ -2508,20 +2514,27 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
   count_launch(); count_launch(); count_launch();
   if (use_warp) {
     const size_t wsm = warp_layout(a.dmax, a.pmax).total;
-    if (cudaFuncSetAttribute(split_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm) !=
-        cudaSuccess) {
-      cudaGetLastError();
-      set_error("art_split_level: cannot reserve %zu bytes of shared memory", wsm);
-      return ART_E_UNSUPPORTED;
-    }
-    const int occ = resident_ctas((const void*)split_warp_kernel, kWThreads, wsm);
-    const int64_t resident = (int64_t)device_sm_count() * std::max(occ, 1);
-    const int64_t grid = std::min<int64_t>(resident, (K * R + kWWarps - 1) / kWWarps);
-    prof_begin("split_level", s);
-    split_warp_kernel<<<(unsigned)std::max<int64_t>(grid, 1), kWThreads, wsm, s>>>(a);
-    prof_end(s);
-    count_launch();
-    if (int rc = check_launch("split_level")) return rc;
+    auto launch_warp = [&](auto kern) -> int {
+      if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("art_split_level: cannot reserve %zu bytes of shared memory", wsm);
+        return ART_E_UNSUPPORTED;
+      }
+      const int occ = resident_ctas((const void*)kern, kWThreads, wsm);
+      const int64_t resident = (int64_t)device_sm_count() * std::max(occ, 1);
+      const int64_t grid = std::min<int64_t>(resident, (K * R + kWWarps - 1) / kWWarps);
+      prof_begin("split_level", s);
+      kern<<<(unsigned)std::max<int64_t>(grid, 1), kWThreads, wsm, s>>>(a);
+      prof_end(s);
+      count_launch();
+      return check_launch("split_level");
+    };
+    const int nbk = (a.pmax + 1 + 7) / 8;  // 8-column blocks of the widest psi
+    int rcw;
+    if (nbk == 1) rcw = launch_warp(split_warp_kernel<1>);
+    else if (nbk == 2) rcw = launch_warp(split_warp_kernel<2>);
+    else rcw = launch_warp(split_warp_kernel<3>);
+    if (rcw) return rcw;
     prof_begin("split_select", s);
     split_select<<<(unsigned)((K + 127) / 128), 128, 0, s>>>(a, *out);
     prof_end(s);
