@@ -22,7 +22,7 @@ Results live in an in-process table keyed by the device (name, SM count,
 compute capability), persisted as JSON at ``$ART_AUTOTUNE_CACHE`` when that
 is set.  Lookups (``cached_*``) read only host-known keys, never device
 data, so they add no synchronisation to a call; an untuned key returns the
-library default (0).  Tuning itself synchronises and is meant for warm-up.
+library default.  Tuning itself synchronises and is meant for warm-up.
 """
 
 from __future__ import annotations
@@ -120,15 +120,16 @@ def cached_ridge_threshold(dims=None, features=None, row_offsets=None, fp64_fact
 
 def cached_split_shape(d: int, p: int, R: int) -> tuple[int, int, int, int]:
     """Tuned (group_restarts, trial_steps, ctas_per_sm, restart_warps) for a
-    (d, p, R) level, or (0, 0, 0, 0)."""
+    (d, p, R) level; untuned: (0, 0, 0, 1), the warp-per-restart form (the
+    library takes the CTA form where the level does not fit it)."""
 
     _load()
     try:
         entry = _TABLE.get(_split_key(d, p, R))
     except RuntimeError:
-        return 0, 0, 0, 0
+        return 0, 0, 0, 1
     if not entry:
-        return 0, 0, 0, 0
+        return 0, 0, 0, 1
     return (int(entry["group_restarts"]), int(entry["trial_steps"]), int(entry.get("ctas_per_sm", 0)),
             int(entry.get("restart_warps", 0)))
 

@@ -1461,6 +1461,7 @@ constexpr int kWTile = 32;                                   // rows per tile
 constexpr int kWMaxPa = 24;                                  // p + 1 (augmented with y)
 constexpr int kWMaxD = 23;                                   // inputs
 constexpr int kWThreads = 128;                               // 4 warps per CTA
+constexpr int kWGangLog = 12;                                // gang items: n + 1 >= 2^12 rows
 constexpr int kWWarps = kWThreads / 32;
 
 // Per-warp shared memory (doubles): psi | cf | sc | tc | th | dn | gr | lf |
@@ -1478,6 +1479,13 @@ __host__ __device__ inline WLayout warp_layout(int dmax, int pmax) {
   L.per_warp = (size_t)kWTile * L.ps + 5 * kWTile + 5 * dt + 2 * pmax + E + 2 * pa + pa + kWTile * L.xs;
   L.total = (size_t)kWWarps * L.per_warp * 8;
   return L;
+}
+
+// A node of n rows is split by the whole CTA (its warps sharing the tiles)
+// when n + 1 >= 2^kWGangLog: on the plan's size buckets, so every gang item
+// precedes every other item in the work list.
+__device__ __forceinline__ bool warp_gang_item(int64_t n) {
+  return ilogb((double)(n + 1)) >= kWGangLog;
 }
 
 __device__ __forceinline__ double wbcast_sum(double v) {
@@ -1532,9 +1540,36 @@ struct SplitWarp {
   int nright = 0, iters = 0, stop = 0, fail = 0, feasit = -1;
   bool active = false, hasfeas = false, conv = false, fbk = false;
 
+  // gang: the CTA's warps share one large item, warp grank taking tiles
+  // grank, grank + gsize, ...; every pass ends with the partial sums of all
+  // members added in member order, so each member holds the same totals and
+  // runs the same control flow
+  int grank = 0, gsize = 1;
+  size_t pw;  // doubles per warp region
+
   __device__ SplitWarp(const SplitArgs& a_, unsigned char* sm, int warp) : a(a_) {
-    base = (double*)sm + (size_t)warp * warp_layout(a.dmax, a.pmax).per_warp;
+    pw = warp_layout(a.dmax, a.pmax).per_warp;
+    base = (double*)sm + (size_t)warp * pw;
     lane = threadIdx.x & 31;
+  }
+  __device__ int64_t tile0() const { return (int64_t)grank * kWTile; }
+  __device__ int64_t tstep() const { return (int64_t)gsize * kWTile; }
+  __device__ void gang_bar() const { asm volatile("bar.sync 1, %0;" ::"r"(kWThreads) : "memory"); }
+  // Gang sums of per-lane partials: each member stores its partials in
+  // slots of its psi region (free between passes), a barrier, then every
+  // member adds slot c of all members in member order (gang_end restores
+  // psi's zero padding after the second barrier).
+  __device__ void gput(int c, double v) const { base[c * kWTile + lane] = v; }
+  __device__ double gsum(int c) const {
+    const double* b0 = base - (size_t)grank * pw;
+    double t = b0[c * kWTile + lane];
+    for (int g = 1; g < gsize; ++g) t += b0[(size_t)g * pw + c * kWTile + lane];
+    return t;
+  }
+  __device__ void gang_end() {
+    gang_bar();
+    for (int f = pa; f < ps; ++f) base[lane * ps + f] = 0.0;
+    __syncwarp();
   }
 
   // Tile rows [t0, t0 + rows): x (coalesced copy) and psi = [phi(x); y],
@@ -1650,6 +1685,23 @@ struct SplitWarp {
   __device__ double gate(double s) const { return a.mixed ? sigm32(s) : sigm(s); }
 
   __device__ void run(int item);
+  // the side Gram blocks (and one extra per-lane partial) summed over the gang
+  __device__ void gang_gram(double (&cL)[NBLK][2], double (&cR)[NBLK][2], double* extra = nullptr) {
+    static_assert(4 * NBLK + 1 <= ps, "gang slots: 32 x ps doubles of psi");
+    if (gsize == 1) return;
+#pragma unroll
+    for (int q = 0; q < NBLK; ++q) {
+      gput(4 * q, cL[q][0]); gput(4 * q + 1, cL[q][1]); gput(4 * q + 2, cR[q][0]); gput(4 * q + 3, cR[q][1]);
+    }
+    if (extra) gput(4 * NBLK, *extra);
+    gang_bar();
+#pragma unroll
+    for (int q = 0; q < NBLK; ++q) {
+      cL[q][0] = gsum(4 * q); cL[q][1] = gsum(4 * q + 1); cR[q][0] = gsum(4 * q + 2); cR[q][1] = gsum(4 * q + 3);
+    }
+    if (extra) *extra = gsum(4 * NBLK);
+    gang_end();
+  }
   __device__ bool solve_sides(const double (&cL)[NBLK][2], const double (&cR)[NBLK][2]);
   __device__ void gram_pass(const double* w, bool hard, int req, bool accumulate, double (&cL)[NBLK][2],
                             double (&cR)[NBLK][2]);
@@ -1703,16 +1755,22 @@ __device__ void SplitWarp<NB>::gram_pass(const double* w, bool hard, int req, bo
   for (int q = 0; q < NBLK; ++q) cL[q][0] = cL[q][1] = cR[q][0] = cR[q][1] = 0.0;
   int cnt = 0;
   if (hard) {  // count first: the Grams are needed only when both sides are large enough
-    for (int64_t t0 = 0; t0 < n; t0 += kWTile) {
+    for (int64_t t0 = tile0(); t0 < n; t0 += tstep()) {
       double yv;
       const int rows = load_tile(t0, yv);
       if (lane < rows) cnt += right_side(psi() + lane * ps + xcol, w, d, z) ? 1 : 0;
+    }
+    if (gsize > 1) {  // integers: exact in any order
+      gput(0, (double)cnt);
+      gang_bar();
+      cnt = (int)gsum(0);
+      gang_end();
     }
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
     nright = cnt;
     if (nright < req || (int)n - nright < req || !accumulate) return;
   }
-  for (int64_t t0 = 0; t0 < n; t0 += kWTile) {
+  for (int64_t t0 = tile0(); t0 < n; t0 += tstep()) {
     double yv;
     const int rows = load_tile(t0, yv);
     double qL = 0.0, qR = 0.0;
@@ -1733,6 +1791,7 @@ __device__ void SplitWarp<NB>::gram_pass(const double* w, bool hard, int req, bo
     }
     gram_tile(qL, qR, cL, cR);
   }
+  gang_gram(cL, cR);
 }
 
 // Soft residual pass at theta with the current child models: loss,
@@ -1748,7 +1807,7 @@ __device__ void SplitWarp<NB>::resid_pass() {
 #pragma unroll
   for (int I = 0; I < NB; ++I) g[I][0] = g[I][1] = 0.0;
   double sl = 0.0, sa = 0.0, snr = 0.0;
-  for (int64_t t0 = 0; t0 < n; t0 += kWTile) {
+  for (int64_t t0 = tile0(); t0 < n; t0 += tstep()) {
     double yv;
     const int rows = load_tile(t0, yv);
     double u, fl, fr;
@@ -1764,6 +1823,16 @@ __device__ void SplitWarp<NB>::resid_pass() {
       snr += pi >= 0.5 ? 1.0 : 0.0;
     }
     grad_tile(c, g);
+  }
+  if (gsize > 1) {
+#pragma unroll
+    for (int I = 0; I < NB; ++I) gput(I, g[I][0]);  // column 0 only is used
+    gput(NB, sl); gput(NB + 1, sa); gput(NB + 2, snr);
+    gang_bar();
+#pragma unroll
+    for (int I = 0; I < NB; ++I) g[I][0] = gsum(I);
+    sl = gsum(NB); sa = gsum(NB + 1); snr = gsum(NB + 2);
+    gang_end();
   }
   // psi column 8 I + m of the gradient sits in lane (k = 0, m), block I
   __syncwarp();
@@ -1813,7 +1882,7 @@ __device__ double SplitWarp<NB>::trial_gram_pass(double invT_next, double (&cL)[
   for (int q = 0; q < NBLK; ++q) cL[q][0] = cL[q][1] = cR[q][0] = cR[q][1] = 0.0;
   const bool same_t = invT_next == invT;
   double sl = 0.0;
-  for (int64_t t0 = 0; t0 < n; t0 += kWTile) {
+  for (int64_t t0 = tile0(); t0 < n; t0 += tstep()) {
     double yv;
     const int rows = load_tile(t0, yv);
     double u, fl, fr;
@@ -1829,6 +1898,7 @@ __device__ double SplitWarp<NB>::trial_gram_pass(double invT_next, double (&cL)[
     }
     gram_tile(qL, qR, cL, cR);
   }
+  gang_gram(cL, cR, &sl);
   return wbcast_sum(sl) / (double)n;
 }
 
@@ -1839,7 +1909,7 @@ __device__ void SplitWarp<NB>::hard_losses() {
   double b[NK];
   score_operand(th(), b);
   double sL = 0.0, sR = 0.0;
-  for (int64_t t0 = 0; t0 < n; t0 += kWTile) {
+  for (int64_t t0 = tile0(); t0 < n; t0 += tstep()) {
     double yv;
     const int rows = load_tile(t0, yv);
     double u, fl, fr;
@@ -1849,6 +1919,12 @@ __device__ void SplitWarp<NB>::hard_losses() {
       const double e = yv - (right ? fr : fl);
       (right ? sR : sL) += e * e;
     }
+  }
+  if (gsize > 1) {
+    gput(0, sL); gput(1, sR);
+    gang_bar();
+    sL = gsum(0); sR = gsum(1);
+    gang_end();
   }
   const double tl = wbcast_sum(sL), trr = wbcast_sum(sR);
   const int nl = (int)n - nright;
@@ -1909,7 +1985,7 @@ __device__ void SplitWarp<NB>::run(int item) {
   lamL = lamR = 0.0;
   if (n == 0) { active = false; fail = ART_SPLIT_MIN_SIDE_POINTS; }
   auto record_trace = [&](int iter) {
-    if (lane != 0) return;
+    if (lane != 0 || grank != 0) return;
     if (a.tr_loss) a.tr_loss[kr * (M + 1) + iter] = loss;
     if (a.tr_gnorm) a.tr_gnorm[kr * (M + 1) + iter] = gnorm;
   };
@@ -2016,7 +2092,7 @@ __device__ void SplitWarp<NB>::run(int item) {
     T = T_next;
     invT = invT_next;
     iters = iter + 1;
-    if (lane == 0) {
+    if (lane == 0 && grank == 0) {
       if (a.tr_step) a.tr_step[kr * P.max_iters + iter] = step;
       if (a.tr_back) a.tr_back[kr * P.max_iters + iter] = nb_;
     }
@@ -2053,7 +2129,7 @@ __device__ void SplitWarp<NB>::run(int item) {
   }
   // ----------------------------------------------------------- write results
   __syncwarp();
-  if (lane == 0) {
+  if (lane == 0 && grank == 0) {
     const int dts = a.dmax + 1;
     for (int i = 0; i <= d; ++i) a.r_theta[kr * dts + i] = th()[i];
     a.r_fail[kr] = fail;
@@ -2084,15 +2160,43 @@ __device__ void SplitWarp<NB>::run(int item) {
 template <int NB>
 __global__ void __launch_bounds__(kWThreads, NB == 3 ? 3 : 4) split_warp_kernel(SplitArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_q;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   SplitWarp<NB> W(a, smem, warp);
   const int count = a.counts[0];
+  // Items come largest first.  While they are large the whole CTA takes one
+  // at a time (a gang of all its warps); from the first small item on, each
+  // warp pops its own, warp 0 starting with the CTA's last pop.  (One call
+  // site of run keeps it inlined and the state in registers.)
+  bool cta_phase = true;
   for (;;) {
-    int q = 0;
-    if (lane == 0) q = atomicAdd(&a.counts[1], 1);
-    q = __shfl_sync(0xffffffffu, q, 0);
-    if (q >= count) break;
-    W.run(a.items[q].x);
+    int item = -1;
+    if (cta_phase) {
+      if (threadIdx.x == 0) s_q = atomicAdd(&a.counts[1], 1);
+      __syncthreads();
+      const int q = s_q;
+      __syncthreads();
+      if (q >= count) return;
+      item = a.items[q].x;
+      const int64_t k = item / a.R;
+      if (warp_gang_item(a.row_offsets[k + 1] - a.row_offsets[k])) {
+        W.grank = warp;
+        W.gsize = kWWarps;
+      } else {
+        cta_phase = false;
+        W.grank = 0;
+        W.gsize = 1;
+        if (warp != 0) item = -1;
+      }
+    }
+    if (item < 0) {
+      int q = 0;
+      if (lane == 0) q = atomicAdd(&a.counts[1], 1);
+      q = __shfl_sync(0xffffffffu, q, 0);
+      if (q >= count) return;
+      item = a.items[q].x;
+    }
+    W.run(item);
   }
 }
 

@@ -498,7 +498,10 @@ def leg_split(args, stream):
     """Batched soft oblique split search: 4096 nodes, d = 16, n log-uniform in
     [256, 16384], 16 restarts x 60 projected-gradient steps, affine child fits
     (lambda = 1e-6), temperature annealed 0.2 -> 0.02; the plain FP64 form
-    and the mixed form (single-precision gates, FP64 sums and solves)."""
+    and the mixed form (single-precision gates, FP64 sums and solves) in the
+    tuned launch form (one warp per restart unless a CTA shape timed faster),
+    the FP64 CTA form at its best tuned shape, and the mixed CTA form with
+    the tensor-core Gram."""
 
     from art import _native as N
     from art import autotune
@@ -521,14 +524,25 @@ def leg_split(args, stream):
     out = {"metric": "split restart-steps/s", "unit": "restart-steps/s", "nodes": wl.count, "rows": wl.n_rows,
            "restarts": 16, "iterations": 60, "autotune": tuned}
     thetas = {}
-    for prec in ("fp64", "mixed", "mixed_tc"):
-        sp.precision = "mixed" if prec == "mixed_tc" else prec
-        sp.tensor_gram = prec == "mixed_tc"
+    # best CTA-form shape among the tuned candidates (keys g x h x c x w)
+    cta_shape = (4, 2, 1, 0)
+    if tuned:
+        cta = {k: v for k, v in tuned["candidates_ms"].items() if k.endswith("x0")}
+        if cta:
+            cta_shape = tuple(int(v) for v in min(cta, key=cta.get).split("x"))
+    out["cta_shape"] = list(cta_shape)
+    variants = (("fp64", "fp64", False, None), ("mixed", "mixed", False, None), ("fp64_cta", "fp64", False, cta_shape),
+                ("mixed_tc", "mixed", True, (0, 0, 0, 0)))
+    for prec, precision, tensor, shape in variants:
+        sp.precision = precision
+        sp.tensor_gram = tensor
+        kw = {} if shape is None else dict(group_restarts=shape[0], trial_steps=shape[1], ctas_per_sm=shape[2],
+                                           restart_warps=shape[3])
 
         def step():
             return split_level(sp, wl.x, wl.y, wl.row_offsets, wl.dims, wl.kinds, wl.temperature, wl.ridge,
                                theta0=wl.theta0, anneal_ratio=0.1, hard_refit=True, max_dim=wl.d,
-                               max_features=wl.d + 1, stream=stream)
+                               max_features=wl.d + 1, stream=stream, **kw)
 
         N.profile_reset()
         N.profile_enable(True)
@@ -543,7 +557,7 @@ def leg_split(args, stream):
                      "achieved_fp64_tflops": flops / (ms / 1000.0) / 1e12, "kernel": top[0],
                      "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()}}
     hbm, bf16, peak_kind = peaks()
-    for prec in ("fp64", "mixed", "mixed_tc"):
+    for prec in ("fp64", "mixed", "fp64_cta", "mixed_tc"):
         kern = out[prec]["kernels"].get("split_level")
         if kern:
             kms = kern["ms"] / max(kern["launches"], 1)
@@ -567,6 +581,7 @@ def leg_split(args, stream):
     out["value"] = out["fp64"]["value"]
     out["mixed_speedup"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
     out["mixed_tc_speedup"] = out["fp64"]["ms_per_step"] / out["mixed_tc"]["ms_per_step"]
+    out["warp_form_speedup_vs_cta_form"] = out["fp64_cta"]["ms_per_step"] / out["fp64"]["ms_per_step"]
     out["mixed_vs_fp64_hard_loss_rel_diff_median"] = float(np.median(np.abs(lb[ok] - la[ok]) / np.abs(la[ok])))
     out["mixed_same_partition_fraction"] = float(np.mean(thetas["fp64"][1] == thetas["mixed"][1]))
     return out

@@ -52,7 +52,7 @@ def test_autotune_table_persists_and_is_keyed_by_device(tmp_path, monkeypatch):
     monkeypatch.setattr(autotune, "_LOADED", False)
     autotune.clear()
     try:
-        assert autotune.cached_split_shape(16, 17, 16) == (0, 0, 0, 0)
+        assert autotune.cached_split_shape(16, 17, 16) == (0, 0, 0, 1)
         assert autotune.cached_ridge_choice() == (0, None)
         autotune._store(autotune._split_key(16, 17, 16), {"group_restarts": 8, "trial_steps": 2,
                                                                   "ctas_per_sm": 2})
@@ -64,7 +64,7 @@ def test_autotune_table_persists_and_is_keyed_by_device(tmp_path, monkeypatch):
         assert autotune.cached_split_shape(16, 17, 16) == (8, 2, 2, 0)    # reloaded from the file
         assert autotune.cached_ridge_choice() == (153, False)
         monkeypatch.setattr(autotune, "device_key", lambda: "other-device|sm132|cc9.0")
-        assert autotune.cached_split_shape(16, 17, 16) == (0, 0, 0, 0)    # another device: untuned
+        assert autotune.cached_split_shape(16, 17, 16) == (0, 0, 0, 1)    # another device: untuned
     finally:
         autotune.clear()
 

@@ -351,6 +351,53 @@ def test_gang_split_of_large_nodes_matches_oracle_and_is_batch_independent(ctas_
                                           getattr(res, name).cpu().numpy()[k], err_msg=f"{name} {k}")
 
 
+@pytest.mark.parametrize("kind,d", [(O.AFFINE, 3), (O.POLY2, 3), (O.AFFINE, 20)])
+def test_warp_gangs_match_oracle_and_are_batch_independent(kind, d):
+    """In the warp-per-restart form, nodes of at least 4,095 rows are split
+    by all warps of a CTA, which add their pass sums in warp order: each
+    restart meets the per-node oracle, and results are bit-identical whether
+    the node is split alone or in a batch.  Covers one, two and three 8-column
+    blocks of psi (d = 3 affine, d = 3 quadratic, d = 20 affine)."""
+
+    from art.splitters import level_result_to_split, split_level
+
+    rng = np.random.default_rng(31 + d + kind)
+    ns = [9000, 300, 4095, 4094]         # gang, solo, gang (the boundary), solo
+    R = 2
+    Xs = [rng.uniform(-1, 1, (n, d)) for n in ns]
+    ys = [np.sin(2 * X[:, 0]) + 0.5 * np.tanh(4 * (X[:, 1] - X[:, 2])) for X in Xs]
+    init = np.random.default_rng(5)
+    th0 = np.array([[S.initialize_theta(X, init) for _ in range(R)] for X in Xs])
+    T, lam, iters = 0.2, 1e-6, 8
+    s = splitter_for(kind, T, lam, R, iters, {"min_side_points": 1})
+    ro = np.concatenate([[0], np.cumsum(ns)])
+    K = len(ns)
+    x, y = np.concatenate([X.reshape(-1) for X in Xs]), np.concatenate(ys)
+    res = split_level(s, x, y, ro, [d] * K, [kind] * K, T, lam, parent_loss=[1.0] * K, theta0=th0,
+                      restart_warps=1, traces=True)
+    p = S.Params(max_iters=iters, n_restarts=R, min_side_points=1)
+    picks = (res.flags.cpu().numpy() >> 8) & 255
+    for k in range(K):
+        per = []
+        for r in range(R):
+            opt = S.optimize(Xs[k], ys[k], th0[k][r], T, kind, lam, p)
+            hr = S.hard_result(Xs[k], ys[k], opt["theta"], kind, lam, 1.0, p, True)
+            hr.update(opt)
+            per.append(hr)
+        ref = per[int(picks[k])]
+        assert ref["loss"] <= min(h["loss"] for h in per) * (1 + 1e-9)
+        out = level_result_to_split(s, res, k, ns[k], 1.0, True)
+        np.testing.assert_allclose(np.r_[out.w, out.z], np.r_[ref["w"], ref["z"]], rtol=1e-9, atol=1e-11)
+        assert out.n_iters == ref["n_iters"] and out.n_right == ref["n_right"]
+        np.testing.assert_allclose(out.metadata["soft_loss_history"], ref["losses"], rtol=1e-10, atol=1e-14)
+    for k in range(K):
+        alone = split_level(s, Xs[k].reshape(-1), ys[k], [0, ns[k]], [d], [kind], T, lam, parent_loss=[1.0],
+                            theta0=th0[k:k + 1], restart_warps=1)
+        for name in ("theta", "loss", "n_right", "n_iters", "beta"):
+            np.testing.assert_array_equal(getattr(alone, name).cpu().numpy()[0],
+                                          getattr(res, name).cpu().numpy()[k], err_msg=f"{name} {k}")
+
+
 def c3_nodes(seed, ns, d=16):
     """Nodes of the C3 configuration: x uniform in a random axis box inside
     [-1,1]^16 (sides U[0.25,1]*2), y = 8 Gaussian bumps (widths U(0.1,0.6),
