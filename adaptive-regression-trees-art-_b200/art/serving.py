@@ -35,6 +35,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _native as N
+from .autotune import WARP_MAX_DIM, WARP_MAX_FEATURES
 from ._device import ptr, require_cuda, stream_handle, torch
 from .models import AffineRidgeModel, segment_residuals, solve_weighted_ridge_batched
 from .splitters import SoftObliqueSplitter, split_level
@@ -325,12 +326,16 @@ class ServingEngine:
                 split_idx.append(k)
         # max_iters is a per-call parameter of the split search (one call per
         # distinct value); the minimum side count goes per node, so nodes of
-        # every dimension share a launch.  A node's split never depends on the
-        # jobs it is batched with.
-        groups: dict[int, list[int]] = {}
+        # every dimension share a launch.  Jobs whose models fit the
+        # warp-per-restart form (d and p at most 23) and the others go to
+        # separate launches, since the form of a launch follows its widest
+        # node: so a node's split never depends on the jobs it is batched with.
+        groups: dict[tuple[int, bool], list[int]] = {}
         for k in split_idx:
-            groups.setdefault(work[k][0].job.max_iters, []).append(k)
-        for iters, ks in sorted(groups.items()):
+            job = work[k][0].job
+            warp = job.dim <= WARP_MAX_DIM and job.n_features <= WARP_MAX_FEATURES
+            groups.setdefault((job.max_iters, warp), []).append(k)
+        for (iters, _), ks in sorted(groups.items()):
             self._split([work[k] for k in ks], x, y, ro, xo, d, kinds, ks, iters)
 
     def _split(self, sub, x, y, ro, xo, d, kinds, idx, iters) -> None:
