@@ -36,6 +36,8 @@ import numpy as np
 
 from . import _native as N
 from .autotune import WARP_MAX_DIM, WARP_MAX_FEATURES
+
+WARP_MAX_ROWS = 1 << 16  # split nodes up to this size take the warp-per-restart form
 from ._device import ptr, require_cuda, stream_handle, torch
 from .models import AffineRidgeModel, segment_residuals, solve_weighted_ridge_batched
 from .splitters import SoftObliqueSplitter, split_level
@@ -326,19 +328,21 @@ class ServingEngine:
                 split_idx.append(k)
         # max_iters is a per-call parameter of the split search (one call per
         # distinct value); the minimum side count goes per node, so nodes of
-        # every dimension share a launch.  Jobs whose models fit the
-        # warp-per-restart form (d and p at most 23) and the others go to
-        # separate launches, since the form of a launch follows its widest
-        # node: so a node's split never depends on the jobs it is batched with.
+        # every dimension share a launch.  Nodes for the warp-per-restart form
+        # (d and p at most 23, at most WARP_MAX_ROWS rows: larger nodes take
+        # the CTA form, whose gangs span many SMs) and the others go to
+        # separate launches, since the form of a launch is one for all its
+        # nodes: so a node's split never depends on the nodes batched with it.
         groups: dict[tuple[int, bool], list[int]] = {}
         for k in split_idx:
             job = work[k][0].job
-            warp = job.dim <= WARP_MAX_DIM and job.n_features <= WARP_MAX_FEATURES
+            warp = (job.dim <= WARP_MAX_DIM and job.n_features <= WARP_MAX_FEATURES
+                    and ro[k + 1] - ro[k] <= WARP_MAX_ROWS)
             groups.setdefault((job.max_iters, warp), []).append(k)
-        for (iters, _), ks in sorted(groups.items()):
-            self._split([work[k] for k in ks], x, y, ro, xo, d, kinds, ks, iters)
+        for (iters, warp), ks in sorted(groups.items()):
+            self._split([work[k] for k in ks], x, y, ro, xo, d, kinds, ks, iters, warp)
 
-    def _split(self, sub, x, y, ro, xo, d, kinds, idx, iters) -> None:
+    def _split(self, sub, x, y, ro, xo, d, kinds, idx, iters, warp) -> None:
         t = torch()
         dev = x.device
         # the split nodes' rows, gathered from the fit batch
@@ -358,7 +362,7 @@ class ServingEngine:
         res = split_level(sp, xs, ys, sro, dd, kinds[idx], temps, ridge, x_offsets=sxo, hard_refit=False,
                           node_keys=keys, max_dim=int(dd.max()), max_features=int(max(st.job.n_features for st, _ in sub)),
                           min_side_points=min_side, group_restarts=0, trial_steps=0, ctas_per_sm=0,
-                          stream=self.stream)
+                          restart_warps=int(warp), stream=self.stream)
         failure = res.failure.cpu().numpy()
         theta = res.theta
         ok = failure == 0
