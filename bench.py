@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--split-nodes", type=int, default=4096)
     ap.add_argument("--har-chains", type=int, default=16384)
     ap.add_argument("--tree-builds", type=int, default=2)
+    ap.add_argument("--tree-cohort", type=int, default=256,
+                    help="BFS cohort size (node_batch_size) of both tree-build forms")
     ap.add_argument("--serve-jobs", type=int, default=2000)
     ap.add_argument("--serve-seconds", type=float, default=30.0,
                     help="admission window of the serving stream (seconds of wall clock)")
@@ -671,10 +673,11 @@ def leg_tree(args, stream):
     iterations), affine leaves (lambda = 1e-6), children topped up by
     hit-and-run with device Philox draws, then 2 refinement rounds of 1024
     new points in the 4 leaves of largest fit error.  Two GPU forms with the
-    same random stream (so the same tree): the level-batched build (one split
-    launch, one top-up launch and one mixed-form fit with FP64 refinement per
-    cohort, CUDA graphs) against the plain FP64 per-node build (one split
-    call, one top-up and one FP64 fit per node); held-out RMSE of each on
+    same random stream and the same BFS cohorts of up to ``--tree-cohort``
+    nodes (so the same tree): the level-batched build (one split launch, one
+    top-up launch and one mixed-form fit with FP64 refinement per cohort, CUDA
+    graphs) against the plain FP64 per-node build (one split call, one top-up
+    and one FP64 fit per node); held-out RMSE of each on
     20,000 uniform points.  The CPU baseline is the oracle's depth-first
     build (the reference's trees) with the same refinement driver."""
 
@@ -697,6 +700,7 @@ def leg_tree(args, stream):
                                   batched_fits=batched, cohort_top_up=batched, cuda_graphs=batched,
                                   fit_precision="mixed" if batched else "fp64", isotropic_sampling=False,
                                   refinement_rounds=2, refinement_points=1024, refinement_leaves=4,
+                                  node_batch_size=args.tree_cohort,
                                   sampler=HitAndRunSampler(burn_in=0, thinning=5, rng_mode="device"))
         return b.build()
 
@@ -730,10 +734,11 @@ def leg_tree(args, stream):
     out["heldout_rmse_rel_diff"] = abs(a - b) / max(abs(b), 1e-300)
     ids = [[n.node_id for n in trees[k].tree.iter_nodes()] for k in trees]
     out["same_tree"] = ids[0] == ids[1]
+    out["cohort"] = args.tree_cohort
     out["roofline"] = {"bound": "latency", "kernel": out["level_batched_mixed"]["top_kernel"]["name"],
                        "gpu_busy_fraction": out["level_batched_mixed"]["gpu_busy_fraction"],
-                       "note": "a 2-d tree of ~100 nodes of 4,096 rows: kernel time is a small part of the "
-                               "wall time; host policy, oracle calls and launches dominate"}
+                       "note": "hit-and-run top-ups are one chain per child, about 10^4 dependent steps each, so "
+                               "a top-up launch lasts as long as its longest chain whatever the cohort size"}
     if not args.no_cpu:
         rate, cores, sample, _ = cpu_tree_rate(f, refinement_rounds=2, refinement_points=1024,
                                                refinement_leaves=4)
