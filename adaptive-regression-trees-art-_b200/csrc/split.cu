@@ -1526,13 +1526,14 @@ struct SplitWarp {
   // the x tile: its own buffer, or for affine features psi itself
   __device__ double* xt() const {
     return aff ? base : (double*)fidx() + (a.pmax + 1);
-  }
-  __device__ int xs() const { return aff ? ps : (a.dmax | 1); }
+  }  __device__ int xs() const { return aff ? ps : (a.dmax | 1); }
   __device__ int kq() const { return lane & 3; }   // fragment coordinates of this lane
   __device__ int mq() const { return lane >> 2; }
   // item
   int64_t k, r0, n, xoff, kr;
   int d, kind, p, pa, E, xcol;
+  int tail, nks, nbx;  // columns of the last block row; score steps and gradient blocks holding data
+  bool narrow;         // tail <= 4: the tail rows of both sides in one MMA per block column
   double ridge, T0;
   // restart state (uniform)
   double loss = 0, dd = 0, tol = 0, gnorm = 0, T = 0, invT = 0, alpha = 0, lamL = 0, lamR = 0;
@@ -1628,7 +1629,8 @@ struct SplitWarp {
       double c[2] = {0.0, 0.0};
       const double* pr = psi() + (8 * rb + mq()) * ps + kq();
 #pragma unroll
-      for (int s = 0; s < NK; ++s) dmma_884(c, pr[4 * s], b[s]);
+      for (int s = 0; s < NK; ++s)
+        if (s < NK - 1 || nks == NK) dmma_884(c, pr[4 * s], b[s]);  // the last step may be all padding
       if (kq() == 0) { sc()[8 * rb + mq()] = c[0]; sc()[kWTile + 8 * rb + mq()] = c[1]; }
       else if (kq() == 1) sc()[2 * kWTile + 8 * rb + mq()] = c[0];
     }
@@ -1642,10 +1644,47 @@ struct SplitWarp {
   // G_side += (q_side psi)^T psi over the tile (lower 8 x 8 blocks), the
   // weights staged in cf.  Rows past the tile's end are zero rows.
   static constexpr int NBLK = NB * (NB + 1) / 2;  // lower-triangular 8 x 8 blocks
+  //
+  // Narrow tail (the item's last block row holds tail <= 4 columns, or none):
+  // the blocks of the first NB - 1 block rows as above, then the tail rows of
+  // both sides in one MMA per block column: A = psi block J, B = [q_L psi_T,
+  // q_R psi_T] (columns n < tail: left side, tail <= n < 2 tail: right), so
+  // D[m][n] = G_side[T + n'][8 J + m] with T = 8 (NB - 1).  The results sit in
+  // cL's last block row; cR's stays zero.
   __device__ void gram_tile(double qL, double qR, double (&cL)[NBLK][2], double (&cR)[NBLK][2]) {
     cf()[lane] = qL;
     cf()[kWTile + lane] = qR;
     __syncwarp();
+    if (narrow) {
+      constexpr int T = 8 * (NB - 1);
+      const int tcol = mq() < tail ? mq() : mq() - tail;
+      const bool tl = tail > 0 && mq() < 2 * tail;
+#pragma unroll 2
+      for (int k0 = 0; k0 < kWTile; k0 += 4) {
+        const int row = k0 + kq();
+        const double* pr = psi() + row * ps + mq();
+        const double ql = cf()[row], qr = cf()[kWTile + row];
+        double v[NB];
+#pragma unroll
+        for (int I = 0; I < NB; ++I) v[I] = pr[8 * I];
+#pragma unroll
+        for (int I = 0; I < NB - 1; ++I) {
+          const double aL = ql * v[I], aR = qr * v[I];
+#pragma unroll
+          for (int J = 0; J <= I; ++J) {
+            dmma_884(cL[I * (I + 1) / 2 + J], aL, v[J]);
+            dmma_884(cR[I * (I + 1) / 2 + J], aR, v[J]);
+          }
+        }
+        if (tail > 0) {  // warp-uniform
+          const double bt = tl ? (mq() < tail ? ql : qr) * psi()[row * ps + T + tcol] : 0.0;
+#pragma unroll
+          for (int J = 0; J < NB; ++J) dmma_884(cL[(NB - 1) * NB / 2 + J], v[J], bt);
+        }
+      }
+      __syncwarp();
+      return;
+    }
 #pragma unroll 2
     for (int k0 = 0; k0 < kWTile; k0 += 4) {
       const int row = k0 + kq();
@@ -1677,7 +1716,8 @@ struct SplitWarp {
       const double* pr = psi() + row * ps + mq();
       const double b = mq() == 0 ? cf()[row] : 0.0;
 #pragma unroll
-      for (int I = 0; I < NB; ++I) dmma_884(g[I], pr[8 * I], b);
+      for (int I = 0; I < NB; ++I)
+        if (I < NB - 1 || nbx == NB) dmma_884(g[I], pr[8 * I], b);  // blocks holding x columns
     }
     __syncwarp();
   }
@@ -1725,9 +1765,23 @@ __device__ bool SplitWarp<NB>::solve_sides(const double (&cL)[NBLK][2], const do
 #pragma unroll
         for (int t = 0; t < 2; ++t) {
           const int i = 8 * I + mq(), j = 8 * J + 2 * kq() + t;
-          if (i < pa && j <= i)
+          if ((!narrow || I < NB - 1) && i < pa && j <= i)
             A()[i * (i + 1) / 2 + j] = side ? cR[I * (I + 1) / 2 + J][t] : cL[I * (I + 1) / 2 + J][t];
         }
+    if (narrow && tail > 0) {
+      // tail rows: lane (m, k) holds D[m][n], n = 2 k + t: side n / tail, row
+      // T + n % tail, column 8 J + m
+#pragma unroll
+      for (int J = 0; J < NB; ++J)
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+          const int n_ = 2 * kq() + t;
+          if (n_ < 2 * tail && (n_ >= tail) == (side == 1)) {
+            const int i = 8 * (NB - 1) + (n_ < tail ? n_ : n_ - tail), j = 8 * J + mq();
+            if (i < pa && j <= i) A()[i * (i + 1) / 2 + j] = cL[(NB - 1) * NB / 2 + J][t];
+          }
+        }
+    }
     __syncwarp();
     double lam;
     if (warp_ridge_solve(A(), z_, p, ridge, lam)) {
@@ -1947,6 +2001,10 @@ __device__ void SplitWarp<NB>::run(int item) {
   pa = p + 1;
   E = pa * (pa + 1) / 2;
   xcol = x_column(kind);
+  tail = pa - 8 * (NB - 1);
+  narrow = tail <= 4;
+  nks = (p + 3) >> 2;
+  nbx = (xcol + d + 7) >> 3;
   T0 = a.temperature[k];
   ridge = a.ridge[k];
   const int req = max(a.min_side ? max(1, a.min_side[k]) : P.min_side_points,
