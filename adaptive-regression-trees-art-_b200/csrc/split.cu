@@ -51,6 +51,8 @@ constexpr int kErrSlot = 2 + 2 * kBuckets;  // counts[kErrSlot]: a bounded wait 
 // depends on n alone, so a node's result never depends on its batch.
 constexpr int kGangRows = 16384;
 constexpr int kGangMax = 16;
+// CTA form with FP64 MMA Grams: (side, 8 x 8 block) items per warp, at most
+constexpr int kDgMax = 6;
 // A gang forms when its last member is popped, which can wait for other
 // work items to finish: that wait is bounded by a longer limit than the
 // in-pass barriers (members then run side by side).
@@ -91,6 +93,7 @@ struct SplitArgs {
   int R, Rg, groups, dmax, pmax, H, TC, S, CH;
   int mixed;  // ART_PRECISION_MIXED: gates in single precision
   int tc;     // mixed form with the soft-pass Grams on the tensor cores
+  int dg;     // side Grams as FP64 MMA tiles (8 x 8 blocks of (q psi)^T psi, at most kDgMax per warp)
   // per (node, restart) results, index k * R + r
   double* r_theta;   // [.. ][dmax + 1]
   double* r_loss;
@@ -125,7 +128,13 @@ struct SLayout {
       tcop, tcbar, total;
 };
 __host__ __device__ inline size_t al(size_t v) { return (v + 15) & ~(size_t)15; }
-__host__ __device__ inline SLayout split_layout(int dmax, int pmax, int Rg, int H, int S, int CH, int tc = 0) {
+// phi's row stride: odd, and covering whole 8-column blocks for the MMA Grams
+__host__ __device__ inline int phi_stride(int pmax, int dg) {
+  const int pa = pmax + 1;
+  return dg ? ((8 * ((pa + 7) / 8)) | 1) : (pa | 1);
+}
+__host__ __device__ inline SLayout split_layout(int dmax, int pmax, int Rg, int H, int S, int CH, int tc = 0,
+                                                int dg = 0) {
   SLayout L;
   const int pa = pmax + 1, E = pa * (pa + 1) / 2, dt = dmax + 1;
   size_t o = 0;
@@ -136,7 +145,7 @@ __host__ __device__ inline SLayout split_layout(int dmax, int pmax, int Rg, int 
   // row-indexed arrays use odd row strides (in doubles), so that lanes
   // reading different rows of a chunk fall in different banks
   L.xp = o; o = al(o + (size_t)CH * (dmax | 1) * 8);
-  L.phi = o; o = al(o + (size_t)CH * (pa | 1) * 8);
+  L.phi = o; o = al(o + (size_t)CH * phi_stride(pmax, dg) * 8);
   L.tcop = 0;
   if (tc) {
     // the weights Q (hard Gram pass), the row cache (residual and trial
@@ -191,6 +200,14 @@ __device__ __forceinline__ int row_groups(int items) {
 __device__ __forceinline__ double group_sum(double v, int RG) {
   for (int o = 1; o < RG; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
+}
+
+// D = A B + D for one 8 x 8 x 4 FP64 tile (warp-wide): lane l holds
+// A[l / 4][l % 4], B[l % 4][l / 4] and D[l / 4][2 (l % 4) + {0, 1}].
+__device__ __forceinline__ void dmma_884(double (&c)[2], double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+      : "+d"(c[0]), "+d"(c[1])
+      : "d"(a), "d"(b));
 }
 
 struct Item {
@@ -325,7 +342,7 @@ struct SplitCta {
   uint32_t tc_commits = 0, tc_waits = 0, tmem = 0;
 
   __device__ SplitCta(const SplitArgs& a_, unsigned char* sm_) : a(a_), sm(sm_) {
-    L = split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S, a.CH, a.tc);
+    L = split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S, a.CH, a.tc, a.dg);
     rbar = (uint64_t*)(sm + L.bars);
     xs = (const double*)(sm + L.ring); ys = xs; phi = (double*)(sm + L.phi);
     xp = (double*)(sm + L.xp);
@@ -495,6 +512,96 @@ struct SplitCta {
     return s0 + s1;
   }
 
+  // ---- Gram pass on the FP64 tensor path: G_c = (Q[:, c] psi)^T psi over
+  // the rows, as lower 8 x 8 blocks (I, J) of NB = ceil((pmax + 1) / 8) block
+  // rows, one mma.sync.m8n8k4 per 4 rows.  The (column c, block) items are
+  // dealt to the warps (item t to warp t % 8, at most kDgMax each); lane
+  // (m, k) of a warp holds rows 8 I + m, columns 8 J + 2 k + {0, 1}.  The
+  // gates are computed as in gram_pass.
+  __device__ void gram_pass_dg(bool hard) {
+    const int C2 = 2 * a.Rg;
+    const int NB = (a.pmax + 1 + 7) >> 3, NBLK = NB * (NB + 1) / 2;
+    const int nitems = C2 * NBLK;
+    const int kq = lane & 3, mq = lane >> 2;
+    int code[kDgMax];  // c | I << 8 | J << 16, or -1
+#pragma unroll
+    for (int u = 0; u < kDgMax; ++u) {
+      const int t = warp + kWarps * u;
+      code[u] = -1;
+      if (t < nitems) {
+        const int c = t / NBLK, b = t - c * NBLK;
+        int I = 0;
+        while ((I + 1) * (I + 2) / 2 <= b) ++I;
+        const int J = b - I * (I + 1) / 2;
+        code[u] = c | (I << 8) | (J << 16);
+      }
+    }
+    double acc[kDgMax][2];
+#pragma unroll
+    for (int u = 0; u < kDgMax; ++u) acc[u][0] = acc[u][1] = 0.0;
+    begin_pass();
+    for (int64_t c0 = (int64_t)grank * a.CH; c0 < it.n; c0 += (int64_t)gsize * a.CH) {
+      const int rows = load_chunk(c0);
+      for (int pr = tid; pr < rows * a.Rg; pr += kSplitThreads) {
+        const int row = pr / a.Rg, r = pr - row * a.Rg;
+        double qL = 0.0, qR = 0.0;
+        if (r < it.rn && S(r, RS_ACTIVE) != 0.0) {
+          if (hard) {
+            const double* w = th + r * dt();
+            const bool right = right_side(xp + row * xps, w, it.d, w[it.d]);
+            qL = right ? 0.0 : 1.0;
+            qR = right ? 1.0 : 0.0;
+            if (right) atomicAdd(&S(r, RS_NRIGHT), 1.0);  // integers: exact in any order
+          } else {
+            const double pi = gate((score(r, row) - th[r * dt() + it.d]) * S(r, RS_INVT));
+            qL = fmax(1.0 - pi, a.prm.weight_floor);
+            qR = fmax(pi, a.prm.weight_floor);
+          }
+        }
+        Q[row * qs + 2 * r] = qL;
+        Q[row * qs + 2 * r + 1] = qR;
+      }
+      __syncthreads();
+      for (int k0 = 0; k0 < rows; k0 += 4) {
+        const int row = k0 + kq;
+        const bool in = row < rows;
+        const double* prow = phi + row * phs + mq;
+#pragma unroll
+        for (int u = 0; u < kDgMax; ++u) {
+          if (code[u] >= 0) {  // warp-uniform
+            const int c = code[u] & 0xff, I = (code[u] >> 8) & 0xff, J = code[u] >> 16;
+            const double av = in ? Q[row * qs + c] * prow[8 * I] : 0.0;
+            const double bv = in ? prow[8 * J] : 0.0;
+            dmma_884(acc[u], av, bv);
+          }
+        }
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int u = 0; u < kDgMax; ++u) {
+      if (code[u] >= 0) {
+        const int c = code[u] & 0xff, I = (code[u] >> 8) & 0xff, J = code[u] >> 16;
+#pragma unroll
+        for (int t2 = 0; t2 < 2; ++t2) {
+          const int i = 8 * I + mq, j = 8 * J + 2 * kq + t2;
+          if (i < it.pa && j <= i) G[(size_t)pk(i, j) * C2 + c] = acc[u][t2];
+        }
+      }
+    }
+    __syncthreads();
+    if (gsize > 1) {
+      gang_reduce(G, it.E * C2);
+      if (hard) {  // right-side counts (integers: exact in any order)
+        if (tid < a.Rg) red[tid] = S(tid, RS_NRIGHT);
+        __syncthreads();
+        gang_reduce(red, a.Rg);
+        if (tid < a.Rg) S(tid, RS_NRIGHT) = red[tid];
+        __syncthreads();
+      }
+    }
+  }
+
   // ---- Gram pass: G[e][c] = sum_k Q[k][c] P[k][e]; hard = gates from the
   // exact side of each row (weights 1/0, no floor), else soft gates.
   // Threads beyond the tiles share their rows: RG row groups, group g taking
@@ -502,6 +609,10 @@ struct SplitCta {
   // group order at the end (RG = 1, one thread per tile, when the tiles
   // already fill the CTA).
   __device__ void gram_pass(bool hard) {
+    if (a.dg) {
+      gram_pass_dg(hard);
+      return;
+    }
     const int E = it.E, C2 = 2 * a.Rg;
     const int nct = (C2 + TC - 1) / TC, net = (E + TE - 1) / TE;
     const int ntiles = nct * net;
@@ -1083,7 +1194,7 @@ __device__ void SplitCta<TC, TCG>::run(int item_id, int rank, int members) {
   it.p = feature_count(it.d, it.kind);
   it.pa = it.p + 1;
   xps = it.d | 1;
-  phs = it.pa | 1;
+  phs = a.dg ? phi_stride(a.pmax, 1) : (it.pa | 1);
   it.E = it.pa * (it.pa + 1) / 2;
   it.T0 = a.temperature[k];
   it.ridge = a.ridge[k];
@@ -1100,6 +1211,8 @@ __device__ void SplitCta<TC, TCG>::run(int item_id, int rank, int members) {
     eidx[2 * e + 1] = (int16_t)j;
   }
   for (int q = tid; q < a.Rg * 32; q += kSplitThreads) rs[q] = 0.0;
+  if (a.dg)  // phi's columns past this item's pa read as zeros in the MMA Grams
+    for (int e = tid; e < a.CH * phs; e += kSplitThreads) phi[e] = 0.0;
   __syncthreads();
   // initial theta: projected theta0 (splitters.py:379)
   if (tid < it.rn) {
@@ -1448,14 +1561,6 @@ __device__ void SplitCta<TC, TCG>::run(int item_id, int rank, int members) {
 // needs no separate Gram pass.  Same objective, stop rules, Armijo steps,
 // AdaptiveAlpha, feasibility tracking, hard partition and refits as the CTA
 // kernel above; the summation order differs.
-
-// D = A B + D for one 8 x 8 x 4 FP64 tile (warp-wide): lane l holds
-// A[l / 4][l % 4], B[l % 4][l / 4] and D[l / 4][2 (l % 4) + {0, 1}].
-__device__ __forceinline__ void dmma_884(double (&c)[2], double a, double b) {
-  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-      : "+d"(c[0]), "+d"(c[1])
-      : "d"(a), "d"(b));
-}
 
 constexpr int kWTile = 32;                                   // rows per tile
 constexpr int kWMaxPa = 24;                                  // p + 1 (augmented with y)
@@ -2654,6 +2759,14 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
     prof_end(s);
     count_launch();
   }
+  // CTA form without the tensor-core Gram, one or two restarts per CTA: side
+  // Grams as FP64 MMA tiles when the (side, block) items fit the warps'
+  // accumulators (measured on the B200: 1.8x on wide single-restart levels;
+  // with 4 restarts per CTA the thread-tile sums are faster)
+  if (!use_warp && !use_tc && Rg <= 2) {
+    const int nb = (pr->max_features + 1 + 7) / 8;
+    a.dg = 2 * Rg * (nb * (nb + 1) / 2) <= kWarps * kDgMax ? 1 : 0;
+  }
   if (use_warp) {
     // one work item per (node, restart), largest nodes first
     a.Rg = 1;
@@ -2716,16 +2829,17 @@ extern "C" int art_split_level(const ArtSplitProblem* pr, const ArtSplitParams* 
     a.S = kMaxStages;
     while (a.S > 2 && split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S, a.CH, 1).total > 227 * 1024) --a.S;
   } else {
-    if (minb == 2 && split_layout(a.dmax, a.pmax, a.Rg, a.H, 1, 32).total > kHalfSmem) minb = 1;
+    if (minb == 2 && split_layout(a.dmax, a.pmax, a.Rg, a.H, 1, 32, 0, a.dg).total > kHalfSmem) minb = 1;
     const size_t chunk_budget = minb == 2 ? 100 * 1024 : 200 * 1024;
     const size_t smem_budget = minb == 2 ? kHalfSmem : 227 * 1024;
     const int min_stages = minb == 2 ? 2 : 4;
     a.CH = kMaxCH;
-    while (a.CH > 32 && split_layout(a.dmax, a.pmax, a.Rg, a.H, min_stages, a.CH).total > chunk_budget) a.CH >>= 1;
+    while (a.CH > 32 && split_layout(a.dmax, a.pmax, a.Rg, a.H, min_stages, a.CH, 0, a.dg).total > chunk_budget)
+      a.CH >>= 1;
     a.S = kMaxStages;
-    while (a.S > 1 && split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S, a.CH).total > smem_budget) --a.S;
+    while (a.S > 1 && split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S, a.CH, 0, a.dg).total > smem_budget) --a.S;
   }
-  const size_t smem = split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S, a.CH, a.tc).total;
+  const size_t smem = split_layout(a.dmax, a.pmax, a.Rg, a.H, a.S, a.CH, a.tc, a.dg).total;
   if (smem > 227 * 1024) { set_error("art_split_level: shared memory %zu too large", smem); return ART_E_UNSUPPORTED; }
   auto launch = [&](auto kern) -> int {
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
