@@ -379,15 +379,36 @@ class ServingEngine:
                                        ptr(perm), ptr(n_right), stream_handle(self.stream)), "art_partition_rows")
         nr = n_right.cpu().numpy()
         th = theta.cpu().numpy()
+        # each job's nodes are consecutive in the batch, with one row width:
+        # its rows in partitioned order by one gather, written back by one
+        # slice copy (or one indexed copy when its nodes' row ranges have gaps);
+        # unsplit nodes are copied unchanged
+        j0 = 0
+        while j0 < len(sub):
+            st = sub[j0][0]
+            j1 = j0
+            while j1 + 1 < len(sub) and sub[j1 + 1][0] is st:
+                j1 += 1
+            dim = st.job.dim
+            s0, s1 = int(sro[j0]), int(sro[j1 + 1])
+            src = xs[int(sxo[j0]): int(sxo[j0]) + (s1 - s0) * dim].view(s1 - s0, dim)
+            loc = perm[s0:s1] - s0
+            r0s = np.array([sub[j][1].r0 for j in range(j0, j1 + 1)], dtype=np.int64)
+            lens = n[j0:j1 + 1]
+            if np.all(r0s[1:] == r0s[:-1] + lens[:-1]):
+                st.X[int(r0s[0]): int(r0s[0]) + s1 - s0] = src[loc]
+                st.y[int(r0s[0]): int(r0s[0]) + s1 - s0] = ys[s0:s1][loc]
+            else:
+                dst = t.as_tensor(np.repeat(r0s - (np.cumsum(lens) - lens), lens) + np.arange(s1 - s0), device=dev)
+                st.X[dst] = src[loc]
+                st.y[dst] = ys[s0:s1][loc]
+            j0 = j1 + 1
         for j, (st, nd) in enumerate(sub):
             if not ok[j]:
                 st.leaves.append(nd)   # no valid split: the node stays a leaf
                 continue
             a, b = int(sro[j]), int(sro[j + 1])
             dim = st.job.dim
-            local = perm[a:b] - a
-            st.X[nd.r0:nd.r1] = xs[sxo[j]: sxo[j] + (b - a) * dim].view(b - a, dim)[local]
-            st.y[nd.r0:nd.r1] = ys[a:b][local]
             nl = (b - a) - int(nr[j])
             w, z = th[j, :dim].copy(), float(th[j, dim])
             nd.theta = th[j, : dim + 1].copy()
