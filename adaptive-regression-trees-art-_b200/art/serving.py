@@ -148,6 +148,28 @@ def _target_numpy(job: SurrogateJob):
     return f
 
 
+def _ranges(starts, lens) -> np.ndarray:
+    """The concatenation of arange(s, s + l) over (starts, lens)."""
+    lens = np.asarray(lens, dtype=np.int64)
+    return np.repeat(np.asarray(starts, dtype=np.int64) - (np.cumsum(lens) - lens), lens) + np.arange(int(lens.sum()))
+
+
+def _runs(work):
+    """(job state, node row starts, node row counts) for each job's consecutive nodes of ``work``."""
+    out = []
+    q0 = 0
+    while q0 < len(work):
+        st = work[q0][0]
+        q1 = q0
+        while q1 + 1 < len(work) and work[q1 + 1][0] is st:
+            q1 += 1
+        nodes = [nd for _, nd in work[q0:q1 + 1]]
+        out.append((st, np.array([nd.r0 for nd in nodes], dtype=np.int64),
+                    np.array([nd.r1 - nd.r0 for nd in nodes], dtype=np.int64)))
+        q0 = q1 + 1
+    return out
+
+
 @dataclass
 class _Node:
     path: str
@@ -294,8 +316,16 @@ class ServingEngine:
         """Concatenate the rows of the given (job, node) pairs into one batch."""
 
         t = torch()
-        xs = [st.X[nd.r0:nd.r1].reshape(-1) for st, nd in work]
-        ys = [st.y[nd.r0:nd.r1] for st, nd in work]
+        xs, ys = [], []
+        for st, r0s, lens in _runs(work):
+            if np.all(r0s[1:] == r0s[:-1] + lens[:-1]):  # one contiguous range of the job's rows
+                a, b = int(r0s[0]), int(r0s[0] + lens.sum())
+                xs.append(st.X[a:b].reshape(-1))
+                ys.append(st.y[a:b])
+            else:
+                idx = t.as_tensor(_ranges(r0s, lens), device=st.X.device)
+                xs.append(st.X[idx].reshape(-1))
+                ys.append(st.y[idx])
         n = np.array([nd.r1 - nd.r0 for _, nd in work], dtype=np.int64)
         d = np.array([st.job.dim for st, _ in work], dtype=np.int32)
         ro = np.concatenate([[0], np.cumsum(n)]).astype(np.int64)
@@ -345,9 +375,30 @@ class ServingEngine:
     def _split(self, sub, x, y, ro, xo, d, kinds, idx, iters, warp) -> None:
         t = torch()
         dev = x.device
-        # the split nodes' rows, gathered from the fit batch
-        xs = t.cat([x[xo[k]: xo[k] + (ro[k + 1] - ro[k]) * d[k]] for k in idx])
-        ys = t.cat([y[ro[k]: ro[k + 1]] for k in idx])
+        # the split nodes' rows, gathered from the fit batch: a job's nodes are
+        # consecutive there, with one row width, so one slice or gather per job
+        xl, yl = [], []
+        q0 = 0
+        while q0 < len(idx):
+            q1 = q0
+            while q1 + 1 < len(idx) and sub[q1 + 1][0] is sub[q0][0]:
+                q1 += 1
+            ks = np.asarray(idx[q0:q1 + 1])
+            dim = int(d[ks[0]])
+            lens = ro[ks + 1] - ro[ks]
+            if np.all(ks[1:] == ks[:-1] + 1):
+                a, b = int(ro[ks[0]]), int(ro[ks[-1] + 1])
+                xl.append(x[int(xo[ks[0]]): int(xo[ks[0]]) + (b - a) * dim])
+                yl.append(y[a:b])
+            else:
+                rows = t.as_tensor(_ranges(ro[ks], lens), device=dev)
+                base = int(xo[ks[0]]) - int(ro[ks[0]]) * dim   # the job's block of x, viewed as rows
+                blk = x[base + int(ro[ks[0]]) * dim: base + int(ro[ks[-1] + 1]) * dim].view(-1, dim)
+                xl.append(blk[rows - int(ro[ks[0]])].reshape(-1))
+                yl.append(y[rows])
+            q0 = q1 + 1
+        xs = t.cat(xl)
+        ys = t.cat(yl)
         n = np.array([ro[k + 1] - ro[k] for k in idx], dtype=np.int64)
         dd = d[idx]
         sro = np.concatenate([[0], np.cumsum(n)]).astype(np.int64)
