@@ -356,6 +356,9 @@ class ServingEngine:
                 st.leaves.append(nd)
             else:
                 split_idx.append(k)
+        # (The CTA form runs two CTAs per SM here: many small single-restart
+        # nodes keep one CTA per SM waiting at its barriers; 1.34x on a level
+        # of 4,609 such d = 32 nodes.)
         # max_iters is a per-call parameter of the split search (one call per
         # distinct value); the minimum side count goes per node, so nodes of
         # every dimension share a launch.  Nodes for the warp-per-restart form
@@ -412,8 +415,8 @@ class ServingEngine:
                                  n_restarts=1)
         res = split_level(sp, xs, ys, sro, dd, kinds[idx], temps, ridge, x_offsets=sxo, hard_refit=False,
                           node_keys=keys, max_dim=int(dd.max()), max_features=int(max(st.job.n_features for st, _ in sub)),
-                          min_side_points=min_side, group_restarts=0, trial_steps=0, ctas_per_sm=0,
-                          restart_warps=int(warp), stream=self.stream)
+                          min_side_points=min_side, group_restarts=0, trial_steps=0,
+                          ctas_per_sm=0 if warp else 2, restart_warps=int(warp), stream=self.stream)
         failure = res.failure.cpu().numpy()
         theta = res.theta
         ok = failure == 0
