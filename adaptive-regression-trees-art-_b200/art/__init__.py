@@ -66,6 +66,7 @@ from .sampling import (
     floor_covariance_eigenvalues,
     hit_and_run_device,
     infer_box_bounds,
+    covariance_eigendecomposition_batched,
     sample_covariance_eigendecomposition,
     sample_uniform_box,
 )

@@ -151,6 +151,7 @@ SIGNATURES = {
     "art_segment_residuals": (C.c_int, [C.POINTER(ArtSegments), P, P, P, I64, P, P, P]),
     "art_tree_predict": (C.c_int, [I32, I64, P, P, I64, P, I64, P, I64, P, P, P, P]),
     "art_median_nn_distance": (C.c_int, [I64, P, P, P, P, P, I32, F64, P, P]),
+    "art_covariance_eigh": (C.c_int, [P, P, I64, I32, P, P, P, P]),
     "art_last_error": (C.c_char_p, []),
     "art_abi_version": (C.c_int, []),
     "art_launch_count": (C.c_uint64, []),

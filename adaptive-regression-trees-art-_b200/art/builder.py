@@ -47,6 +47,7 @@ from .models import (
 from .sampling import (
     HitAndRunSampler,
     Sampler,
+    covariance_eigendecomposition_batched,
     floor_covariance_eigenvalues,
     sample_covariance_eigendecomposition,
     sample_uniform_box,
@@ -510,6 +511,9 @@ class RegressionTreeBuilder:
                                                    [r[5] for r in reqs])
                 out = [None] * len(reqs)
                 main_idx, spectra, starts = [], [], []
+                good = [q for q, pl in enumerate(pilots) if not isinstance(pl, Exception)
+                        and np.asarray(pl, float).shape == (pilot_len, self.dimension)]
+                eig = dict(zip(good, self._pilot_spectra([np.asarray(pilots[q], float) for q in good], sp)))
                 for q, pilot in enumerate(pilots):
                     if isinstance(pilot, Exception):
                         if reqs[q][6][1] is not None:  # failed after the main seed was drawn: undo
@@ -524,7 +528,7 @@ class RegressionTreeBuilder:
                     if pilot.shape != (pilot_len, self.dimension):
                         out[q] = RuntimeError(f"Pilot sampler returned shape {pilot.shape}.")
                         continue
-                    vecs, vals = sample_covariance_eigendecomposition(pilot)
+                    vecs, vals = eig[q]
                     safe, floor = floor_covariance_eigenvalues(vals, sp.direction_eigenvalue_floor)
                     saturated = bool(np.any(vals <= floor))
                     metas[q] = {"sampling_method": "isotropic_hit_and_run", "sampling_thinning": sp.thinning,
@@ -881,6 +885,17 @@ class RegressionTreeBuilder:
                        "sampling_covariance_condition_number": None, "sampling_warnings": ()}
         return self._sample_region(region, self._target_samples, x0=None, sampler=self.root_sampler)
 
+    def _pilot_spectra(self, pilots, sampler):
+        """(eigenvectors, eigenvalues) of each pilot's sample covariance
+        (builder.py:1141-1200): on the host with numpy's eigh when the sampler
+        follows the reference's random stream, else all pilots in one device
+        launch (``art_covariance_eigh``), so covariance-shaped top-ups stay on
+        the GPU; one-at-a-time and cohort top-ups take the same path."""
+
+        if getattr(sampler, "rng_mode", "reference") == "device":
+            return covariance_eigendecomposition_batched(pilots)
+        return [sample_covariance_eigendecomposition(p) for p in pilots]
+
     def _sample_region(self, region, n, *, x0, sampler):
         with self._timing_context("sampling"):
             return self._sample_region_untimed(region, n, x0=x0, sampler=sampler)
@@ -899,7 +914,7 @@ class RegressionTreeBuilder:
             pilot = np.asarray(pilot_sampler.sample(region, pilot_len, random_state=self._next_seed(), x0=x0), float)
             if pilot.shape != (pilot_len, self.dimension):
                 raise RuntimeError(f"Pilot sampler returned shape {pilot.shape}.")
-            vecs, vals = sample_covariance_eigendecomposition(pilot)
+            vecs, vals = self._pilot_spectra([pilot], sampler)[0]
             safe, floor = floor_covariance_eigenvalues(vals, sampler.direction_eigenvalue_floor)
             saturated = bool(np.any(vals <= floor))
             node_sampler = replace(sampler, direction_eigenvectors=vecs, direction_eigenvalues=vals)

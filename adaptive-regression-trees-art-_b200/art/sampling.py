@@ -72,6 +72,45 @@ def sample_covariance_eigendecomposition(samples, *, assume_centered: bool = Fal
     return eigenvectors, eigenvalues
 
 
+def covariance_eigendecomposition_batched(sample_sets, *, stream=None):
+    """``sample_covariance_eigendecomposition`` for many point sets of one
+    dimension in one device launch (``art_covariance_eigh``): returns a list
+    of (eigenvectors, eigenvalues) host arrays, eigenvalues ascending and
+    eigenvector j in column j as numpy's ``eigh``.  Each eigenvector's
+    largest-magnitude component is positive (numpy's signs are LAPACK's),
+    and values agree with ``eigh`` to rounding.  Raises like the host form
+    for sets of fewer than two points or with non-finite values."""
+
+    t = torch()
+    dev = require_cuda()
+    sets = [np.asarray(v, dtype=float) for v in sample_sets]
+    if not sets:
+        return []
+    d = sets[0].shape[1] if sets[0].ndim == 2 else -1
+    for v in sets:
+        if v.ndim != 2 or v.shape[1] != d:
+            raise ValueError("every sample set must have shape (n_samples, d) with one d.")
+        if v.shape[0] < 2:
+            raise ValueError("samples must contain at least two points.")
+        if not np.all(np.isfinite(v)):
+            raise ValueError("samples must contain only finite values.")
+    lib = N.load_library()
+    x = to_device(np.concatenate(sets).reshape(-1), t.float64, dev)
+    ro = to_device(np.concatenate([[0], np.cumsum([v.shape[0] for v in sets])]).astype(np.int64), t.int64, dev)
+    K = len(sets)
+    vals = t.empty((K, d), dtype=t.float64, device=dev)
+    vecs = t.empty((K, d, d), dtype=t.float64, device=dev)
+    status = t.empty(K, dtype=t.int32, device=dev)
+    N.check(lib.art_covariance_eigh(ptr(x), ptr(ro), K, d, ptr(vals), ptr(vecs), ptr(status), stream_handle(stream)),
+            "art_covariance_eigh")
+    st = status.cpu().numpy()
+    if np.any(st != 0):
+        raise RuntimeError(f"covariance eigendecomposition failed for set(s) {np.flatnonzero(st != 0).tolist()} "
+                           f"(status {st[st != 0].tolist()}).")
+    vals_h, vecs_h = vals.cpu().numpy(), vecs.cpu().numpy()
+    return [(vecs_h[k], vals_h[k]) for k in range(K)]
+
+
 def floor_covariance_eigenvalues(eigenvalues, floor_ratio: float):
     """sampling.py:109-127."""
 

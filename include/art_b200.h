@@ -403,6 +403,21 @@ ART_API int art_median_nn_distance(int64_t count, const double* x, const int64_t
                            const int64_t* sample_rows, int32_t max_set, double c,
                            double* temperature, art_stream_t stream);
 
+/* Sample covariance and its eigendecomposition for `count` point sets of
+ * dimension dim <= 64 (the pilot-chain spectrum of the covariance-shaped
+ * sampler: sample_covariance_eigendecomposition, sampling.py:86-106, called
+ * per child at builder.py:1141-1200).  Set k holds rows
+ * [row_offsets[k], row_offsets[k+1]) of samples (row-major, dim doubles a
+ * row); C = (X - mean)^T (X - mean) / (n - 1).  Writes eigenvalues [count][dim]
+ * in ascending order and eigenvectors [count][dim][dim] with eigenvector j in
+ * column j (numpy.linalg.eigh's layout); each eigenvector's largest-magnitude
+ * component is positive.  status[k]: 0 converged, 1 not converged in 40
+ * Jacobi sweeps, -1 fewer than two rows, -2 a non-finite sample (then NaN
+ * outputs).                                                                  */
+ART_API int art_covariance_eigh(const double* samples, const int64_t* row_offsets, int64_t count,
+                                int32_t dim, double* eigenvalues, double* eigenvectors,
+                                int32_t* status, art_stream_t stream);
+
 /* ======================================================================== */
 /*  Misc                                                                     */
 /* ======================================================================== */
