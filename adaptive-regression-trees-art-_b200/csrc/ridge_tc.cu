@@ -48,6 +48,10 @@ constexpr int kLBO = 128;                  // bytes between K-adjacent core matr
 constexpr int kSBO = (kKC / kKE) * 128;    // bytes between 8-feature groups
 constexpr int kOpBytes = kGroups * kSBO;   // one operand array (hi or lo)
 constexpr int kMaxRefine = 14;
+constexpr int kRefRows = 3;                // rows per warp step in the refinement passes
+constexpr int kGenRows = kKC / (kTcThreads / 32);  // operand rows generated per warp and chunk
+constexpr int kLaneFeat = kPmax / 32;      // features per lane
+static_assert(kGenRows == 4, "a warp's rows form one K-row of core matrices");
 // TMEM accumulation chains are restarted every kDrainChunks stages: the
 // FP32 accumulator of the tensor core loses low bits on every step, so the
 // chain length bounds the Gram error (~steps * 2^-24 relative); drained
@@ -59,7 +63,7 @@ constexpr int kDrainChunks = 4;
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) { return smem_desc_kmajor(addr, kLBO, kSBO); }
 // ------------------------------------------------------------- smem layout
 struct TcLayout {
-  size_t x[2], y[2], w[2], q, sq, op, bars, tmem, gram, vec, fidx, total;
+  size_t x[2], y[2], w[2], op, bars, tmem, gram, vec, fidx, total;
 };
 __host__ __device__ inline size_t a16(size_t v) { return (v + 15) & ~(size_t)15; }
 __host__ __device__ inline TcLayout tc_layout(int pmax, int dmax, int factor_bytes) {
@@ -70,8 +74,6 @@ __host__ __device__ inline TcLayout tc_layout(int pmax, int dmax, int factor_byt
     L.y[s] = o; o = a16(o + (size_t)kKC * 8 + 16);
     L.w[s] = o; o = a16(o + (size_t)kKC * 8 + 16);
   }
-  L.q = o; o = a16(o + kKC * 8);
-  L.sq = o; o = a16(o + kKC * 8);
   o = (o + 127) & ~(size_t)127;
   L.op = o; o = a16(o + (size_t)2 * kOpBytes);     // one stage: hi, lo
   L.bars = o; o = a16(o + 4 * 8);
@@ -104,8 +106,6 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
   TF* Gf = (TF*)(smem + lay.gram);
   double* vec = (double*)(smem + lay.vec);
   int16_t* fidx = (int16_t*)(smem + lay.fidx);
-  double* sq_qy = (double*)(smem + lay.q);  // q_r y_r of the chunk's rows
-  double* sq_s = (double*)(smem + lay.sq);
   unsigned char* op = smem + lay.op;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
@@ -149,8 +149,10 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
       fidx[2 * f] = (int16_t)fa_;
       fidx[2 * f + 1] = (int16_t)fb_;
     }
-    // item slots of this thread: (f, octet) = (j % P16, j / P16), j = tid + 256 s
-    double hacc[3] = {0.0, 0.0, 0.0}, dacc[3] = {0.0, 0.0, 0.0};
+    // exact h and diag partial sums of this lane's features over its warp's rows
+    double hacc[kLaneFeat], dacc[kLaneFeat];
+#pragma unroll
+    for (int m = 0; m < kLaneFeat; ++m) hacc[m] = dacc[m] = 0.0;
     int bad = 0;
     if (tid == 0) {
       for (int64_t c = 0; c < min((int64_t)2, nchunks); ++c) {
@@ -167,6 +169,13 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
     }
     for (int64_t c = 0; c < min((int64_t)2, nchunks); ++c) S.load_issued[c]++;
     __syncthreads();
+    // this lane's feature factors, packed as (a + 8) | (b + 8) << 8
+    int gfab[kLaneFeat];
+#pragma unroll
+    for (int m = 0; m < kLaneFeat; ++m) {
+      const int f = lane + 32 * m;
+      gfab[m] = f < P16 ? (fidx[2 * f] + 8) | ((fidx[2 * f + 1] + 8) << 8) : 5 | (7 << 8);
+    }
     const uint32_t id1 = idesc_tf32(128, N1), id2 = idesc_tf32(128, two ? N2 : 16);
     for (int64_t c = 0; c < nchunks && !abort; ++c) {
       const int st = (int)(c & 1);
@@ -182,18 +191,30 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
       // input checks and the per-row q y and sqrt(q) need only this chunk's
       // rows, so they run while the tensor core may still hold the operand
       // buffer (the previous chunk's generation finished reading them)
-      if (okl) {
+      if (okl)
         for (int e = tid; e < rows * d; e += kTcThreads) bad |= isfinite(xs[e]) ? 0 : 1;
-        if (tid < kKC) {
-          double qv = 0.0;
-          if (tid < rows) {
-            bad |= isfinite(ys[tid]) ? 0 : 1;
-            const double wv = ws ? ws[tid] : 1.0;
-            if (!(wv >= 0.0) || !isfinite(wv)) bad |= 2;
-            qv = fmax(wv, a.weight_floor);
-          }
-          sq_qy[tid] = tid < rows ? qv * ys[tid] : 0.0;
-          sq_s[tid] = sqrt(qv);
+      // warp w generates rows 4w .. 4w+3 of the chunk (one K-row of core
+      // matrices), lane l the features l + 32 m; lanes 0..3 form the per-row
+      // sqrt(q) and q y of the warp's rows and broadcast them
+      const int rw = kGenRows * warp;
+      double sqr[kGenRows], qyr[kGenRows];
+      const double* xw[kGenRows];
+      {
+        double sq_l = 0.0, qy_l = 0.0;
+        if (okl && lane < kGenRows && rw + lane < rows) {
+          const double yv = ys[rw + lane];
+          bad |= isfinite(yv) ? 0 : 1;
+          const double wv = ws ? ws[rw + lane] : 1.0;
+          if (!(wv >= 0.0) || !isfinite(wv)) bad |= 2;
+          const double qv = fmax(wv, a.weight_floor);
+          qy_l = qv * yv;
+          sq_l = sqrt(qv);
+        }
+#pragma unroll
+        for (int u = 0; u < kGenRows; ++u) {
+          sqr[u] = __shfl_sync(0xffffffffu, sq_l, u);
+          qyr[u] = __shfl_sync(0xffffffffu, qy_l, u);
+          xw[u] = xs + (int64_t)(rw + u < rows ? rw + u : 0) * d;
         }
       }
       // one operand buffer: every MMA issued so far (chunks c-2 on barrier st,
@@ -209,37 +230,30 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
       if (p1) S.mma_waits[st ^ 1]++;
       unsigned char* hi = op;
       unsigned char* lo = hi + kOpBytes;
-      const int nitems = P16 * (kKC / 8);
 #pragma unroll
-      for (int s = 0; s < 3; ++s) {
-        const int j = tid + s * kTcThreads;
-        if (j < nitems) {
-          const int f = j % P16, oct = j / P16;
-          const int ia = fidx[2 * f], ib = fidx[2 * f + 1];
-          uint32_t ph[8], pl[8];
+      for (int m = 0; m < kLaneFeat; ++m) {
+        const int f = lane + 32 * m;
+        if (f < P16) {
+          const int ia = (gfab[m] & 255) - 8, ib = (gfab[m] >> 8) - 8;
+          uint32_t ph[kGenRows], pl[kGenRows];
 #pragma unroll
-          for (int e = 0; e < 8; ++e) {
-            const int r = oct * 8 + e;
+          for (int u = 0; u < kGenRows; ++u) {
             float v = 0.0f;
-            if (r < rows && ia != -3) {
-              const double* xr = xs + (int64_t)r * d;
-              const double phi = (ia < 0 ? 1.0 : xr[ia]) * (ib < 0 ? 1.0 : xr[ib]);
+            if (rw + u < rows && ia != -3) {
+              const double phi = (ia < 0 ? 1.0 : xw[u][ia]) * (ib < 0 ? 1.0 : xw[u][ib]);
               // h += phi (q y) and diag += (sqrt(q) phi)^2: one product fewer
               // and no separate y load per feature
-              const double sphi = sq_s[r] * phi;
-              hacc[s] = fma(phi, sq_qy[r], hacc[s]);
-              dacc[s] = fma(sphi, sphi, dacc[s]);
+              const double sphi = sqr[u] * phi;
+              hacc[m] = fma(phi, qyr[u], hacc[m]);
+              dacc[m] = fma(sphi, sphi, dacc[m]);
               v = (float)sphi;
             }
-            ph[e] = to_tf32(v);
-            pl[e] = to_tf32(v - __uint_as_float(ph[e]));
+            ph[u] = to_tf32(v);
+            pl[u] = to_tf32(v - __uint_as_float(ph[u]));
           }
-          // rows 8*oct .. 8*oct+7 span two K-adjacent core matrices (4 rows each)
-          const size_t off = (size_t)(f >> 3) * kSBO + (size_t)(2 * oct) * 128 + (size_t)(f & 7) * 16;
+          const size_t off = (size_t)(f >> 3) * kSBO + (size_t)warp * 128 + (size_t)(f & 7) * 16;
           *(uint4*)(hi + off) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
-          *(uint4*)(hi + off + 128) = make_uint4(ph[4], ph[5], ph[6], ph[7]);
           *(uint4*)(lo + off) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
-          *(uint4*)(lo + off + 128) = make_uint4(pl[4], pl[5], pl[6], pl[7]);
         }
       }
       fence_proxy_async();  // operand writes -> visible to the tensor core
@@ -338,15 +352,14 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
       __syncthreads();
       continue;
     }
-    // ---- reduce exact h and diag over the row octets (fixed order)
-    double* red = (double*)op;  // operand buffers are idle now
-    const int nitems = P16 * (kKC / 8);
+    // ---- reduce exact h and diag over the warps (fixed order)
+    double* red = (double*)op;  // operand buffers are idle now: [warp][P16] pairs
 #pragma unroll
-    for (int s = 0; s < 3; ++s) {
-      const int j = tid + s * kTcThreads;
-      if (j < nitems) {
-        red[2 * j] = hacc[s];
-        red[2 * j + 1] = dacc[s];
+    for (int m = 0; m < kLaneFeat; ++m) {
+      const int f = lane + 32 * m;
+      if (f < P16) {
+        red[2 * (warp * P16 + f)] = hacc[m];
+        red[2 * (warp * P16 + f) + 1] = dacc[m];
       }
     }
     {
@@ -362,9 +375,9 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
     double* v2 = vec + 5 * vs;
     for (int f = tid; f < p; f += kTcThreads) {
       double hs = 0.0, ds = 0.0;
-      for (int oct = 0; oct < kKC / 8; ++oct) {
-        hs += red[2 * (oct * P16 + f)];
-        ds += red[2 * (oct * P16 + f) + 1];
+      for (int wv = 0; wv < kTcThreads / 32; ++wv) {
+        hs += red[2 * (wv * P16 + f)];
+        ds += red[2 * (wv * P16 + f) + 1];
       }
       h[f] = hs;
       dg[f] = ds;
@@ -490,23 +503,39 @@ __global__ void __launch_bounds__(kTcThreads, sizeof(TF) == 4 ? 2 : 1) ridge_tc_
         const double* ws = a.w ? (const double*)(op + st * rstage + rx_bytes +
                                                  (((uintptr_t)(a.w + it.r0 + c * RC)) & 15))
                                : nullptr;
-        for (int j = slot; j < rows; j += kTcThreads / 32) {
-          const double* xk = xs + j * d;
-          double ph[5];
-          double dot = 0.0;
+        // kRefRows rows per warp and step, their dot products and shuffle
+        // sums interleaved; the accumulation still runs row by row in the
+        // warp's row order (the tail test is warp-uniform)
+        constexpr int kStep = kTcThreads / 32;
+        for (int j = slot; j < rows; j += kStep * kRefRows) {
+          double ph[kRefRows][5], dot[kRefRows];
 #pragma unroll
-          for (int m = 0; m < 5; ++m) {
-            const int ua = rfa[m], ub = rfb[m];
-            const double va = ua >= 0 ? xk[ua] : (ua == -1 ? 1.0 : 0.0);
-            const double vb = ub >= 0 ? xk[ub] : 1.0;
-            ph[m] = va * vb;
-            dot = fma(ph[m], bt[m], dot);
+          for (int u = 0; u < kRefRows; ++u) {
+            const int jj = j + kStep * u;
+            dot[u] = 0.0;
+            const double* xk = xs + (jj < rows ? jj : j) * d;
+#pragma unroll
+            for (int m = 0; m < 5; ++m) {
+              const int ua = rfa[m], ub = rfb[m];
+              const double va = ua >= 0 ? xk[ua] : (ua == -1 ? 1.0 : 0.0);
+              const double vb = ub >= 0 ? xk[ub] : 1.0;
+              ph[u][m] = va * vb;
+              dot[u] = fma(ph[u][m], bt[m], dot[u]);
+            }
           }
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
-          const double e = fmax(ws ? ws[j] : 1.0, a.weight_floor) * dot;
+          for (int o = 16; o > 0; o >>= 1)
 #pragma unroll
-          for (int m = 0; m < 5; ++m) accb[m] = fma(e, ph[m], accb[m]);
+            for (int u = 0; u < kRefRows; ++u) dot[u] += __shfl_xor_sync(0xffffffffu, dot[u], o);
+#pragma unroll
+          for (int u = 0; u < kRefRows; ++u) {
+            const int jj = j + kStep * u;
+            if (jj < rows) {
+              const double e = fmax(ws ? ws[jj] : 1.0, a.weight_floor) * dot[u];
+#pragma unroll
+              for (int m = 0; m < 5; ++m) accb[m] = fma(e, ph[u][m], accb[m]);
+            }
+          }
         }
         __syncthreads();  // every warp is done with this stage
         if (c + 2 < nch) {

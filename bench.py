@@ -35,10 +35,10 @@ sys.path.insert(0, str(ROOT))
 METRIC = "ridge solves/s"
 # DRAM bytes (read + write) per row of the tensor-core class, from the ncu
 # capture of the tensor-core ridge kernel on the 8,192-system case at the
-# tuned threshold (153 features): 1.0643 GB read + 0.0178 GB written over the
+# tuned threshold (153 features): 1.0477 GB read + 0.0180 GB written over the
 # class's 3,296,275 rows (the first pass reads x, y, w; the refinement passes
 # re-read x and w).
-RIDGE_TC_DRAM_BYTES_PER_ROW = 1.082126e9 / 3296275
+RIDGE_TC_DRAM_BYTES_PER_ROW = 1.065706e9 / 3296275
 UNIT = "solves/s"
 WORKLOAD = ("batched weighted ridge: 65,536 systems/GPU, n log-uniform [64, 8192], d in {8,16}, "
             "affine or quadratic features (p = 9/17/45/153), sigmoid-product weights, "
